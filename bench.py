@@ -1,0 +1,266 @@
+"""Walker-propagation benchmark (MPSQMC2::Walk hot path) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference] [--workload chain64]
+
+Workload chain64 (the L=64 chain configuration): D_T=64 trial, 2048 walkers of D_W=32 (trial
+compressed + N(0,1e-3) noise), dtau=0.01, one walker-step = propagation over all 63 couplings,
+local energy, statistics and threshold branching.  Prints one JSON line (rank 0).
+
+Timing: W untimed steps, then K steps in one engine call; device time from CUDA events recorded on
+the engine's stream around those K steps (the walker population, 1.8 GB, exceeds L2 so no flush
+is needed).  Multi-GPU: independent replicas (one population per rank), max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "walker-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--workload", default="chain64")
+    ap.add_argument("--walkers", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("gloo", timeout=timedelta(seconds=120))
+        pg = dist
+    return rank, world, local, pg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    return json.load(open(p)) if os.path.exists(p) else {}
+
+
+def fp64_peak_tflops():
+    """cuBLAS DGEMM 8192^3, best of 5 (CUDA events): the FP64 denominator (none is pre-measured)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = a @ b
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def reference_cpu(wl, sample_walkers=None, steps=1, threads=None):
+    """The reference's own classes (oracle/_ref/ref_harness, built from the reference sources) timed on
+    this host: propagation of `sample_walkers` walkers for `steps` steps, energy excluded (the
+    reference's H*Psi_T MPS does not fit at L=64, D_T=64)."""
+    from oracle import pyoracle as po
+    if not po.harness_available():
+        return None
+    threads = threads or os.cpu_count()
+    sample_walkers = sample_walkers or threads
+    with tempfile.TemporaryDirectory() as t:
+        path = os.path.join(t, "trial.mps")
+        po.write_mps(path, po.MPS(wl.trial.dims, wl.trial.data))
+        out = po.run_harness("propagate", path, wl.DW, sample_walkers, wl.dtau, steps,
+                             env_extra={"OMP_NUM_THREADS": str(threads)})
+    r = json.loads(out.strip().splitlines()[-1])
+    r["sample"] = (f"{sample_walkers} walkers x {steps} step(s) of {wl.name}, propagation only "
+                   f"(reference classes, per-coupling trial terms, no energy)")
+    r["cores"] = threads
+    return r
+
+
+def main():
+    args = parse()
+    rank, world, local, pg = dist_setup(args.gpus)
+    from mpsqmc_b200 import workloads
+
+    wl = workloads.chain64(Nw=args.walkers or 2048)
+    cfg = {"workload": f"{wl.name}: L={wl.L} Heisenberg chain, D_T={wl.DT}, D_W={wl.DW}, {wl.Nw} walkers/GPU, "
+                       f"dtau={wl.dtau}, Marsaglia(4) grid, FP64",
+           "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.DW, "dtau": wl.dtau,
+           "l2": "population (1.8 GB) larger than L2; no flush", "parallelism": f"replicas x{world}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        r = reference_cpu(wl, steps=1)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built"}))
+            return
+        total_t = 0.0
+        ws = 0
+        for _ in range(max(1, args.steps)):
+            rr = reference_cpu(wl, steps=1)
+            total_t += rr["seconds"]
+            ws += rr["walker_steps"]
+        v = ws / total_t
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "walker-steps/s", "n_gpus": 0,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
+                "data": "synthetic", "config": cfg,
+                "cpu_baseline": {"value": v, "unit": "walker-steps/s", "cores": r["cores"], "kind": "reference",
+                                 "sample": r["sample"]},
+                "e2e": {"value": v, "unit": "walker-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    from mpsqmc_b200 import Engine
+
+    inputs = wl.inputs()
+    walkers = wl.walkers()
+    eng = Engine(device=local, **inputs)
+    N = walkers.shape[0]
+    eng.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
+    eng.set_rng(wl.seed + 7919 * rank, 0)
+    eng.walk(args.warmup)
+    with ClockSampler(local) as clk:
+        stats = eng.walk(args.steps)
+        tim = eng.last_timing()
+    ws_done = sum(s["n_walkers"] for s in stats)
+    t_ms = tim["total_ms"]
+    k_ms = tim["step_kernel_ms"]
+    if pg is not None:
+        tt = torch.tensor([t_ms, k_ms, float(ws_done)], dtype=torch.float64)
+        mx = tt.clone()
+        pg.all_reduce(mx, op=pg.ReduceOp.MAX)
+        sm = tt.clone()
+        pg.all_reduce(sm, op=pg.ReduceOp.SUM)
+        t_ms, k_ms, ws_all = float(mx[0]), float(mx[1]), float(sm[2])
+    else:
+        ws_all = float(ws_done)
+    value = ws_all / (t_ms * 1e-3)
+
+    # roofline of the dominant kernel (walker_step_kernel): canonical FP64 work / kernel time
+    flops_ws = workloads.algorithmic_flops_per_walker_step(inputs["trial_dims"], inputs["walker_dims"],
+                                                           list(zip(inputs["ci"], inputs["cj"])))
+    achieved = flops_ws * ws_done / (k_ms * 1e-3) / 1e12
+    peak = fp64_peak_tflops() if rank == 0 else None
+
+    # end to end through the public API: host population -> device, K steps (stats read back each
+    # step), population -> host; host wall clock.
+    e2e = None
+    if not args.no_e2e:
+        eng2 = Engine(device=local, **inputs)
+        host_w = np.ascontiguousarray(walkers)
+        t0 = time.perf_counter()
+        eng2.set_walkers(host_w, np.ones(N), None, np.zeros(N), normalize=True)
+        eng2.set_rng(wl.seed + 7919 * rank, 0)
+        st2 = eng2.walk(args.steps)
+        back = eng2.get_walkers()
+        t1 = time.perf_counter()
+        ws2 = sum(s["n_walkers"] for s in st2)
+        nbytes = host_w.nbytes
+        e2e = {"value": ws2 * world / (t1 - t0), "unit": "walker-steps/s",
+               "h2d_bytes_per_step": int(nbytes / args.steps),
+               "d2h_bytes_per_step": int(back[0].nbytes / args.steps + 72)}
+        eng2.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        r = reference_cpu(wl, steps=1)
+        if r is not None:
+            cpu = {"value": r["walker_steps_per_s"], "unit": "walker-steps/s", "cores": r["cores"],
+                   "kind": "reference", "sample": r["sample"]}
+
+    if rank == 0:
+        prof_traffic = None
+        tp = os.path.join(ROOT, "profiles", "walker_step_kernel_traffic.json")
+        if os.path.exists(tp):
+            prof_traffic = json.load(open(tp)).get("bytes_per_launch")
+        line = {
+            "metric": METRIC, "value": value, "unit": "walker-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "energy": {"E_P_last": stats[-1]["E_P"], "E_T_last": stats[-1]["E_T"], "walkers_last": stats[-1]["n_after"]},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if peak else None, "traffic": prof_traffic,
+                         "kernel": "walker_step_kernel", "flops_per_walker_step": flops_ws,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor path)"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": tim["launches"],
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    eng.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,142 @@
+/*
+ * mpsqmc_gpu.h -- C ABI of the B200 walker-propagation engine (libmpsqmc_b200.so).
+ *
+ * Drop-in boundary for the reference's MPSQMC2 hot path.  The reference keeps the walk inside
+ * C++ objects (MPSQMC2.h:13-166, Walker.h:13-52, MPSstate.h:19-102, TrotterHeisenberg.h:16-40);
+ * these entry points are what those objects (or any FFI: ctypes, cgo, JNI) bind to.  Every call
+ * returns an int status (0 = success, negative = MPSQMC_E_*); nothing throws, nothing aborts.
+ * All arrays are plain host pointers; the library owns every device allocation.
+ *
+ * Data conventions (identical to the reference):
+ *   - MPS bond dims dims[0..L], dims[0] = dims[L] = 1 (MPSstate.cpp:20-28);
+ *   - site s stores dims[s]*dims[s+1]*d doubles, element [r + dims[s]*(c + dims[s+1]*sigma)]
+ *     (MPStensor.cpp:91-96); sites are concatenated in order;
+ *   - two-site propagator SVD tables per distinct coupling J: S[k], U[i + d*(j + d*k)],
+ *     VT[k + d*d*(i + d*j)] (TrotterHeisenberg.cpp:345-431);
+ *   - grid points grid[i + d*d*p] (GridGenerator.cpp:40-44);
+ *   - couplings (ci[c] < cj[c], J_c != 0) in the order MPSQMC2.cpp:286-299 builds them.
+ */
+#ifndef MPSQMC_GPU_H
+#define MPSQMC_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define MPSQMC_OK 0
+#define MPSQMC_E_ARG (-1)         /* invalid argument or size mismatch */
+#define MPSQMC_E_CUDA (-2)        /* a CUDA call failed (message: mpsqmc_last_error) */
+#define MPSQMC_E_NODEVICE (-3)    /* no CUDA device: there is no CPU fallback */
+#define MPSQMC_E_UNSUPPORTED (-4) /* configuration outside what the kernels implement */
+#define MPSQMC_E_CAPACITY (-5)    /* branching would exceed the walker capacity */
+#define MPSQMC_E_NUMERIC (-6)     /* NaN/Inf or non-positive weight sum detected */
+#define MPSQMC_E_EXTINCT (-7)     /* population control left no walker */
+
+typedef struct mpsqmc_ctx mpsqmc_ctx;
+
+/* Everything MPSQMC2's constructor (MPSQMC2.cpp:68-103) derives from its arguments. */
+typedef struct {
+  int L;                 /* chain length (HeisenbergMPO::gLength) */
+  int d;                 /* local dimension; the kernels implement d = 2 */
+  int nC;                /* number of couplings */
+  const int *ci;         /* first site of each coupling */
+  const int *cj;         /* second site of each coupling (only cj = ci + 1 is implemented) */
+  const double *cJ;      /* coupling strength of each coupling */
+  double h;              /* magnetic field (HeisenbergMPO::gField) */
+  double dtau;           /* imaginary time step */
+  const int *trial_dims; /* trial bond dims [L+1] (left-normalized trial, MPSQMC2.cpp:239) */
+  const double *trial;   /* trial tensors */
+  int nJ;                /* number of distinct couplings */
+  const double *Jvals;   /* [nJ] */
+  const double *U;       /* [nJ][d^4] */
+  const double *S;       /* [nJ][d^2] */
+  const double *VT;      /* [nJ][d^4] */
+  int G;                 /* grid points */
+  const double *grid;    /* [G][d^2] */
+  int Ndesired;          /* totalNDesiredWalkers */
+  int capacity;          /* walker slots (reference: max(1000, 3*Nwalkers), MPSQMC2.cpp:41) */
+  const int *walker_dims;/* common walker bond dims [L+1] */
+  int device;            /* CUDA device ordinal */
+} mpsqmc_config;
+
+/* Per-step statistics of Walk (MPSQMC2.cpp:465-498). */
+typedef struct {
+  int step;              /* step number (1-based, continues across calls) */
+  int n_walkers;         /* totalNCurrentWalkers during the step (before branching) */
+  int n_after;           /* walkers after population control */
+  double sum_weight;     /* sum of walker weights after propagation */
+  double avg_weight;     /* sum_weight / n_walkers */
+  double E_P;            /* projected (mixed) energy */
+  double E_T;            /* target energy log(scaling)/dtau */
+  double omega;          /* fluctuation metric */
+  double scaling;        /* Ndesired / sum_weight */
+  uint64_t draws;        /* uniforms consumed by this step */
+} mpsqmc_step_stats;
+
+/* Creation copies every input to the device.  Replaces MPSQMC2::MPSQMC2 + SetupTrial
+ * (MPSQMC2.cpp:68-103, 219-332) minus the trial-term copies, which the kernels do not need. */
+int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out);
+int mpsqmc_destroy(mpsqmc_ctx *ctx);
+
+/* Message of the last failure in this thread (static storage, never NULL). */
+const char *mpsqmc_last_error(void);
+
+/* Library version string. */
+const char *mpsqmc_version(void);
+
+/* Number of doubles in one walker (sum over sites of dims[s]*dims[s+1]*d). */
+long mpsqmc_walker_size(const mpsqmc_ctx *ctx);
+
+/* Upload N walkers in logical order (walkers: [N][walker_size]) with their weight, overlap and
+ * energy history (Walker.h:224-234).  Replaces SetupWalkers (MPSQMC2.cpp:381-441) and
+ * Walker(Walker*) copies.  When normalize != 0 each walker is first brought into the state
+ * Walker::setOverlap leaves it in (Walker.cpp:54-66): left-normalized, overlap recomputed,
+ * sign fixed; the given overlaps are then ignored. */
+int mpsqmc_set_walkers(mpsqmc_ctx *ctx, int N, const double *walkers, const double *weights,
+                       const double *overlaps, const double *ehist, int normalize);
+
+/* Download the current population in logical order; *N receives the count.  Any pointer may
+ * be NULL.  walkers must hold capacity*walker_size doubles (or the current N). */
+int mpsqmc_get_walkers(mpsqmc_ctx *ctx, int *N, double *walkers, double *weights,
+                       double *overlaps, double *ehist);
+
+/* Random stream: mt19937(seed) advanced by `skip` 32-bit outputs; every uniform is one output
+ * divided by 2^32 (Random.cpp:28-59 with Boost's uniform_real_distribution). */
+int mpsqmc_set_rng(mpsqmc_ctx *ctx, uint32_t seed, uint64_t skip);
+int mpsqmc_get_rng_draws(mpsqmc_ctx *ctx, uint64_t *draws_since_set);
+
+/* EnergyFunctionAndHistory(1, &E, false) (MPSQMC2.cpp:447, 688-747) on the current population. */
+int mpsqmc_energy(mpsqmc_ctx *ctx, double *E_P);
+
+/* Run `nsteps` iterations of the body of MPSQMC2::Walk (MPSQMC2.cpp:465-511): propagation of
+ * every walker (PropagateSeparately, 518-611), weight sum, E_T, local energies and history
+ * (688-747), threshold population control (613-686).  stats may be NULL or hold nsteps
+ * entries. */
+int mpsqmc_walk(mpsqmc_ctx *ctx, int nsteps, mpsqmc_step_stats *stats);
+
+/* Per-walker data of the most recent step, in the logical order used during that step (before
+ * branching): weight, overlap and local energy after propagation; parent[k] is the pre-branch
+ * index that walker k of the new population was copied from.  Any pointer may be NULL. */
+int mpsqmc_last_step_walkers(mpsqmc_ctx *ctx, int *n_before, double *weight, double *overlap,
+                             double *energy, int *n_after, int *parent);
+
+/* Optional per-coupling trace of the next mpsqmc_walk step (for parity tests):
+ * [N][nC][16 + 5] = C[16], PDF norm, uniform, grid index, weight, overlap after the coupling.
+ * Enable before the step; read after.  Costs one device buffer of capacity*nC*21 doubles. */
+int mpsqmc_set_trace(mpsqmc_ctx *ctx, int enable);
+int mpsqmc_get_trace(mpsqmc_ctx *ctx, double *trace, int *n_walkers);
+
+/* Device timing of the last mpsqmc_walk call: milliseconds spent in the walker-step kernel
+ * (summed over steps), and the number of kernel launches the call made. */
+int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms,
+                       int *kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPSQMC_GPU_H */

@@ -1,0 +1,212 @@
+"""ctypes binding of the C ABI in include/mpsqmc_gpu.h (libmpsqmc_b200.so).
+
+There is no CPU fallback: loading fails loudly when the library is missing, and creating an
+engine fails with MPSQMC_E_NODEVICE when no CUDA device is visible.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+OK = 0
+E_ARG, E_CUDA, E_NODEVICE, E_UNSUPPORTED, E_CAPACITY, E_NUMERIC, E_EXTINCT = -1, -2, -3, -4, -5, -6, -7
+TRACE_STRIDE = 21
+
+# Every symbol include/mpsqmc_gpu.h declares.
+EXPORTED = [
+    "mpsqmc_create", "mpsqmc_destroy", "mpsqmc_last_error", "mpsqmc_version", "mpsqmc_walker_size",
+    "mpsqmc_set_walkers", "mpsqmc_get_walkers", "mpsqmc_set_rng", "mpsqmc_get_rng_draws",
+    "mpsqmc_energy", "mpsqmc_walk", "mpsqmc_last_step_walkers", "mpsqmc_set_trace",
+    "mpsqmc_get_trace", "mpsqmc_last_timing",
+]
+
+
+class MpsqmcError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"mpsqmc error {code}: {msg}")
+        self.code = code
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("L", C.c_int), ("d", C.c_int), ("nC", C.c_int),
+        ("ci", C.POINTER(C.c_int)), ("cj", C.POINTER(C.c_int)), ("cJ", C.POINTER(C.c_double)),
+        ("h", C.c_double), ("dtau", C.c_double),
+        ("trial_dims", C.POINTER(C.c_int)), ("trial", C.POINTER(C.c_double)),
+        ("nJ", C.c_int), ("Jvals", C.POINTER(C.c_double)), ("U", C.POINTER(C.c_double)),
+        ("S", C.POINTER(C.c_double)), ("VT", C.POINTER(C.c_double)),
+        ("G", C.c_int), ("grid", C.POINTER(C.c_double)),
+        ("Ndesired", C.c_int), ("capacity", C.c_int),
+        ("walker_dims", C.POINTER(C.c_int)), ("device", C.c_int),
+    ]
+
+
+class StepStats(C.Structure):
+    _fields_ = [
+        ("step", C.c_int), ("n_walkers", C.c_int), ("n_after", C.c_int),
+        ("sum_weight", C.c_double), ("avg_weight", C.c_double), ("E_P", C.c_double),
+        ("E_T", C.c_double), ("omega", C.c_double), ("scaling", C.c_double),
+        ("draws", C.c_uint64),
+    ]
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True):
+    """Load libmpsqmc_b200.so (building it with nvcc if absent and allowed)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_build.LIB):
+        if not build_if_missing:
+            raise FileNotFoundError(f"{_build.LIB} is missing; run mpsqmc_b200.build.build()")
+        _build.build()
+    lib = C.CDLL(_build.LIB)
+    P = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    sig = {
+        "mpsqmc_create": (C.c_int, [C.POINTER(Config), C.POINTER(P)]),
+        "mpsqmc_destroy": (C.c_int, [P]),
+        "mpsqmc_last_error": (C.c_char_p, []),
+        "mpsqmc_version": (C.c_char_p, []),
+        "mpsqmc_walker_size": (C.c_long, [P]),
+        "mpsqmc_set_walkers": (C.c_int, [P, C.c_int, dp, dp, dp, dp, C.c_int]),
+        "mpsqmc_get_walkers": (C.c_int, [P, ip, dp, dp, dp, dp]),
+        "mpsqmc_set_rng": (C.c_int, [P, C.c_uint32, C.c_uint64]),
+        "mpsqmc_get_rng_draws": (C.c_int, [P, C.POINTER(C.c_uint64)]),
+        "mpsqmc_energy": (C.c_int, [P, dp]),
+        "mpsqmc_walk": (C.c_int, [P, C.c_int, C.POINTER(StepStats)]),
+        "mpsqmc_last_step_walkers": (C.c_int, [P, ip, dp, dp, dp, ip, ip]),
+        "mpsqmc_set_trace": (C.c_int, [P, C.c_int]),
+        "mpsqmc_get_trace": (C.c_int, [P, dp, ip]),
+        "mpsqmc_last_timing": (C.c_int, [P, dp, dp, ip]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int)) if a is not None else None
+
+
+def check(rc: int):
+    if rc != OK:
+        raise MpsqmcError(rc, load().mpsqmc_last_error().decode())
+    return rc
+
+
+class Engine:
+    """One device-resident walker population (an mpsqmc_ctx)."""
+
+    def __init__(self, *, L, ci, cj, cJ, h, dtau, trial_dims, trial, Jvals, U, S, VT, grid,
+                 Ndesired, capacity, walker_dims, device=0, d=2):
+        lib = load()
+        self._keep = dict(
+            ci=np.ascontiguousarray(ci, dtype=np.int32), cj=np.ascontiguousarray(cj, dtype=np.int32),
+            cJ=np.ascontiguousarray(cJ, dtype=np.float64),
+            trial_dims=np.ascontiguousarray(trial_dims, dtype=np.int32),
+            trial=np.ascontiguousarray(trial, dtype=np.float64),
+            Jvals=np.ascontiguousarray(Jvals, dtype=np.float64), U=np.ascontiguousarray(U, dtype=np.float64),
+            S=np.ascontiguousarray(S, dtype=np.float64), VT=np.ascontiguousarray(VT, dtype=np.float64),
+            grid=np.ascontiguousarray(grid, dtype=np.float64),
+            walker_dims=np.ascontiguousarray(walker_dims, dtype=np.int32))
+        k = self._keep
+        cfg = Config(L=L, d=d, nC=len(k["ci"]), ci=_ip(k["ci"]), cj=_ip(k["cj"]), cJ=_dp(k["cJ"]), h=h,
+                     dtau=dtau, trial_dims=_ip(k["trial_dims"]), trial=_dp(k["trial"]), nJ=len(k["Jvals"]),
+                     Jvals=_dp(k["Jvals"]), U=_dp(k["U"]), S=_dp(k["S"]), VT=_dp(k["VT"]),
+                     G=k["grid"].shape[0], grid=_dp(k["grid"]), Ndesired=Ndesired, capacity=capacity,
+                     walker_dims=_ip(k["walker_dims"]), device=device)
+        self._ctx = C.c_void_p()
+        check(lib.mpsqmc_create(C.byref(cfg), C.byref(self._ctx)))
+        self.lib = lib
+        self.L, self.nC, self.capacity = L, len(k["ci"]), capacity
+        self.walker_size = lib.mpsqmc_walker_size(self._ctx)
+
+    def close(self):
+        if self._ctx:
+            self.lib.mpsqmc_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_walkers(self, walkers, weights, overlaps=None, ehist=None, normalize=True):
+        w = np.ascontiguousarray(walkers, dtype=np.float64)
+        N = w.shape[0]
+        wt = np.ascontiguousarray(weights, dtype=np.float64)
+        ov = None if overlaps is None else np.ascontiguousarray(overlaps, dtype=np.float64)
+        eh = None if ehist is None else np.ascontiguousarray(ehist, dtype=np.float64)
+        check(self.lib.mpsqmc_set_walkers(self._ctx, N, _dp(w), _dp(wt), _dp(ov), _dp(eh), int(normalize)))
+
+    def get_walkers(self):
+        n = C.c_int(0)
+        check(self.lib.mpsqmc_get_walkers(self._ctx, C.byref(n), None, None, None, None))
+        N = n.value
+        w = np.zeros((N, self.walker_size))
+        wt, ov, eh = np.zeros(N), np.zeros(N), np.zeros(N)
+        check(self.lib.mpsqmc_get_walkers(self._ctx, C.byref(n), _dp(w), _dp(wt), _dp(ov), _dp(eh)))
+        return w, wt, ov, eh
+
+    def set_rng(self, seed: int, skip: int = 0):
+        check(self.lib.mpsqmc_set_rng(self._ctx, seed & 0xFFFFFFFF, skip))
+
+    def rng_draws(self) -> int:
+        v = C.c_uint64(0)
+        check(self.lib.mpsqmc_get_rng_draws(self._ctx, C.byref(v)))
+        return v.value
+
+    def energy(self) -> float:
+        e = C.c_double(0)
+        check(self.lib.mpsqmc_energy(self._ctx, C.byref(e)))
+        return e.value
+
+    def walk(self, nsteps: int):
+        st = (StepStats * max(nsteps, 1))()
+        check(self.lib.mpsqmc_walk(self._ctx, nsteps, st))
+        return [dict(step=s.step, n_walkers=s.n_walkers, n_after=s.n_after, sum_weight=s.sum_weight,
+                     avg_weight=s.avg_weight, E_P=s.E_P, E_T=s.E_T, omega=s.omega, scaling=s.scaling,
+                     draws=s.draws) for s in st[:nsteps]]
+
+    def last_step_walkers(self):
+        nb, na = C.c_int(0), C.c_int(0)
+        check(self.lib.mpsqmc_last_step_walkers(self._ctx, C.byref(nb), None, None, None, C.byref(na), None))
+        w, o, e = np.zeros(nb.value), np.zeros(nb.value), np.zeros(nb.value)
+        par = np.zeros(max(na.value, 1), dtype=np.int32)
+        check(self.lib.mpsqmc_last_step_walkers(self._ctx, C.byref(nb), _dp(w), _dp(o), _dp(e), C.byref(na),
+                                                _ip(par)))
+        return dict(weight=w, overlap=o, energy=e, parent=par[:na.value])
+
+    def set_trace(self, on: bool):
+        check(self.lib.mpsqmc_set_trace(self._ctx, int(on)))
+
+    def get_trace(self):
+        n = C.c_int(0)
+        buf = np.zeros((self.capacity, self.nC, TRACE_STRIDE))
+        check(self.lib.mpsqmc_get_trace(self._ctx, _dp(buf), C.byref(n)))
+        return buf[: n.value]
+
+    def last_timing(self):
+        k, t, n = C.c_double(0), C.c_double(0), C.c_int(0)
+        check(self.lib.mpsqmc_last_timing(self._ctx, C.byref(k), C.byref(t), C.byref(n)))
+        return dict(step_kernel_ms=k.value, total_ms=t.value, launches=n.value)

@@ -1,0 +1,571 @@
+// Host implementation of the C ABI declared in include/mpsqmc_gpu.h.
+//
+// The context owns every device buffer; walkers live in `capacity` fixed-size slots in HBM and
+// a logical->slot table gives the population order the reference's theWalkers array has
+// (MPSQMC2.h:119-123).  One call of mpsqmc_walk issues, per step, the kernels of
+// walker_kernels.cuh on one stream and reads back a small statistics record.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/mpsqmc_gpu.h"
+#include "walker_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_err = "";
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                             \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(MPSQMC_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
+  } while (0)
+
+template <typename T>
+int dalloc(T **p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess) return fail(MPSQMC_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+double op_sz(int d, int i, int j) { return (i == j) ? 0.5 * (1 - d) + i : 0.0; }
+double ladder(int d, int k) { return 0.25 * std::sqrt(d * d - 1.0 - (1.0 - d + 2 * k) * (3.0 - d + 2 * k)); }
+double op_sx(int d, int i, int j) {
+  if (i == j + 1) return ladder(d, j);
+  if (i + 1 == j) return ladder(d, i);
+  return 0.0;
+}
+double op_isy(int d, int i, int j) {
+  if (i == j + 1) return ladder(d, j);
+  if (i + 1 == j) return -ladder(d, i);
+  return 0.0;
+}
+
+bool valid_dims(const int *dims, int L, int d) {
+  if (dims[0] != 1 || dims[L] != 1) return false;
+  for (int k = 0; k < L; ++k) {
+    if (dims[k] < 1 || dims[k + 1] < 1) return false;
+    if (dims[k + 1] > d * dims[k] || dims[k] > d * dims[k + 1]) return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+struct mpsqmc_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int L = 0, d = 2, nC = 0, G = 0, nJ = 0, Ndesired = 0, capacity = 0;
+  double dtau = 0.0, h = 0.0;
+  std::vector<int> aT, bW;
+  std::vector<long> toff, woff, roff;
+  long wsize = 0, wstride = 0, scr_stride = 0, foff = 0;
+  int maxA = 1, maxB = 1, pa = 4, pb = 4, pq = 4;
+  size_t smem_bytes = 0;
+  int sm_count = 1, max_ctas = 1;
+  // device memory
+  int *d_aT = nullptr, *d_bW = nullptr;
+  long *d_toff = nullptr, *d_woff = nullptr, *d_roff = nullptr;
+  double *d_trial = nullptr, *d_walkers = nullptr;
+  int *d_slot_of = nullptr, *d_slot_new = nullptr, *d_free = nullptr, *d_copy_src = nullptr,
+      *d_copy_dst = nullptr, *d_parent = nullptr, *d_flag_pos = nullptr, *d_ncur = nullptr;
+  double *d_weight = nullptr, *d_overlap = nullptr, *d_ehist = nullptr, *d_energy = nullptr,
+         *d_ovout = nullptr, *d_wtout = nullptr, *d_sw = nullptr, *d_uni = nullptr, *d_ubr = nullptr;
+  int *d_bond_c = nullptr, *d_bond_j = nullptr;
+  double *d_bondJ = nullptr, *d_tabU = nullptr, *d_tabS = nullptr, *d_tabVT = nullptr, *d_grid = nullptr;
+  double *d_scratch = nullptr, *d_trace = nullptr;
+  int *d_err = nullptr;
+  mq::MtState *d_mt = nullptr;
+  mq::StepDev *d_sd = nullptr;
+  bool trace_on = false;
+  int n_cur = 0, step_count = 0, last_n_before = 0, last_n_after = 0;
+  unsigned long long draws = 0;
+  double last_kernel_ms = 0.0, last_total_ms = 0.0;
+  int last_launches = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  double opSx[4], opISy[4], opSz[4];
+};
+
+namespace {
+
+mq::Dev make_dev(mpsqmc_ctx *c) {
+  mq::Dev p;
+  std::memset(&p, 0, sizeof p);
+  p.L = c->L;
+  p.d = c->d;
+  p.nC = c->nC;
+  p.G = c->G;
+  p.nJ = c->nJ;
+  p.maxA = c->maxA;
+  p.maxB = c->maxB;
+  p.pa = c->pa;
+  p.pb = c->pb;
+  p.pq = c->pq;
+  p.aT = c->d_aT;
+  p.bW = c->d_bW;
+  p.toff = c->d_toff;
+  p.woff = c->d_woff;
+  p.trial = c->d_trial;
+  p.wstride = c->wstride;
+  p.walkers = c->d_walkers;
+  p.slot_of = c->d_slot_of;
+  p.n_cur = c->d_ncur;
+  p.weight = c->d_weight;
+  p.overlap = c->d_overlap;
+  p.ehist = c->d_ehist;
+  p.energy = c->d_energy;
+  p.ov_out = c->d_ovout;
+  p.wt_out = c->d_wtout;
+  p.uni = c->d_uni;
+  p.bond_c = c->d_bond_c;
+  p.bond_j = c->d_bond_j;
+  p.bondJ = c->d_bondJ;
+  p.tabU = c->d_tabU;
+  p.tabS = c->d_tabS;
+  p.tabVT = c->d_tabVT;
+  p.grid = c->d_grid;
+  for (int k = 0; k < 4; ++k) {
+    p.opSx[k] = c->opSx[k];
+    p.opISy[k] = c->opISy[k];
+    p.opSz[k] = c->opSz[k];
+  }
+  p.h = c->h;
+  p.scratch = c->d_scratch;
+  p.scr_stride = c->scr_stride;
+  p.roff = c->d_roff;
+  p.foff = c->foff;
+  p.trace = c->trace_on ? c->d_trace : nullptr;
+  p.err = c->d_err;
+  return p;
+}
+
+int grid_for(const mpsqmc_ctx *c, int n) { return std::max(1, std::min(n, c->max_ctas)); }
+
+int check_err(mpsqmc_ctx *c) {
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (e & mq::kErrCapacity)
+    return fail(MPSQMC_E_CAPACITY, "population control exceeded the walker capacity");
+  if (e & mq::kErrNumeric) return fail(MPSQMC_E_NUMERIC, "non-finite weight, overlap or energy");
+  return 0;
+}
+
+void free_all(mpsqmc_ctx *c) {
+  void *ptrs[] = {c->d_aT, c->d_bW, c->d_toff, c->d_woff, c->d_roff, c->d_trial, c->d_walkers,
+                  c->d_slot_of, c->d_slot_new, c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
+                  c->d_flag_pos, c->d_ncur, c->d_weight, c->d_overlap, c->d_ehist, c->d_energy,
+                  c->d_ovout, c->d_wtout, c->d_sw, c->d_uni, c->d_ubr, c->d_bond_c, c->d_bond_j,
+                  c->d_bondJ, c->d_tabU, c->d_tabS, c->d_tabVT, c->d_grid, c->d_scratch, c->d_trace,
+                  c->d_err, c->d_mt, c->d_sd};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *mpsqmc_last_error(void) { return g_err.c_str(); }
+
+const char *mpsqmc_version(void) { return "mpsqmc_b200 0.1 (sm_100a, fp64 dmma)"; }
+
+long mpsqmc_walker_size(const mpsqmc_ctx *ctx) { return ctx ? ctx->wsize : -1; }
+
+int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
+  if (!cfg || !out) return fail(MPSQMC_E_ARG, "null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(MPSQMC_E_NODEVICE, "no CUDA device visible; the engine has no CPU fallback");
+  if (cfg->device < 0 || cfg->device >= ndev) return fail(MPSQMC_E_ARG, "device ordinal out of range");
+  if (cfg->d != mq::kMaxD) return fail(MPSQMC_E_UNSUPPORTED, "only d = 2 (spin 1/2) is implemented");
+  const int L = cfg->L, d = cfg->d;
+  if (L < 3) return fail(MPSQMC_E_ARG, "L must be >= 3 (HeisenbergMPO.cpp:10)");
+  if (cfg->nC < 1 || !cfg->ci || !cfg->cj || !cfg->cJ) return fail(MPSQMC_E_ARG, "no couplings");
+  if (cfg->G < 1 || !cfg->grid) return fail(MPSQMC_E_ARG, "empty grid");
+  if (cfg->nJ < 1 || !cfg->Jvals || !cfg->U || !cfg->S || !cfg->VT)
+    return fail(MPSQMC_E_ARG, "missing Trotter tables");
+  if (cfg->capacity < 1 || cfg->Ndesired < 1) return fail(MPSQMC_E_ARG, "bad walker counts");
+  if (!cfg->trial_dims || !cfg->trial || !cfg->walker_dims) return fail(MPSQMC_E_ARG, "missing MPS data");
+  if (!valid_dims(cfg->trial_dims, L, d) || !valid_dims(cfg->walker_dims, L, d))
+    return fail(MPSQMC_E_ARG, "bond dimensions inconsistent with the chain");
+  std::vector<int> bond_c(L - 1, -1), bond_j(L - 1, -1);
+  std::vector<double> bondJ(L - 1, 0.0);
+  for (int c = 0; c < cfg->nC; ++c) {
+    const int i = cfg->ci[c], j = cfg->cj[c];
+    if (i < 0 || j >= L || i >= j) return fail(MPSQMC_E_ARG, "coupling indices out of order");
+    if (j != i + 1)
+      return fail(MPSQMC_E_UNSUPPORTED, "only nearest-neighbour chain couplings are implemented");
+    if (bond_c[i] >= 0) return fail(MPSQMC_E_ARG, "duplicate coupling");
+    if (c > 0 && cfg->ci[c - 1] >= i) return fail(MPSQMC_E_ARG, "couplings must be ordered by site");
+    int q = -1;
+    for (int t = 0; t < cfg->nJ; ++t)
+      if (cfg->Jvals[t] == cfg->cJ[c]) {
+        q = t;
+        break;
+      }
+    if (q < 0) return fail(MPSQMC_E_ARG, "coupling strength without Trotter tables");
+    bond_c[i] = c;
+    bond_j[i] = q;
+    bondJ[i] = cfg->cJ[c];
+  }
+
+  mpsqmc_ctx *c = new mpsqmc_ctx();
+  c->device = cfg->device;
+  if (cudaSetDevice(c->device) != cudaSuccess) {
+    delete c;
+    return fail(MPSQMC_E_CUDA, "cudaSetDevice failed");
+  }
+  c->L = L;
+  c->d = d;
+  c->nC = cfg->nC;
+  c->G = cfg->G;
+  c->nJ = cfg->nJ;
+  c->Ndesired = cfg->Ndesired;
+  c->capacity = cfg->capacity;
+  c->dtau = cfg->dtau;
+  c->h = cfg->h;
+  c->aT.assign(cfg->trial_dims, cfg->trial_dims + L + 1);
+  c->bW.assign(cfg->walker_dims, cfg->walker_dims + L + 1);
+  c->toff.resize(L);
+  c->woff.resize(L);
+  long to = 0, wo = 0;
+  for (int k = 0; k < L; ++k) {
+    c->toff[k] = to;
+    c->woff[k] = wo;
+    to += (long)c->aT[k] * c->aT[k + 1] * d;
+    wo += (long)c->bW[k] * c->bW[k + 1] * d;
+  }
+  c->wsize = wo;
+  c->wstride = (wo + 31) & ~31L;
+  c->maxA = *std::max_element(c->aT.begin(), c->aT.end());
+  c->maxB = *std::max_element(c->bW.begin(), c->bW.end());
+  c->pa = mq::padld(c->maxA);
+  c->pb = mq::padld(c->maxB);
+  c->pq = mq::padld(d * c->maxB);
+  c->smem_bytes = sizeof(double) * (size_t)mq::smem_doubles(c->maxA, c->maxB, c->G, c->pa, c->pb, c->pq,
+                                                            nullptr, nullptr);
+  c->roff.resize(L + 1);
+  long ro = 0;
+  for (int k = 0; k <= L; ++k) {
+    c->roff[k] = ro;
+    ro += ((long)c->aT[k] * c->bW[k] + 3) & ~3L;
+  }
+  c->foff = ro;
+  c->scr_stride = ro + 2L * 4 * c->maxA * c->maxB;
+  c->scr_stride = (c->scr_stride + 31) & ~31L;
+  for (int s = 0; s < 2; ++s)
+    for (int t = 0; t < 2; ++t) {
+      c->opSx[s + 2 * t] = op_sx(d, s, t);
+      c->opISy[s + 2 * t] = op_isy(d, s, t);
+      c->opSz[s + 2 * t] = op_sz(d, s, t);
+    }
+
+  auto bail = [&](int code) {
+    free_all(c);
+    delete c;
+    return code;
+  };
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) return bail(fail(MPSQMC_E_CUDA, "properties"));
+  if (c->smem_bytes > (size_t)prop.sharedMemPerBlockOptin)
+    return bail(fail(MPSQMC_E_UNSUPPORTED, "bond dimensions exceed the shared-memory budget of one CTA"));
+  c->sm_count = prop.multiProcessorCount;
+  if (cudaFuncSetAttribute(mq::walker_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)c->smem_bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(mq::set_overlap_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)c->smem_bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(mq::energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)c->smem_bytes) != cudaSuccess)
+    return bail(fail(MPSQMC_E_CUDA, "cudaFuncSetAttribute failed"));
+  int occ = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mq::walker_step_kernel, mq::kThreads, c->smem_bytes);
+  c->max_ctas = std::max(1, occ) * c->sm_count;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(MPSQMC_E_CUDA, "stream"));
+  for (auto &e : c->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return bail(fail(MPSQMC_E_CUDA, "event"));
+  const int cap = c->capacity;
+  int rc = 0;
+  rc |= dalloc(&c->d_aT, L + 1) | dalloc(&c->d_bW, L + 1) | dalloc(&c->d_toff, L) | dalloc(&c->d_woff, L) |
+        dalloc(&c->d_roff, L + 1) | dalloc(&c->d_trial, to) | dalloc(&c->d_walkers, (size_t)cap * c->wstride) |
+        dalloc(&c->d_slot_of, cap) | dalloc(&c->d_slot_new, cap) | dalloc(&c->d_free, cap) |
+        dalloc(&c->d_copy_src, cap) | dalloc(&c->d_copy_dst, cap) | dalloc(&c->d_parent, cap) |
+        dalloc(&c->d_flag_pos, cap) | dalloc(&c->d_ncur, 1) | dalloc(&c->d_weight, cap) |
+        dalloc(&c->d_overlap, cap) | dalloc(&c->d_ehist, cap) | dalloc(&c->d_energy, cap) |
+        dalloc(&c->d_ovout, cap) | dalloc(&c->d_wtout, cap) | dalloc(&c->d_sw, cap) |
+        dalloc(&c->d_uni, (size_t)cap * c->nC) | dalloc(&c->d_ubr, cap) | dalloc(&c->d_bond_c, L - 1) |
+        dalloc(&c->d_bond_j, L - 1) | dalloc(&c->d_bondJ, L - 1) | dalloc(&c->d_tabU, 16 * c->nJ) |
+        dalloc(&c->d_tabS, 4 * c->nJ) | dalloc(&c->d_tabVT, 16 * c->nJ) | dalloc(&c->d_grid, 4 * c->G) |
+        dalloc(&c->d_scratch, (size_t)c->max_ctas * c->scr_stride) | dalloc(&c->d_err, 1) |
+        dalloc(&c->d_mt, 1) | dalloc(&c->d_sd, 1);
+  if (rc) return bail(MPSQMC_E_CUDA);
+  auto up = [&](void *dst, const void *src, size_t bytes) {
+    return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+  };
+  bool ok = up(c->d_aT, c->aT.data(), sizeof(int) * (L + 1)) && up(c->d_bW, c->bW.data(), sizeof(int) * (L + 1)) &&
+            up(c->d_toff, c->toff.data(), sizeof(long) * L) && up(c->d_woff, c->woff.data(), sizeof(long) * L) &&
+            up(c->d_roff, c->roff.data(), sizeof(long) * (L + 1)) &&
+            up(c->d_trial, cfg->trial, sizeof(double) * to) &&
+            up(c->d_bond_c, bond_c.data(), sizeof(int) * (L - 1)) &&
+            up(c->d_bond_j, bond_j.data(), sizeof(int) * (L - 1)) &&
+            up(c->d_bondJ, bondJ.data(), sizeof(double) * (L - 1)) &&
+            up(c->d_tabU, cfg->U, sizeof(double) * 16 * c->nJ) && up(c->d_tabS, cfg->S, sizeof(double) * 4 * c->nJ) &&
+            up(c->d_tabVT, cfg->VT, sizeof(double) * 16 * c->nJ) && up(c->d_grid, cfg->grid, sizeof(double) * 4 * c->G);
+  if (!ok) return bail(fail(MPSQMC_E_CUDA, "upload failed"));
+  if (cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess || cudaMemset(c->d_sd, 0, sizeof(mq::StepDev)) != cudaSuccess ||
+      cudaMemset(c->d_ncur, 0, sizeof(int)) != cudaSuccess)
+    return bail(fail(MPSQMC_E_CUDA, "memset failed"));
+  *out = c;
+  // default stream position: seed 5489 (std::mt19937 default), nothing skipped
+  return mpsqmc_set_rng(c, 5489u, 0);
+}
+
+int mpsqmc_destroy(mpsqmc_ctx *ctx) {
+  if (!ctx) return 0;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_all(ctx);
+  delete ctx;
+  return 0;
+}
+
+int mpsqmc_set_rng(mpsqmc_ctx *c, uint32_t seed, uint64_t skip) {
+  if (!c) return fail(MPSQMC_E_ARG, "null context");
+  std::mt19937 gen(seed);
+  gen.discard(skip);
+  std::stringstream ss;
+  ss << gen;  // 624 state words followed by the position
+  mq::MtState st;
+  std::memset(&st, 0, sizeof st);
+  for (int q = 0; q < 624; ++q) {
+    unsigned long v;
+    ss >> v;
+    st.mt[q] = (uint32_t)v;
+  }
+  ss >> st.idx;
+  st.draws = 0;
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(c->d_mt, &st, sizeof st, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->draws = 0;
+  return 0;
+}
+
+int mpsqmc_get_rng_draws(mpsqmc_ctx *c, uint64_t *draws) {
+  if (!c || !draws) return fail(MPSQMC_E_ARG, "null argument");
+  mq::MtState st;
+  CK(cudaMemcpy(&st, c->d_mt, sizeof st, cudaMemcpyDeviceToHost));
+  *draws = st.draws;
+  return 0;
+}
+
+int mpsqmc_set_walkers(mpsqmc_ctx *c, int N, const double *walkers, const double *weights,
+                       const double *overlaps, const double *ehist, int normalize) {
+  if (!c || !walkers || !weights) return fail(MPSQMC_E_ARG, "null argument");
+  if (N < 1 || N > c->capacity) return fail(MPSQMC_E_ARG, "walker count outside [1, capacity]");
+  CK(cudaSetDevice(c->device));
+  for (int w = 0; w < N; ++w)
+    CK(cudaMemcpyAsync(c->d_walkers + (size_t)w * c->wstride, walkers + (size_t)w * c->wsize,
+                       sizeof(double) * c->wsize, cudaMemcpyHostToDevice, c->stream));
+  std::vector<int> slots(N), freel(c->capacity - N);
+  for (int w = 0; w < N; ++w) slots[w] = w;
+  for (int q = 0; q < c->capacity - N; ++q) freel[q] = c->capacity - 1 - q;
+  std::vector<double> zeros(N, 0.0), ones(N, 1.0);
+  CK(cudaMemcpyAsync(c->d_slot_of, slots.data(), sizeof(int) * N, cudaMemcpyHostToDevice, c->stream));
+  if (!freel.empty())
+    CK(cudaMemcpyAsync(c->d_free, freel.data(), sizeof(int) * freel.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_weight, weights, sizeof(double) * N, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_overlap, overlaps ? overlaps : ones.data(), sizeof(double) * N,
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_ehist, ehist ? ehist : zeros.data(), sizeof(double) * N, cudaMemcpyHostToDevice,
+                     c->stream));
+  mq::StepDev sd;
+  std::memset(&sd, 0, sizeof sd);
+  sd.n_cur = N;
+  sd.n_free = c->capacity - N;
+  CK(cudaMemcpyAsync(c->d_sd, &sd, sizeof sd, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_ncur, &N, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+  c->n_cur = N;
+  if (normalize) {
+    mq::Dev p = make_dev(c);
+    mq::set_overlap_kernel<<<grid_for(c, N), mq::kThreads, c->smem_bytes, c->stream>>>(p);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return check_err(c);
+}
+
+int mpsqmc_get_walkers(mpsqmc_ctx *c, int *N, double *walkers, double *weights, double *overlaps,
+                       double *ehist) {
+  if (!c) return fail(MPSQMC_E_ARG, "null context");
+  CK(cudaSetDevice(c->device));
+  const int n = c->n_cur;
+  if (N) *N = n;
+  std::vector<int> slots(n);
+  CK(cudaMemcpy(slots.data(), c->d_slot_of, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  std::vector<double> buf(c->capacity);
+  auto gather = [&](double *dst, const double *src) -> int {
+    if (!dst) return 0;
+    CK(cudaMemcpy(buf.data(), src, sizeof(double) * c->capacity, cudaMemcpyDeviceToHost));
+    for (int w = 0; w < n; ++w) dst[w] = buf[slots[w]];
+    return 0;
+  };
+  int rc = gather(weights, c->d_weight) | gather(overlaps, c->d_overlap) | gather(ehist, c->d_ehist);
+  if (rc) return rc;
+  if (walkers)
+    for (int w = 0; w < n; ++w)
+      CK(cudaMemcpy(walkers + (size_t)w * c->wsize, c->d_walkers + (size_t)slots[w] * c->wstride,
+                    sizeof(double) * c->wsize, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int mpsqmc_energy(mpsqmc_ctx *c, double *E_P) {
+  if (!c || !E_P) return fail(MPSQMC_E_ARG, "null argument");
+  if (c->n_cur < 1) return fail(MPSQMC_E_ARG, "no walkers");
+  CK(cudaSetDevice(c->device));
+  mq::Dev p = make_dev(c);
+  mq::energy_kernel<<<grid_for(c, c->n_cur), mq::kThreads, c->smem_bytes, c->stream>>>(p);
+  CK(cudaGetLastError());
+  mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 1, 0, c->d_flag_pos, c->d_sw);
+  CK(cudaGetLastError());
+  mq::StepDev sd;
+  CK(cudaMemcpyAsync(&sd, c->d_sd, sizeof sd, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int rc = check_err(c);
+  if (rc) return rc;
+  *E_P = sd.EP;
+  return 0;
+}
+
+int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
+  if (!c) return fail(MPSQMC_E_ARG, "null context");
+  if (nsteps < 0) return fail(MPSQMC_E_ARG, "negative step count");
+  if (c->n_cur < 1) return fail(MPSQMC_E_ARG, "no walkers");
+  CK(cudaSetDevice(c->device));
+  if (c->trace_on && !c->d_trace) {
+    if (dalloc(&c->d_trace, (size_t)c->capacity * c->nC * mq::kTraceStride)) return MPSQMC_E_CUDA;
+  }
+  double kernel_ms = 0.0;
+  int launches = 0;
+  CK(cudaEventRecord(c->ev[2], c->stream));
+  for (int s = 0; s < nsteps; ++s) {
+    const int N = c->n_cur;
+    const int step = ++c->step_count;
+    mq::Dev p = make_dev(c);
+    mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, c->d_ncur, 0, c->nC, c->d_uni);
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    mq::walker_step_kernel<<<grid_for(c, N), mq::kThreads, c->smem_bytes, c->stream>>>(p);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, step, 1, c->d_flag_pos, c->d_sw);
+    mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, &c->d_sd->n_flag, 0, 1, c->d_ubr);
+    mq::branch_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->d_flag_pos, c->d_sw, c->d_ubr, c->d_slot_new,
+                                                 c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
+                                                 c->capacity);
+    mq::copy_walkers_kernel<<<std::min(N * 4, 4 * c->sm_count), 256, 0, c->stream>>>(p, c->d_sd, c->d_copy_src,
+                                                                                     c->d_copy_dst);
+    mq::finish_branch_kernel<<<1, 1024, 0, c->stream>>>(c->d_sd, c->d_ncur, c->d_slot_of, c->d_slot_new, c->d_err,
+                                                        c->capacity);
+    CK(cudaGetLastError());
+    launches += 7;
+    mq::StepDev sd;
+    int err = 0;
+    CK(cudaMemcpyAsync(&sd, c->d_sd, sizeof sd, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&err, c->d_err, sizeof err, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+    kernel_ms += ms;
+    if (err & mq::kErrNumeric) return fail(MPSQMC_E_NUMERIC, "non-finite weight, overlap or energy");
+    if (err & mq::kErrCapacity) return fail(MPSQMC_E_CAPACITY, "population control exceeded the walker capacity");
+    const unsigned long long dr = (unsigned long long)N * c->nC + (unsigned long long)sd.n_flag;
+    c->draws += dr;
+    c->last_n_before = N;
+    c->last_n_after = sd.n_new;
+    c->n_cur = sd.n_new;
+    if (stats) {
+      mpsqmc_step_stats &o = stats[s];
+      o.step = step;
+      o.n_walkers = N;
+      o.n_after = sd.n_new;
+      o.sum_weight = sd.sumw;
+      o.avg_weight = sd.sumw / N;
+      o.E_P = sd.EP;
+      o.E_T = sd.ET;
+      o.omega = sd.omega;
+      o.scaling = sd.scaling;
+      o.draws = dr;
+    }
+    if (sd.n_new == 0) return fail(MPSQMC_E_EXTINCT, "population control removed every walker");
+  }
+  CK(cudaEventRecord(c->ev[3], c->stream));
+  CK(cudaEventSynchronize(c->ev[3]));
+  float tot = 0.f;
+  CK(cudaEventElapsedTime(&tot, c->ev[2], c->ev[3]));
+  c->last_kernel_ms = kernel_ms;
+  c->last_total_ms = tot;
+  c->last_launches = launches;
+  return 0;
+}
+
+int mpsqmc_last_step_walkers(mpsqmc_ctx *c, int *n_before, double *weight, double *overlap,
+                             double *energy, int *n_after, int *parent) {
+  if (!c) return fail(MPSQMC_E_ARG, "null context");
+  CK(cudaSetDevice(c->device));
+  const int nb = c->last_n_before, na = c->last_n_after;
+  if (n_before) *n_before = nb;
+  if (n_after) *n_after = na;
+  if (weight && nb) CK(cudaMemcpy(weight, c->d_wtout, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  if (overlap && nb) CK(cudaMemcpy(overlap, c->d_ovout, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  if (energy && nb) CK(cudaMemcpy(energy, c->d_energy, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  if (parent && na) CK(cudaMemcpy(parent, c->d_parent, sizeof(int) * na, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int mpsqmc_set_trace(mpsqmc_ctx *c, int enable) {
+  if (!c) return fail(MPSQMC_E_ARG, "null context");
+  c->trace_on = enable != 0;
+  return 0;
+}
+
+int mpsqmc_get_trace(mpsqmc_ctx *c, double *trace, int *n_walkers) {
+  if (!c || !trace) return fail(MPSQMC_E_ARG, "null argument");
+  if (!c->d_trace) return fail(MPSQMC_E_ARG, "trace was not enabled for a step");
+  CK(cudaSetDevice(c->device));
+  const int nb = c->last_n_before;
+  if (n_walkers) *n_walkers = nb;
+  CK(cudaMemcpy(trace, c->d_trace, sizeof(double) * (size_t)nb * c->nC * mq::kTraceStride,
+                cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int mpsqmc_last_timing(mpsqmc_ctx *c, double *step_kernel_ms, double *total_ms, int *kernel_launches) {
+  if (!c) return fail(MPSQMC_E_ARG, "null context");
+  if (step_kernel_ms) *step_kernel_ms = c->last_kernel_ms;
+  if (total_ms) *total_ms = c->last_total_ms;
+  if (kernel_launches) *kernel_launches = c->last_launches;
+  return 0;
+}
+
+}  // extern "C"

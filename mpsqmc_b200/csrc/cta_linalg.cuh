@@ -1,0 +1,207 @@
+// CTA-cooperative FP64 dense linear algebra for the walker kernels (sm_100a).
+//
+// All matrices are column-major with an explicit leading dimension and may live in shared or
+// global memory (generic pointers).  Every routine is called by all threads of the CTA and
+// returns without a trailing barrier unless stated; callers place __syncthreads() between
+// dependent calls.
+//
+// FP64 products use the tensor-core DMMA instruction mma.sync.m8n8k4.f64 (tcgen05 has no f64
+// kind, so this is Blackwell's FP64 tensor path).  Fragment layouts follow the PTX ISA for
+// .f64 m8n8k4: A (8x4, row): lane holds A[lane>>2][lane&3]; B (4x8, col): B[lane&3][lane>>2];
+// C/D (8x8): C[lane>>2][2*(lane&3) + i], i = 0,1.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mq {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+__device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+// C (M x N, ldc) = alpha * op(A) * op(B) + beta * C, op(A) M x K, op(B) K x N.
+//   ta == false: A[m + lda*k];  ta == true: A[k + lda*m]
+//   tb == false: B[k + ldb*n];  tb == true: B[n + ldb*k]
+// Each warp owns 16x16 output blocks (2x2 DMMA tiles); element bounds are checked, so any
+// M, N, K >= 0 is valid.  Output element (m, n) is always written by the same thread for a
+// given (M, N), so two calls with the same M, N may accumulate into C without a barrier.
+__device__ __noinline__ void cta_gemm(int M, int N, int K, double alpha, const double *A, int lda,
+                                      bool ta, const double *B, int ldb, bool tb, double beta,
+                                      double *C, int ldc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int bm = (M + 15) >> 4, bn = (N + 15) >> 4;
+  for (int blk = warp; blk < bm * bn; blk += kWarps) {
+    const int m0 = (blk % bm) << 4, n0 = (blk / bm) << 4;
+    double acc[2][2][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    const int ma = m0 + g, mb = m0 + 8 + g;
+    const int na = n0 + g, nb = n0 + 8 + g;
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      const int k = k0 + t;
+      const bool kin = k < K;
+      double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+      if (kin) {
+        if (ma < M) a0 = ta ? A[k + (long)lda * ma] : A[ma + (long)lda * k];
+        if (mb < M) a1 = ta ? A[k + (long)lda * mb] : A[mb + (long)lda * k];
+        if (na < N) b0 = tb ? B[na + (long)ldb * k] : B[k + (long)ldb * na];
+        if (nb < N) b1 = tb ? B[nb + (long)ldb * k] : B[k + (long)ldb * nb];
+      }
+      dmma884(acc[0][0][0], acc[0][0][1], a0, b0);
+      dmma884(acc[0][1][0], acc[0][1][1], a0, b1);
+      dmma884(acc[1][0][0], acc[1][0][1], a1, b0);
+      dmma884(acc[1][1][0], acc[1][1][1], a1, b1);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int m = m0 + 8 * i + g, n = n0 + 8 * j + 2 * t + e;
+          if (m < M && n < N) {
+            double *c = C + m + (long)ldc * n;
+            const double v = alpha * acc[i][j][e];
+            *c = (beta == 0.0) ? v : v + beta * (*c);
+          }
+        }
+  }
+}
+
+// Sum of v over the CTA; result returned to every thread.  red: >= kWarps doubles of smem.
+__device__ __forceinline__ double cta_sum(double v, double *red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) s += red[w];
+  return s;
+}
+
+// Four sums at once (one pair of barriers).  red: >= 4*kWarps doubles.
+__device__ __forceinline__ void cta_sum4(double v[4], double *red) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) red[q * kWarps + warp] = v[q];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    double s = 0.0;
+    for (int w = 0; w < kWarps; ++w) s += red[q * kWarps + w];
+    v[q] = s;
+  }
+}
+
+__device__ __forceinline__ double dlapy2(double x, double y) {
+  const double xa = fabs(x), ya = fabs(y);
+  const double w = fmax(xa, ya), z = fmin(xa, ya);
+  if (z == 0.0) return w;
+  const double r = z / w;
+  return w * sqrt(1.0 + r * r);
+}
+
+// Householder QR of A (m x n, m >= n, ld lda, shared memory) in LAPACK's conventions
+// (dgeqr2 + dorg2r, with dlarfg's beta = -sign(alpha)*||x||, tau = 0 when the column below the
+// diagonal is zero or m - i == 1).  On exit A holds Q (m x n, orthonormal columns) and R
+// (n x n, ld ldr, upper triangular) holds the triangular factor.  tau, w: >= n doubles of
+// shared memory, red: >= kWarps doubles.  Ends with a barrier.
+__device__ __noinline__ void cta_householder_qr(int m, int n, double *A, int lda, double *R, int ldr,
+                                                double *tau, double *w, double *red) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  __shared__ double s_scale;
+  for (int i = 0; i < n; ++i) {
+    double *col = A + (long)lda * i;
+    double part = 0.0;
+    for (int r = i + 1 + tid; r < m; r += kThreads) part += col[r] * col[r];
+    const double ss = cta_sum(part, red);
+    if (tid == 0) {
+      double ti = 0.0, sc = 1.0;
+      if (m - i > 1 && ss > 0.0) {
+        const double alpha = col[i];
+        const double mag = dlapy2(alpha, sqrt(ss));
+        const double beta = (alpha >= 0.0) ? -mag : mag;
+        ti = (beta - alpha) / beta;
+        sc = 1.0 / (alpha - beta);
+        col[i] = beta;
+      }
+      tau[i] = ti;
+      s_scale = sc;
+    }
+    __syncthreads();
+    const double ti = tau[i];
+    if (ti != 0.0) {
+      const double sc = s_scale;
+      for (int r = i + 1 + tid; r < m; r += kThreads) col[r] *= sc;
+      __syncthreads();
+      // w_j = v^T A(i:m, j), v = (1, col[i+1..m))
+      for (int j = i + 1 + warp; j < n; j += kWarps) {
+        const double *cj = A + (long)lda * j;
+        double s = 0.0;
+        for (int r = i + 1 + lane; r < m; r += 32) s += col[r] * cj[r];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) w[j] = s + cj[i];
+      }
+      __syncthreads();
+      const int rows = m - i, cols = n - i - 1;
+      for (int q = tid; q < rows * cols; q += kThreads) {
+        const int r = i + q % rows, j = i + 1 + q / rows;
+        const double v = (r == i) ? 1.0 : col[r];
+        A[r + (long)lda * j] -= ti * v * w[j];
+      }
+    }
+    __syncthreads();
+  }
+  for (int q = tid; q < n * n; q += kThreads) {
+    const int r = q % n, c = q / n;
+    R[r + (long)ldr * c] = (r <= c) ? A[r + (long)lda * c] : 0.0;
+  }
+  __syncthreads();
+  // dorg2r, k = n
+  for (int i = n - 1; i >= 0; --i) {
+    double *col = A + (long)lda * i;
+    const double ti = tau[i];
+    if (i < n - 1 && ti != 0.0) {
+      for (int j = i + 1 + warp; j < n; j += kWarps) {
+        const double *cj = A + (long)lda * j;
+        double s = 0.0;
+        for (int r = i + 1 + lane; r < m; r += 32) s += col[r] * cj[r];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) w[j] = s + cj[i];
+      }
+      __syncthreads();
+      const int rows = m - i, cols = n - i - 1;
+      for (int q = tid; q < rows * cols; q += kThreads) {
+        const int r = i + q % rows, j = i + 1 + q / rows;
+        const double v = (r == i) ? 1.0 : col[r];
+        A[r + (long)lda * j] -= ti * v * w[j];
+      }
+      __syncthreads();
+    }
+    for (int r = tid; r < m; r += kThreads) {
+      if (r > i) col[r] *= -ti;
+      else if (r == i) col[r] = 1.0 - ti;
+      else col[r] = 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace mq

@@ -1,0 +1,864 @@
+// Walker-propagation kernels (sm_100a, FP64).
+//
+// One CTA owns one walker at a time (persistent grid striding over walkers) and runs the whole
+// timestep of MPSQMC2::PropagateSeparately (MPSQMC2.cpp:518-611) for it:
+//
+//   phase A  right sweep (LQ, site L-1 .. 1): right-canonical form with the orthogonality centre
+//            on site 0, right environments R[k] = <Psi_T|phi> contracted over sites k..L-1,
+//            overlap and sign fix (Walker::setOverlap, Walker.cpp:54-66, at MPSQMC2.cpp:534);
+//   phase B  left-to-right sweep over the bonds.  For a bond (i, i+1) that carries a coupling:
+//            the 16 numbers C_kl = <Psi_T|(sqrt(s_k)U_k)_i (sqrt(s_l)V_l)_j|phi> from the left
+//            environment, 4 left branches, 4 right branches and 16 closures (the reference gets
+//            them from 16 full-chain InnerProducts against stored trial copies, 540-549); the
+//            grid PDF, weight update and CDF sample (551-588); the auxiliary-field site
+//            operators (MPSstate.cpp:575-633); renormalisation and new overlap (592).  The centre
+//            then moves to i+1 by one Householder QR.  Compact-MPO left environments built from
+//            the final site tensors give <Psi_T|H|phi> at the end of the sweep, i.e. the local
+//            energy of Walker::calcIndividualProjectedEnergy (Walker.cpp:72-77).
+//
+// Between steps each walker is left-canonical with a normalised centre on site L-1, which is
+// the state Walker::setOverlap leaves behind.  Gauge differs from the reference's after the
+// first coupling (orthogonal transformations on the bonds); every quantity the walk uses
+// (C_kl, PDF, weights, overlaps, energies) is gauge invariant.
+#pragma once
+
+#include "cta_linalg.cuh"
+
+namespace mq {
+
+constexpr int kMaxD = 2;  // local dimension implemented by the kernels
+constexpr int kN2 = kMaxD * kMaxD;
+constexpr int kTraceStride = kN2 * kN2 + 5;
+
+struct Dev {
+  int L, d, nC, G, nJ;
+  int maxA, maxB;   // largest trial / walker bond dimension
+  int pa, pb, pq;   // padded shared-memory leading dimensions
+  const int *aT;    // trial bond dims [L+1]
+  const int *bW;    // walker bond dims [L+1]
+  const long *toff; // trial site offsets [L]
+  const long *woff; // walker site offsets [L]
+  const double *trial;
+  long wstride;     // doubles per walker slot
+  double *walkers;
+  const int *slot_of;  // logical walker -> slot
+  const int *n_cur;    // current number of walkers (device scalar)
+  double *weight, *overlap, *ehist;  // per slot
+  double *energy;      // per logical walker (last step)
+  double *ov_out;      // per logical walker (last step)
+  double *wt_out;      // per logical walker (last step)
+  const double *uni;   // propagation uniforms [N][nC], logical order
+  const int *bond_c;   // coupling index of bond (i, i+1), or -1  [L-1]
+  const int *bond_j;   // distinct-J index of the bond's coupling      [L-1]
+  const double *bondJ; // coupling strength of bond (i, i+1) or 0     [L-1]
+  const double *tabU, *tabS, *tabVT;  // [nJ][16], [nJ][4], [nJ][16]
+  const double *grid;  // [G][4]
+  double opSx[4], opISy[4], opSz[4];  // [sigma + d*tau]
+  double h;
+  double *scratch;     // per-CTA global scratch
+  long scr_stride;
+  const long *roff;    // right-environment offsets [L+1] inside a CTA's scratch
+  long foff;           // compact-MPO environments (2 x 4 x maxA*maxB) inside the scratch
+  double *trace;       // optional [N][nC][kTraceStride]
+  int *err;            // device error word (bit flags)
+};
+
+enum : int { kErrNumeric = 1, kErrCapacity = 2 };
+
+__host__ __device__ inline int padld(int x) {
+  int p = (x + 3) & ~3;
+  if ((p & 7) == 0) p += 4;
+  return p;
+}
+
+struct Smem {
+  double *Lenv, *Cen, *Nxt, *Xb, *Pb, *Qt, *QRb, *Rf, *red, *tau, *wv, *M, *Cm, *O1, *O2, *pdf, *sc;
+  int sbC, sbX;  // sigma-block strides of Cen/Nxt and of Xb/Pb
+};
+
+__host__ __device__ inline long smem_doubles(int maxA, int maxB, int G, int pa, int pb, int pq,
+                                              Smem *s, double *base) {
+  long off = 0;
+  auto take = [&](double *&p, long n) {
+    if (s) p = base + off;
+    off += (n + 3) & ~3L;
+  };
+  double *dummy;
+  const int d = kMaxD;
+  take(s ? s->Lenv : dummy, (long)pa * maxB);
+  take(s ? s->Cen : dummy, (long)pb * maxB * d);
+  take(s ? s->Nxt : dummy, (long)pb * maxB * d);
+  take(s ? s->Xb : dummy, (long)pa * maxB * d);
+  take(s ? s->Pb : dummy, (long)pa * maxB * kN2);
+  take(s ? s->Qt : dummy, (long)pa * maxB);
+  take(s ? s->QRb : dummy, (long)pq * maxB);
+  take(s ? s->Rf : dummy, (long)pb * maxB);
+  take(s ? s->red : dummy, 4 * kWarps);
+  take(s ? s->tau : dummy, maxB);
+  take(s ? s->wv : dummy, maxB);
+  take(s ? s->M : dummy, 16);
+  take(s ? s->Cm : dummy, 16);
+  take(s ? s->O1 : dummy, 4);
+  take(s ? s->O2 : dummy, 4);
+  take(s ? s->pdf : dummy, G);
+  take(s ? s->sc : dummy, 16);
+  if (s) {
+    s->sbC = pb * maxB;
+    s->sbX = pa * maxB;
+  }
+  return off;
+}
+
+// dst[sigma*sb + r + ld*c] = src[r + dl*(c + dr*sigma)]   (site storage -> padded smem)
+__device__ __forceinline__ void load_site(double *dst, int ld, int sb, const double *src, int dl,
+                                          int dr) {
+  const int n = dl * dr * kMaxD;
+  for (int q = threadIdx.x; q < n; q += kThreads) {
+    const int r = q % dl, rest = q / dl, c = rest % dr, s = rest / dr;
+    dst[s * sb + r + ld * c] = src[q];
+  }
+}
+__device__ __forceinline__ void store_site(double *dst, const double *src, int ld, int sb, int dl,
+                                           int dr) {
+  const int n = dl * dr * kMaxD;
+  for (int q = threadIdx.x; q < n; q += kThreads) {
+    const int r = q % dl, rest = q / dl, c = rest % dr, s = rest / dr;
+    dst[q] = src[s * sb + r + ld * c];
+  }
+}
+
+// Compact-MPO / overlap environment update through one site (all threads; ends with barrier).
+//   site tensor T(r, c, sigma) = T[sigma*ss + r + cs*c], r < bl, c < br
+//   Lenv (al x bl, ld pa) -> Lenv' = sum_s B[s]^T Lenv T[s]               (ar x br)
+//   Fcur[0..3] (done, Sx, iSy, Sz; ld maxA) -> Fnxt[0..3]
+// Bond coupling into the site: Jprev (0 if none).  first: Fcur is zero (site 0).
+__device__ void env_update(const Dev &p, Smem &s, const double *B, int al, int ar, int bl, int br,
+                           const double *T, int cs, int ss, const double *Fcur, double *Fnxt,
+                           double Jprev, bool first) {
+  const int d = kMaxD, lda = p.maxA, fstride = p.maxA * p.maxB;
+  // X[tau] = Lenv * T[tau]      (al x br)
+  for (int tau = 0; tau < d; ++tau)
+    cta_gemm(al, br, bl, 1.0, s.Lenv, p.pa, false, T + tau * ss, cs, false, 0.0, s.Xb + tau * s.sbX,
+             p.pa);
+  __syncthreads();
+  // P[sigma + d*tau] = B[sigma]^T X[tau]   (ar x br)
+  for (int sg = 0; sg < d; ++sg)
+    for (int tau = 0; tau < d; ++tau)
+      cta_gemm(ar, br, al, 1.0, B + (long)sg * al * ar, al, true, s.Xb + tau * s.sbX, p.pa, false,
+               0.0, s.Pb + (sg + d * tau) * s.sbX, p.pa);
+  __syncthreads();
+  // Lenv' and the operator channels opened on this site; field closes immediately.
+  for (int q = threadIdx.x; q < ar * br; q += kThreads) {
+    const int r = q % ar, c = q / ar;
+    double P[kN2];
+#pragma unroll
+    for (int k = 0; k < kN2; ++k) P[k] = s.Pb[k * s.sbX + r + p.pa * c];
+    double l = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+#pragma unroll
+    for (int k = 0; k < kN2; ++k) {
+      if ((k % d) == (k / d)) l += P[k];
+      fx += p.opSx[k] * P[k];
+      fy += p.opISy[k] * P[k];
+      fz += p.opSz[k] * P[k];
+    }
+    s.Lenv[r + p.pa * c] = l;
+    Fnxt[0 * fstride + r + lda * c] = -p.h * fz;
+    Fnxt[1 * fstride + r + lda * c] = fx;
+    Fnxt[2 * fstride + r + lda * c] = fy;
+    Fnxt[3 * fstride + r + lda * c] = fz;
+  }
+  __syncthreads();
+  if (first) return;
+  // Fdone' += sum_s B[s]^T ( sum_t G_st T[t] ),
+  // G_st = delta_st Fdone + Jprev (Sx(s,t) F_Sx - iSy(s,t) F_iSy + Sz(s,t) F_Sz)
+  for (int sg = 0; sg < d; ++sg) {
+    for (int q = threadIdx.x; q < al * bl; q += kThreads) {
+      const int r = q % al, c = q / al;
+      const double fd = Fcur[0 * fstride + r + lda * c];
+      const double fx = Fcur[1 * fstride + r + lda * c];
+      const double fy = Fcur[2 * fstride + r + lda * c];
+      const double fz = Fcur[3 * fstride + r + lda * c];
+      for (int tau = 0; tau < d; ++tau) {
+        const int k = sg + d * tau;
+        const double g = ((sg == tau) ? fd : 0.0) +
+                         Jprev * (p.opSx[k] * fx - p.opISy[k] * fy + p.opSz[k] * fz);
+        s.Xb[tau * s.sbX + r + p.pa * c] = g;
+      }
+    }
+    __syncthreads();
+    cta_gemm(al, br, bl, 1.0, s.Xb, p.pa, false, T, cs, false, 0.0, s.Qt, p.pa);
+    for (int tau = 1; tau < d; ++tau)
+      cta_gemm(al, br, bl, 1.0, s.Xb + tau * s.sbX, p.pa, false, T + tau * ss, cs, false, 1.0, s.Qt,
+               p.pa);
+    __syncthreads();
+    cta_gemm(ar, br, al, 1.0, B + (long)sg * al * ar, al, true, s.Qt, p.pa, false, 1.0, Fnxt, lda);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The walker-step kernel
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
+  extern __shared__ double smem_raw[];
+  Smem s;
+  smem_doubles(p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw);
+  const int L = p.L, d = kMaxD, tid = threadIdx.x;
+  const int N = *p.n_cur;
+  double *scr = p.scratch + (long)blockIdx.x * p.scr_stride;
+  double *Fbuf = scr + p.foff;
+  const int fst = 4 * p.maxA * p.maxB;
+  for (int w = blockIdx.x; w < N; w += gridDim.x) {
+    const int slot = p.slot_of[w];
+    double *W = p.walkers + (long)slot * p.wstride;
+    // ---------------- phase A: right sweep --------------------------------------------------
+    {
+      double *R = scr + p.roff[L];
+      if (tid == 0) R[0] = 1.0;
+      load_site(s.Cen, p.pb, s.sbC, W + p.woff[L - 1], p.bW[L - 1], p.bW[L]);
+      __syncthreads();
+      for (int k = L - 1; k >= 1; --k) {
+        const int al = p.aT[k], ar = p.aT[k + 1], bl = p.bW[k], br = p.bW[k + 1];
+        const int bll = p.bW[k - 1];
+        // LQ of the centre (bl x br*d) through QR of its transpose (br*d x bl)
+        for (int q = tid; q < bl * br * d; q += kThreads) {
+          const int r = q % bl, rest = q / bl, c = rest % br, sg = rest / br;
+          s.QRb[(c + br * sg) + p.pq * r] = s.Cen[sg * s.sbC + r + p.pb * c];
+        }
+        __syncthreads();
+        cta_householder_qr(br * d, bl, s.QRb, p.pq, s.Rf, p.pb, s.tau, s.wv, s.red);
+        // site k <- Q'^T : A_k[sg](r, c) = Q'(c + br*sg, r)
+        double *Wk = W + p.woff[k];
+        for (int q = tid; q < bl * br * d; q += kThreads) {
+          const int r = q % bl, rest = q / bl, c = rest % br, sg = rest / br;
+          Wk[q] = s.QRb[(c + br * sg) + p.pq * r];
+        }
+        // R[k] = sum_s B_k[s] (R[k+1] Q_k[s]^T)       (al x bl)
+        const double *Rn = scr + p.roff[k + 1];
+        double *Rk = scr + p.roff[k];
+        const double *Bk = p.trial + p.toff[k];
+        for (int sg = 0; sg < d; ++sg)
+          cta_gemm(ar, bl, br, 1.0, Rn, ar, false, s.QRb + br * sg, p.pq, false, 0.0,
+                   s.Xb + sg * s.sbX, p.pa);
+        // next centre: A_{k-1}[s] * R'^T   (bll x bl)
+        load_site(s.Nxt, p.pb, s.sbC, W + p.woff[k - 1], bll, bl);
+        __syncthreads();
+        cta_gemm(al, bl, ar, 1.0, Bk, al, false, s.Xb, p.pa, false, 0.0, Rk, al);
+        for (int sg = 1; sg < d; ++sg)
+          cta_gemm(al, bl, ar, 1.0, Bk + (long)sg * al * ar, al, false, s.Xb + sg * s.sbX, p.pa,
+                   false, 1.0, Rk, al);
+        for (int sg = 0; sg < d; ++sg)
+          cta_gemm(bll, bl, bl, 1.0, s.Nxt + sg * s.sbC, p.pb, false, s.Rf, p.pb, true, 0.0,
+                   s.Cen + sg * s.sbC, p.pb);
+        __syncthreads();
+      }
+      // centre on site 0 (1 x b1): normalise, overlap with R[1], sign fix
+      {
+        const int a1 = p.aT[1], b1 = p.bW[1];
+        double part = 0.0;
+        for (int q = tid; q < b1 * d; q += kThreads) {
+          const double v = s.Cen[(q / b1) * s.sbC + p.pb * (q % b1)];
+          part += v * v;
+        }
+        const double nrm = sqrt(cta_sum(part, s.red));
+        const double inv = 1.0 / nrm;
+        for (int q = tid; q < b1 * d; q += kThreads) s.Cen[(q / b1) * s.sbC + p.pb * (q % b1)] *= inv;
+        __syncthreads();
+        // ov = sum_s B_0[s] (1 x a1) R[1] (a1 x b1) C[s]^T (b1 x 1)
+        const double *R1 = scr + p.roff[1];
+        const double *B0 = p.trial + p.toff[0];
+        part = 0.0;
+        for (int q = tid; q < a1 * b1 * d; q += kThreads) {
+          const int a = q % a1, rest = q / a1, b = rest % b1, sg = rest / b1;
+          part += B0[a + a1 * sg] * R1[a + a1 * b] * s.Cen[sg * s.sbC + p.pb * b];
+        }
+        double ov = cta_sum(part, s.red);
+        if (ov < 0.0) {  // ChangePhase on site 0 (MPSstate.cpp:307-315)
+          for (int q = tid; q < b1 * d; q += kThreads) s.Cen[(q / b1) * s.sbC + p.pb * (q % b1)] *= -1.0;
+          ov = -ov;
+        }
+        if (tid == 0) s.sc[0] = ov;
+        __syncthreads();
+      }
+    }
+    // ---------------- phase B: coupling sweep -----------------------------------------------
+    double ov = s.sc[0];
+    double wt = p.weight[slot];
+    if (tid == 0) s.Lenv[0] = 1.0;
+    int cur = 0;
+    __syncthreads();
+    for (int i = 0; i < L - 1; ++i) {
+      const int al = p.aT[i], ar = p.aT[i + 1], a2 = p.aT[i + 2];
+      const int bl = p.bW[i], br = p.bW[i + 1], b2 = p.bW[i + 2];
+      const double *Bi = p.trial + p.toff[i];
+      const double *Bj = p.trial + p.toff[i + 1];
+      load_site(s.Nxt, p.pb, s.sbC, W + p.woff[i + 1], br, b2);
+      __syncthreads();
+      const int c = p.bond_c[i];
+      double num = ov;  // overlap numerator after the bond (no coupling: unchanged)
+      if (c >= 0) {
+        const int jq = p.bond_j[i];
+        const double *U = p.tabU + 16 * jq, *S = p.tabS + 4 * jq, *VT = p.tabVT + 16 * jq;
+        // left branches P[s + d t] = B_i[s]^T Lenv C[t]
+        for (int tau = 0; tau < d; ++tau)
+          cta_gemm(al, br, bl, 1.0, s.Lenv, p.pa, false, s.Cen + tau * s.sbC, p.pb, false, 0.0,
+                   s.Xb + tau * s.sbX, p.pa);
+        __syncthreads();
+        for (int sg = 0; sg < d; ++sg)
+          for (int tau = 0; tau < d; ++tau)
+            cta_gemm(ar, br, al, 1.0, Bi + (long)sg * al * ar, al, true, s.Xb + tau * s.sbX, p.pa,
+                     false, 0.0, s.Pb + (sg + d * tau) * s.sbX, p.pa);
+        __syncthreads();
+        // right branches Y[t'] = R[i+2] N[t']^T, Q = B_j[s'] Y[t'], closures M[p + 4q]
+        const double *R2 = scr + p.roff[i + 2];
+        for (int tau = 0; tau < d; ++tau)
+          cta_gemm(a2, br, b2, 1.0, R2, a2, false, s.Nxt + tau * s.sbC, p.pb, true, 0.0,
+                   s.Xb + tau * s.sbX, p.pa);
+        __syncthreads();
+        for (int sg = 0; sg < d; ++sg)
+          for (int tau = 0; tau < d; ++tau) {
+            cta_gemm(ar, br, a2, 1.0, Bj + (long)sg * ar * a2, ar, false, s.Xb + tau * s.sbX, p.pa,
+                     false, 0.0, s.Qt, p.pa);
+            __syncthreads();
+            double v[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int q = tid; q < ar * br; q += kThreads) {
+              const int r = q % ar, cc = q / ar;
+              const double qv = s.Qt[r + p.pa * cc];
+#pragma unroll
+              for (int k = 0; k < 4; ++k) v[k] += s.Pb[k * s.sbX + r + p.pa * cc] * qv;
+            }
+            cta_sum4(v, s.red);
+            if (tid == 0)
+              for (int k = 0; k < 4; ++k) s.M[k + 4 * (sg + d * tau)] = v[k];
+          }
+        __syncthreads();
+        // C[k + 4 l] = sqrt(s_k s_l) sum_{p,q} U[p + 4k] VT[l + 4q] M[p + 4q]
+        if (tid < 16) {
+          const int k = tid & 3, l = tid >> 2;
+          double acc = 0.0;
+          for (int qq = 0; qq < 4; ++qq) {
+            double inner = 0.0;
+            for (int pp = 0; pp < 4; ++pp) inner += U[pp + 4 * k] * s.M[pp + 4 * qq];
+            acc += inner * VT[l + 4 * qq];
+          }
+          s.Cm[k + 4 * l] = sqrt(S[k]) * sqrt(S[l]) * acc;
+        }
+        __syncthreads();
+        // PDF over the grid (MPSQMC2.cpp:554-567)
+        const double fac = 4.0 / (ov * p.G);
+        double part = 0.0;
+        for (int g = tid; g < p.G; g += kThreads) {
+          const double *x = p.grid + 4 * g;
+          double v = 0.0;
+          for (int l = 0; l < 4; ++l)
+            for (int r = 0; r < 4; ++r) v += s.Cm[l + 4 * r] * x[l] * x[r];
+          v = fmax(0.0, v);
+          v *= fac;
+          s.pdf[g] = v;
+          part += v;
+        }
+        const double pnorm = cta_sum(part, s.red);
+        const double pinv = 1.0 / pnorm;
+        for (int g = tid; g < p.G; g += kThreads) s.pdf[g] *= pinv;
+        wt *= pnorm;
+        __syncthreads();
+        if (tid == 0) {
+          const double u = p.uni[(long)w * p.nC + c];
+          int count = 0;
+          double cum = s.pdf[0];
+          while ((cum <= u) && (count < p.G - 1)) {
+            count += 1;
+            cum += s.pdf[count];
+          }
+          const double *x = p.grid + 4 * count;
+          double nm = 0.0;
+          for (int l = 0; l < 4; ++l)
+            for (int r = 0; r < 4; ++r) nm += s.Cm[l + 4 * r] * x[l] * x[r];
+          s.sc[1] = 4.0 * nm;
+          s.sc[2] = count;
+          s.sc[3] = u;
+          s.sc[4] = pnorm;
+          // O1(s,t) = sum_k sqrt(4 s_k) x_k U[s + 2(t + 2k)], O2(s,t) = sum_l sqrt(4 s_l) x_l VT[l + 4(s + 2t)]
+          for (int q = 0; q < 4; ++q) {
+            double o1 = 0.0, o2 = 0.0;
+            for (int k = 0; k < 4; ++k) {
+              const double pf = sqrt(S[k] * 4.0) * x[k];
+              o1 += pf * U[q + 4 * k];
+              o2 += pf * VT[k + 4 * q];
+            }
+            s.O1[q] = o1;
+            s.O2[q] = o2;
+          }
+        }
+        __syncthreads();
+        num = s.sc[1];
+        // apply O1 to the centre (into the QR layout), O2 to site j in place
+        for (int q = tid; q < bl * br; q += kThreads) {
+          const int r = q % bl, cc = q / bl;
+          const double c0 = s.Cen[r + p.pb * cc], c1 = s.Cen[s.sbC + r + p.pb * cc];
+          s.QRb[(r + bl * 0) + p.pq * cc] = s.O1[0] * c0 + s.O1[2] * c1;
+          s.QRb[(r + bl * 1) + p.pq * cc] = s.O1[1] * c0 + s.O1[3] * c1;
+        }
+        for (int q = tid; q < br * b2; q += kThreads) {
+          const int r = q % br, cc = q / br;
+          const double n0 = s.Nxt[r + p.pb * cc], n1 = s.Nxt[s.sbC + r + p.pb * cc];
+          s.Nxt[r + p.pb * cc] = s.O2[0] * n0 + s.O2[2] * n1;
+          s.Nxt[s.sbC + r + p.pb * cc] = s.O2[1] * n0 + s.O2[3] * n1;
+        }
+      } else {
+        for (int q = tid; q < bl * br; q += kThreads) {
+          const int r = q % bl, cc = q / bl;
+          s.QRb[(r + bl * 0) + p.pq * cc] = s.Cen[r + p.pb * cc];
+          s.QRb[(r + bl * 1) + p.pq * cc] = s.Cen[s.sbC + r + p.pb * cc];
+        }
+      }
+      __syncthreads();
+      // move the centre: QR of site i, R into site i+1
+      cta_householder_qr(bl * d, br, s.QRb, p.pq, s.Rf, p.pb, s.tau, s.wv, s.red);
+      for (int sg = 0; sg < d; ++sg)
+        cta_gemm(br, b2, br, 1.0, s.Rf, p.pb, false, s.Nxt + sg * s.sbC, p.pb, false, 0.0,
+                 s.Cen + sg * s.sbC, p.pb);
+      // site i <- Q
+      {
+        double *Wi = W + p.woff[i];
+        for (int q = tid; q < bl * br * d; q += kThreads) {
+          const int r = q % bl, rest = q / bl, cc = rest % br, sg = rest / br;
+          Wi[q] = s.QRb[(r + bl * sg) + p.pq * cc];
+        }
+      }
+      __syncthreads();
+      if (c >= 0) {
+        double part = 0.0;
+        for (int q = tid; q < br * b2 * d; q += kThreads) {
+          const int r = q % br, rest = q / br, cc = rest % b2, sg = rest / b2;
+          const double v = s.Cen[sg * s.sbC + r + p.pb * cc];
+          part += v * v;
+        }
+        const double nrm = sqrt(cta_sum(part, s.red));
+        ov = num / nrm;
+        const double scale = (ov < 0.0) ? -1.0 / nrm : 1.0 / nrm;
+        if (ov < 0.0) ov = -ov;
+        for (int q = tid; q < br * b2 * d; q += kThreads) {
+          const int r = q % br, rest = q / br, cc = rest % b2, sg = rest / b2;
+          s.Cen[sg * s.sbC + r + p.pb * cc] *= scale;
+        }
+        if (p.trace != nullptr && tid == 0) {
+          double *t = p.trace + ((long)w * p.nC + c) * kTraceStride;
+          for (int k = 0; k < 16; ++k) t[k] = s.Cm[k];
+          t[16] = s.sc[4];
+          t[17] = s.sc[3];
+          t[18] = s.sc[2];
+          t[19] = wt;
+          t[20] = ov;
+        }
+      }
+      // environments through the final site i
+      env_update(p, s, Bi, al, ar, bl, br, s.QRb, p.pq, bl, Fbuf + cur * fst, Fbuf + (1 - cur) * fst,
+                 (i > 0) ? p.bondJ[i - 1] : 0.0, i == 0);
+      cur = 1 - cur;
+    }
+    // last site: centre; overlap and energy (final setOverlap, MPSQMC2.cpp:598; Walker.cpp:76)
+    {
+      const int i = L - 1;
+      const int al = p.aT[i], bl = p.bW[i];
+      env_update(p, s, p.trial + p.toff[i], al, 1, bl, 1, s.Cen, p.pb, s.sbC, Fbuf + cur * fst,
+                 Fbuf + (1 - cur) * fst, p.bondJ[i - 1], false);
+      store_site(W + p.woff[i], s.Cen, p.pb, s.sbC, bl, 1);
+      const double ovf = s.Lenv[0];
+      const double en = Fbuf[(1 - cur) * fst + 0];
+      if (tid == 0) {
+        p.overlap[slot] = ovf;
+        p.weight[slot] = wt;
+        p.energy[w] = en / ovf;
+        p.ov_out[w] = ovf;
+        p.wt_out[w] = wt;
+        if (!(isfinite(wt) && isfinite(ovf) && isfinite(en))) atomicOr(p.err, kErrNumeric);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Walker::setOverlap exactly as the reference does it (Walker.cpp:54-66): Householder
+// LeftNormalize (MPSstate.cpp:216-229), overlap <Psi_T|phi>, ChangePhase if negative.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads, 1) set_overlap_kernel(Dev p) {
+  extern __shared__ double smem_raw[];
+  Smem s;
+  smem_doubles(p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw);
+  const int L = p.L, d = kMaxD, tid = threadIdx.x;
+  const int N = *p.n_cur;
+  for (int w = blockIdx.x; w < N; w += gridDim.x) {
+    const int slot = p.slot_of[w];
+    double *W = p.walkers + (long)slot * p.wstride;
+    load_site(s.Cen, p.pb, s.sbC, W + p.woff[0], p.bW[0], p.bW[1]);
+    __syncthreads();
+    for (int k = 0; k < L; ++k) {
+      const int bl = p.bW[k], br = p.bW[k + 1];
+      for (int q = tid; q < bl * br; q += kThreads) {
+        const int r = q % bl, cc = q / bl;
+        for (int sg = 0; sg < d; ++sg) s.QRb[(r + bl * sg) + p.pq * cc] = s.Cen[sg * s.sbC + r + p.pb * cc];
+      }
+      __syncthreads();
+      cta_householder_qr(bl * d, br, s.QRb, p.pq, s.Rf, p.pb, s.tau, s.wv, s.red);
+      double *Wk = W + p.woff[k];
+      for (int q = tid; q < bl * br * d; q += kThreads) {
+        const int r = q % bl, rest = q / bl, cc = rest % br, sg = rest / br;
+        Wk[q] = s.QRb[(r + bl * sg) + p.pq * cc];
+      }
+      if (k < L - 1) {
+        const int b2 = p.bW[k + 2];
+        load_site(s.Nxt, p.pb, s.sbC, W + p.woff[k + 1], br, b2);
+        __syncthreads();
+        for (int sg = 0; sg < d; ++sg)
+          cta_gemm(br, b2, br, 1.0, s.Rf, p.pb, false, s.Nxt + sg * s.sbC, p.pb, false, 0.0,
+                   s.Cen + sg * s.sbC, p.pb);
+      }
+      __syncthreads();
+    }
+    // overlap sweep: Lenv' = sum_s B[s]^T Lenv A[s]
+    if (tid == 0) s.Lenv[0] = 1.0;
+    __syncthreads();
+    for (int k = 0; k < L; ++k) {
+      const int al = p.aT[k], ar = p.aT[k + 1], bl = p.bW[k], br = p.bW[k + 1];
+      const double *A = W + p.woff[k];
+      const double *B = p.trial + p.toff[k];
+      for (int sg = 0; sg < d; ++sg)
+        cta_gemm(al, br, bl, 1.0, s.Lenv, p.pa, false, A + (long)sg * bl * br, bl, false, 0.0,
+                 s.Xb + sg * s.sbX, p.pa);
+      __syncthreads();
+      cta_gemm(ar, br, al, 1.0, B, al, true, s.Xb, p.pa, false, 0.0, s.Qt, p.pa);
+      for (int sg = 1; sg < d; ++sg)
+        cta_gemm(ar, br, al, 1.0, B + (long)sg * al * ar, al, true, s.Xb + sg * s.sbX, p.pa, false,
+                 1.0, s.Qt, p.pa);
+      __syncthreads();
+      for (int q = tid; q < ar * br; q += kThreads) s.Lenv[(q % ar) + p.pa * (q / ar)] = s.Qt[(q % ar) + p.pa * (q / ar)];
+      __syncthreads();
+    }
+    double ov = s.Lenv[0];
+    __syncthreads();
+    if (ov < 0.0) {
+      const int n0 = p.bW[0] * p.bW[1] * d;
+      for (int q = tid; q < n0; q += kThreads) W[p.woff[0] + q] *= -1.0;
+      ov = -ov;
+    }
+    if (tid == 0) p.overlap[slot] = ov;
+    __syncthreads();
+  }
+}
+
+// <Psi_T|H|phi> / overlap for every walker, walker tensors taken as stored (any gauge).
+__global__ void __launch_bounds__(kThreads, 1) energy_kernel(Dev p) {
+  extern __shared__ double smem_raw[];
+  Smem s;
+  smem_doubles(p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw);
+  const int L = p.L, tid = threadIdx.x;
+  const int N = *p.n_cur;
+  double *scr = p.scratch + (long)blockIdx.x * p.scr_stride;
+  double *Fbuf = scr + p.foff;
+  const int fst = 4 * p.maxA * p.maxB;
+  for (int w = blockIdx.x; w < N; w += gridDim.x) {
+    const int slot = p.slot_of[w];
+    const double *W = p.walkers + (long)slot * p.wstride;
+    if (tid == 0) s.Lenv[0] = 1.0;
+    __syncthreads();
+    int cur = 0;
+    for (int k = 0; k < L; ++k) {
+      const int al = p.aT[k], ar = p.aT[k + 1], bl = p.bW[k], br = p.bW[k + 1];
+      env_update(p, s, p.trial + p.toff[k], al, ar, bl, br, W + p.woff[k], bl, bl * br,
+                 Fbuf + cur * fst, Fbuf + (1 - cur) * fst, (k > 0) ? p.bondJ[k - 1] : 0.0, k == 0);
+      cur = 1 - cur;
+    }
+    if (tid == 0) {
+      const double en = Fbuf[cur * fst];
+      p.energy[w] = en / p.overlap[slot];
+      p.ov_out[w] = p.overlap[slot];
+      p.wt_out[w] = p.weight[slot];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// MT19937 (Matsumoto & Nishimura 1998), one CTA, the reference's single random stream.
+// ---------------------------------------------------------------------------------------------
+struct MtState {
+  uint32_t mt[624];
+  int idx;
+  int pad;
+  unsigned long long draws;
+};
+
+__device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
+  y ^= (y >> 11);
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  y ^= (y >> 18);
+  return y;
+}
+
+__device__ void mt_twist_range(uint32_t *mt, int lo, int hi) {
+  // new mt[i] for i in [lo, hi), all inputs already final for this phase
+  uint32_t v = 0;
+  const int i = lo + threadIdx.x;
+  const bool act = i < hi;
+  if (act) {
+    const uint32_t y = (mt[i] & 0x80000000u) | (mt[(i + 1) % 624] & 0x7fffffffu);
+    v = mt[(i + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+  }
+  __syncthreads();
+  if (act) mt[i] = v;
+  __syncthreads();
+}
+
+// Produce the next n uniforms (n from *n_dev when non-null) into out.  blockDim = 1024.
+__global__ void mt_generate_kernel(MtState *st, const int *n_dev, long n_host, long mult,
+                                   double *out) {
+  __shared__ uint32_t mt[624];
+  __shared__ int s_idx;
+  const long n = n_dev ? (long)(*n_dev) * mult : n_host;
+  for (int q = threadIdx.x; q < 624; q += blockDim.x) mt[q] = st->mt[q];
+  if (threadIdx.x == 0) s_idx = st->idx;
+  __syncthreads();
+  long pos = 0;
+  while (pos < n) {
+    if (s_idx >= 624) {
+      mt_twist_range(mt, 0, 227);
+      mt_twist_range(mt, 227, 454);
+      mt_twist_range(mt, 454, 623);
+      mt_twist_range(mt, 623, 624);
+      if (threadIdx.x == 0) s_idx = 0;
+      __syncthreads();
+    }
+    const int idx = s_idx;
+    const long take = min((long)(624 - idx), n - pos);
+    for (int q = threadIdx.x; q < take; q += blockDim.x)
+      out[pos + q] = (double)mt_temper(mt[idx + q]) / 4294967296.0;
+    __syncthreads();
+    if (threadIdx.x == 0) s_idx = idx + (int)take;
+    pos += take;
+    __syncthreads();
+  }
+  for (int q = threadIdx.x; q < 624; q += blockDim.x) st->mt[q] = mt[q];
+  if (threadIdx.x == 0) {
+    st->idx = s_idx;
+    st->draws += (unsigned long long)n;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Statistics and population control (one CTA, 1024 threads)
+// ---------------------------------------------------------------------------------------------
+struct StepDev {
+  int n_cur, n_flag, n_new, n_extra, n_free, step, status, pad;
+  double sumw, EP, ET, omega, scaling;
+};
+
+template <typename T>
+__device__ T block_scan_excl(T v, T *buf, T &total) {  // blockDim.x == 1024
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  T x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  __syncthreads();
+  if (lane == 31) buf[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    T t = buf[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const T y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    buf[lane] = t;
+  }
+  __syncthreads();
+  total = buf[31];
+  const T before = (warp > 0) ? buf[warp - 1] : T(0);
+  __syncthreads();
+  return before + x - v;
+}
+
+__device__ double block_sum_d(double v, double *buf) {  // blockDim.x == 1024
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) buf[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int q = 0; q < 32; ++q) s += buf[q];
+  __syncthreads();
+  return s;
+}
+
+// Weight sum, E_T, E_P, energy history, fluctuation metric (MPSQMC2.cpp:468-487, 688-747),
+// then the branching flags of SeparatePopulationControl (613-648).
+__global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Ndesired, double dtau,
+                                                     int step, int update_history, int *flag_pos,
+                                                     double *sw_out) {
+  __shared__ double dbuf[32];
+  __shared__ int ibuf[32];
+  const int N = sd->n_cur;
+  double sw = 0.0, num = 0.0;
+  for (int w = threadIdx.x; w < N; w += 1024) {
+    const double wt = p.wt_out[w];
+    sw += wt;
+    num += wt * p.energy[w];
+  }
+  const double sumw = block_sum_d(sw, dbuf);
+  const double numer = block_sum_d(num, dbuf);
+  const double avgW = sumw / N;
+  const double scaling = Ndesired / (N * avgW);
+  double se = 0.0, se2 = 0.0;
+  if (update_history) {
+    for (int w = threadIdx.x; w < N; w += 1024) {
+      const int slot = p.slot_of[w];
+      const double h = p.ehist[slot] + p.energy[w];
+      p.ehist[slot] = h;
+      const double e = h / step;
+      se += e;
+      se2 += e * e;
+    }
+  }
+  const double sE = block_sum_d(se, dbuf);
+  const double sE2 = block_sum_d(se2, dbuf);
+  // flags: walkers whose scaled weight leaves [0.25, 1.5] draw one uniform, in walker order
+  int nflag_total = 0;
+  for (int base = 0; base < N; base += 1024) {
+    const int w = base + threadIdx.x;
+    int f = 0;
+    double s = 0.0;
+    if (w < N) {
+      s = p.wt_out[w] * scaling;
+      sw_out[w] = s;
+      f = (s < 0.25 || s > 1.5) ? 1 : 0;
+    }
+    int tot;
+    const int ex = block_scan_excl<int>(f, ibuf, tot);
+    if (w < N) flag_pos[w] = f ? nflag_total + ex : -1;
+    nflag_total += tot;
+  }
+  if (threadIdx.x == 0) {
+    sd->sumw = sumw;
+    sd->scaling = scaling;
+    sd->ET = log(scaling) / dtau;
+    sd->EP = numer / sumw;
+    sd->omega = update_history ? (sE2 - sE * sE / N) / N : 0.0;
+    sd->n_flag = nflag_total;
+    if (!(isfinite(sumw) && sumw > 0.0 && isfinite(numer))) atomicOr(p.err, kErrNumeric);
+  }
+}
+
+// Threshold branching (MPSQMC2.cpp:620-686) with a slot table: the first copy of a surviving
+// walker keeps its slot, extra copies take free slots, killed walkers free theirs.
+__global__ void __launch_bounds__(1024) branch_kernel(Dev p, StepDev *sd, const int *flag_pos,
+                                                      const double *sw_in, const double *ubr,
+                                                      int *slot_of_new, int *free_slots,
+                                                      int *copy_src, int *copy_dst, int *parent,
+                                                      int capacity) {
+  __shared__ int ibuf[32];
+  const int N = sd->n_cur;
+  int nfree = sd->n_free;
+  int new_total = 0, extra_total = 0, killed_total = 0;
+  // pass 1: killed slots onto the free stack (in walker order)
+  for (int base = 0; base < N; base += 1024) {
+    const int w = base + threadIdx.x;
+    int nc = 1;
+    if (w < N) {
+      const double s = sw_in[w];
+      if (flag_pos[w] >= 0) nc = (int)(s + ubr[flag_pos[w]]);
+    }
+    int tot;
+    const int k = block_scan_excl<int>((w < N && nc == 0) ? 1 : 0, ibuf, tot);
+    if (w < N && nc == 0) free_slots[nfree + killed_total + k] = p.slot_of[w];
+    killed_total += tot;
+  }
+  __syncthreads();
+  nfree += killed_total;
+  // pass 2: new logical order
+  for (int base = 0; base < N; base += 1024) {
+    const int w = base + threadIdx.x;
+    int nc = 0;
+    double s = 0.0, neww = 0.0;
+    if (w < N) {
+      s = sw_in[w];
+      nc = 1;
+      neww = s;
+      if (flag_pos[w] >= 0) {
+        nc = (int)(s + ubr[flag_pos[w]]);
+        neww = (s < 0.25) ? 1.0 : s / nc;
+      }
+    }
+    int tot_new, tot_extra;
+    const int pos = block_scan_excl<int>(nc, ibuf, tot_new);
+    const int ex = block_scan_excl<int>(nc > 1 ? nc - 1 : 0, ibuf, tot_extra);
+    if (w < N && nc >= 1) {
+      const int slot = p.slot_of[w];
+      const int dst0 = new_total + pos;
+      if (dst0 < capacity) {
+        slot_of_new[dst0] = slot;
+        parent[dst0] = w;
+      }
+      p.weight[slot] = neww;
+      for (int c = 1; c < nc; ++c) {
+        const int e = extra_total + ex + (c - 1);
+        const int fs = nfree - 1 - e;
+        const int dst = dst0 + c;
+        if (fs >= 0 && dst < capacity) {
+          const int ns = free_slots[fs];
+          slot_of_new[dst] = ns;
+          parent[dst] = w;
+          copy_src[e] = slot;
+          copy_dst[e] = ns;
+        }
+      }
+    }
+    new_total += tot_new;
+    extra_total += tot_extra;
+  }
+  if (threadIdx.x == 0) {
+    sd->n_new = new_total;
+    sd->n_extra = extra_total;
+    if (extra_total > nfree || new_total > capacity) {
+      atomicOr(p.err, kErrCapacity);
+      sd->n_free = nfree;
+    } else {
+      sd->n_free = nfree - extra_total;
+    }
+  }
+}
+
+// Copy walker slots for the extra copies: tensors and scalar state.
+__global__ void copy_walkers_kernel(Dev p, const StepDev *sd, const int *copy_src,
+                                    const int *copy_dst) {
+  const int n = sd->n_extra;
+  if (p.err != nullptr && (*p.err & kErrCapacity)) return;
+  const long per = p.wstride;
+  for (long q = blockIdx.x; q < (long)n; q += gridDim.x) {
+    const int src = copy_src[q], dst = copy_dst[q];
+    const double *a = p.walkers + (long)src * per;
+    double *b = p.walkers + (long)dst * per;
+    for (long e = threadIdx.x; e < per; e += blockDim.x) b[e] = a[e];
+    if (threadIdx.x == 0) {
+      p.weight[dst] = p.weight[src];
+      p.overlap[dst] = p.overlap[src];
+      p.ehist[dst] = p.ehist[src];
+    }
+  }
+}
+
+// New population becomes current: slot table copied back, counts updated (one CTA).
+__global__ void finish_branch_kernel(StepDev *sd, int *n_cur, int *slot_of, const int *slot_of_new,
+                                     const int *err, int capacity) {
+  if (*err & kErrCapacity) return;
+  const int nn = min(sd->n_new, capacity);
+  for (int q = threadIdx.x; q < nn; q += blockDim.x) slot_of[q] = slot_of_new[q];
+  if (threadIdx.x == 0) {
+    sd->n_cur = nn;
+    *n_cur = nn;
+  }
+}
+
+}  // namespace mq

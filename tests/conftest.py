@@ -1,0 +1,33 @@
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the CUDA engine")
+
+
+def load_golden(name: str) -> dict:
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    out = {k: z[k] for k in z.files}
+    if "meta" in out:
+        out["meta"] = json.loads(str(out["meta"]))
+    return out
+
+
+WALK_CASES = ["walk_L16D16_DW16", "walk_L10D8_DW4", "walk_L10D8_DW2_branch", "walk_L10D8_DW1_branch",
+              "walk_debug_DW2"]
+
+
+@pytest.fixture(scope="session")
+def golden():
+    return load_golden

@@ -1,0 +1,132 @@
+"""CUDA engine (libmpsqmc_b200.so through its C ABI) against the reference's own trajectories.
+
+Same trial, Trotter tables, grid, initial walkers and random stream as the reference run that
+produced the fixture; every quantity of the walk is compared:
+  - per-step N, sum of weights, E_P, E_T, fluctuation metric;
+  - per-walker weight, overlap and local energy after propagation (relative 1e-10, FP64 mode);
+  - per-coupling C_kl, uniform and sampled grid index;
+  - branching parents (bit-exact) and the number of uniforms consumed;
+  - final walker states (fidelity with the reference tensors; the engine's gauge differs).
+"""
+import numpy as np
+import pytest
+
+from conftest import WALK_CASES, load_golden
+from mpsqmc_b200 import Engine
+from mpsqmc_b200 import problem as pb
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-10
+
+
+def engine_for(z, capacity=None):
+    meta = z["meta"]
+    L, N = meta["L"], meta["Nw"]
+    ci, cj, cJ = pb.chain(L)
+    eng = Engine(L=L, ci=ci, cj=cj, cJ=cJ, h=0.0, dtau=meta["dtau"], trial_dims=z["trial_ln_dims"],
+                 trial=z["trial_ln_data"], Jvals=[1.0], U=z["U"], S=z["S"], VT=z["VT"], grid=z["grid"],
+                 Ndesired=N, capacity=capacity or max(1000, 3 * N), walker_dims=z["walker0_init_dims"])
+    walkers = np.tile(z["walker0_init_data"], (N, 1))
+    eng.set_walkers(walkers, z["init_weight"], z["init_overlap"], np.zeros(N), normalize=False)
+    eng.set_rng(meta["seed"], meta["setup_draws"])
+    return eng
+
+
+def fidelity(dims_a, a, dims_b, b):
+    A, B = po.MPS(np.asarray(dims_a, np.int32), a), po.MPS(np.asarray(dims_b, np.int32), b)
+    ab = po.inner_product(A, B)
+    return ab / np.sqrt(po.inner_product(A, A) * po.inner_product(B, B))
+
+
+@pytest.mark.parametrize("case", WALK_CASES)
+def test_walk_matches_reference(case):
+    z = load_golden(case)
+    meta = z["meta"]
+    eng = engine_for(z)
+    assert eng.energy() == pytest.approx(meta["E0"], rel=RTOL)
+    total_draws = 0
+    for s in range(1, meta["steps"] + 1):
+        p = f"step{s:03d}_"
+        eng.set_trace(True)
+        st = eng.walk(1)[0]
+        lw = eng.last_step_walkers()
+        tr = eng.get_trace()
+        n = len(z[p + "weight"])
+        assert st["n_walkers"] == n == z["stat_n"][s - 1]
+        assert st["sum_weight"] == pytest.approx(z["stat_sumw"][s - 1], rel=RTOL)
+        assert st["E_P"] == pytest.approx(z["stat_EP"][s - 1], rel=RTOL)
+        assert st["E_T"] == pytest.approx(z["stat_ET"][s - 1], rel=1e-8, abs=1e-8)
+        assert abs(st["omega"] - z["stat_omega"][s - 1]) <= 1e-9 * z["stat_EP"][s - 1] ** 2
+        np.testing.assert_allclose(lw["weight"], z[p + "weight"], rtol=RTOL)
+        np.testing.assert_allclose(lw["overlap"], z[p + "overlap"], rtol=RTOL)
+        np.testing.assert_allclose(lw["energy"], z[p + "energy"], rtol=RTOL)
+        t = tr.reshape(-1, 21)
+        np.testing.assert_array_equal(t[:, 17], z[p + "trace_u"])
+        np.testing.assert_array_equal(t[:, 18].astype(int), z[p + "trace_index"])
+        np.testing.assert_allclose(t[:, :16], z[p + "trace_C"], rtol=0, atol=1e-12)
+        np.testing.assert_allclose(t[:, 16], z[p + "trace_pdfnorm"], rtol=RTOL)
+        np.testing.assert_array_equal(lw["parent"], z[p + "parent"])
+        assert st["draws"] == int(np.sum(z["stat_draws"][s - 1]))
+        total_draws += st["draws"]
+    assert eng.rng_draws() == total_draws
+    w, wt, ov, eh = eng.get_walkers()
+    last = f"step{meta['steps']:03d}_"
+    ref = z[last + "tensors"][z[last + "parent"]]
+    dims = z["walker0_init_dims"]
+    for k in range(w.shape[0]):
+        assert fidelity(dims, w[k], dims, ref[k]) == pytest.approx(1.0, abs=1e-12)
+    np.testing.assert_allclose(wt, z[last + "newweight"], rtol=RTOL)
+    np.testing.assert_allclose(eh, z[last + "ehist"][z[last + "parent"]], rtol=RTOL)
+
+
+def test_set_overlap_is_reference_exact():
+    """Walker::setOverlap on device: Householder LeftNormalize element by element, overlap, sign."""
+    z = load_golden("mpsops_debug")
+    g = load_golden("grids")["marsaglia4"]
+    tr = load_golden("trotter")
+    trial_dims, trial = z["leftnorm_dims"], z["leftnorm_data"]
+    L = len(trial_dims) - 1
+    ci, cj, cJ = pb.chain(L)
+    eng = Engine(L=L, ci=ci, cj=cj, cJ=cJ, h=0.0, dtau=0.01, trial_dims=trial_dims, trial=trial, Jvals=[1.0],
+                 U=tr["dt0.01_J1.0_U"], S=tr["dt0.01_J1.0_S"], VT=tr["dt0.01_J1.0_VT"], grid=g, Ndesired=1,
+                 capacity=4, walker_dims=z["other_dims"])
+    eng.set_walkers(z["other_data"][None, :], [1.0], normalize=True)
+    w, wt, ov, eh = eng.get_walkers()
+    ref = z["other_leftnorm_data"].copy()
+    sc = z["scalars"]
+    ov_ref = sc[5]
+    if ov_ref < 0:  # ChangePhase on site 0
+        n0 = int(z["other_dims"][0] * z["other_dims"][1] * 2)
+        ref[:n0] *= -1
+        ov_ref = -ov_ref
+    np.testing.assert_allclose(w[0], ref, rtol=0, atol=1e-13)
+    assert ov[0] == pytest.approx(ov_ref, rel=1e-12)
+
+
+def test_local_energy_matches_oracle():
+    z = load_golden("walk_L16D16_DW16")
+    eng = engine_for(z)
+    eng.walk(2)
+    w, wt, ov, eh = eng.get_walkers()
+    lw_e = eng.energy()
+    trial = po.MPS(z["trial_ln_dims"], z["trial_ln_data"])
+    ci, cj, cJ = pb.chain(16)
+    num = 0.0
+    den = 0.0
+    for k in range(w.shape[0]):
+        phi = po.MPS(z["walker0_init_dims"], w[k])
+        e = po.energy_numerator(trial, phi, ci, cj, cJ) / ov[k]
+        num += wt[k] * e
+        den += wt[k]
+    assert lw_e == pytest.approx(num / den, rel=RTOL)
+
+
+def test_capacity_overflow_is_an_error_not_a_crash():
+    from mpsqmc_b200.capi import E_CAPACITY, MpsqmcError
+    z = load_golden("walk_L10D8_DW1_branch")
+    eng = engine_for(z, capacity=33)
+    with pytest.raises(MpsqmcError) as ei:
+        eng.walk(8)
+    assert ei.value.code == E_CAPACITY

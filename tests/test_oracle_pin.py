@@ -1,0 +1,152 @@
+"""The CPU oracle (oracle/mpsqmc_oracle.cpp) against outputs of the reference itself.
+
+Fixtures under tests/golden/ were produced by the reference's own C++ (tests/golden/make_golden.py).
+These checks pin the oracle before it is trusted as the checker of the CUDA engine.
+"""
+import numpy as np
+import pytest
+
+from conftest import WALK_CASES, load_golden
+from oracle import pyoracle as po
+
+
+def test_grid_marsaglia_matches_reference():
+    g = load_golden("grids")["marsaglia4"]
+    mine = po.grid_marsaglia(4, 4)
+    assert mine.shape == g.shape == (240, 4)
+    np.testing.assert_allclose(mine, g, rtol=0, atol=1e-15)
+    # isotropy: sum_p x x^T = G/dim * I (GridGenerator.cpp:93-102)
+    np.testing.assert_allclose(g.T @ g, 60.0 * np.eye(4), atol=1e-12)
+
+
+def test_grid_simple_matches_reference():
+    g = load_golden("grids")["simple4"]
+    mine = po.grid_simple(4, 4)
+    assert mine.shape == g.shape
+    np.testing.assert_allclose(mine, g, rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("key", ["dt0.01_J1.0", "dt0.005_J1.0", "dt0.01_J0.5", "dt0.3_J1.0", "dt0.5_J1.0"])
+def test_trotter_tables_match_reference(key):
+    z = load_golden("trotter")
+    dt = float(key.split("_")[0][2:])
+    J = float(key.split("_")[1][1:])
+    U, S, VT = po.trotter(J, dt)
+    np.testing.assert_allclose(S, z[key + "_S"], rtol=1e-13, atol=1e-15)
+
+    def recon(U, S, VT):
+        return U.reshape(4, 4, order="F") @ np.diag(S) @ VT.reshape(4, 4, order="F")
+
+    np.testing.assert_allclose(recon(U, S, VT), recon(z[key + "_U"], z[key + "_S"], z[key + "_VT"]),
+                               atol=1e-14)
+
+
+def _mps(z, prefix):
+    return po.MPS(z[prefix + "_dims"].astype(np.int32), z[prefix + "_data"])
+
+
+def test_inner_product_and_left_normalize_match_reference():
+    z = load_golden("mpsops_debug")
+    sc = z["scalars"]
+    trial = _mps(z, "trial")
+    other = _mps(z, "other")
+    assert po.inner_product(trial, trial) == pytest.approx(sc[0], rel=1e-13)
+    ln, r = po.left_normalize(trial)
+    assert r == pytest.approx(sc[1], rel=1e-13)
+    ref_ln = _mps(z, "leftnorm")
+    np.testing.assert_array_equal(ln.dims, ref_ln.dims)
+    # element by element: same Householder conventions as dgeqrf/dorgqr
+    np.testing.assert_allclose(ln.data, ref_ln.data, rtol=0, atol=1e-13)
+    assert po.inner_product(trial, other) == pytest.approx(sc[2], rel=1e-12)
+    assert po.inner_product(other, trial) == pytest.approx(sc[3], rel=1e-12)
+    oln, r2 = po.left_normalize(other)
+    assert r2 == pytest.approx(sc[4], rel=1e-12)
+    np.testing.assert_allclose(oln.data, _mps(z, "other_leftnorm").data, rtol=0, atol=1e-12)
+    assert po.inner_product(ln, oln) == pytest.approx(sc[5], rel=1e-12)
+
+
+def test_site_operators_match_reference():
+    z = load_golden("mpsops_debug")
+    ln = _mps(z, "leftnorm")
+    tr = load_golden("trotter")
+    U, S, VT = tr["dt0.01_J1.0_U"], tr["dt0.01_J1.0_S"], tr["dt0.01_J1.0_VT"]
+    g = load_golden("grids")["marsaglia4"]
+    got = po.apply_grid_op(ln, 1, 2, S, U, VT, g[37])
+    np.testing.assert_allclose(got.data, _mps(z, "gridop_1_2_37").data, rtol=0, atol=1e-14)
+    got = po.apply_svd_op(ln, 2, 3, S, U, VT, 1, 3, hc=True)
+    np.testing.assert_allclose(got.data, _mps(z, "svdop_2_3_1_3_hc").data, rtol=0, atol=1e-15)
+    ph = po.change_phase(ln)
+    assert po.inner_product(ph, ln) == pytest.approx(z["scalars"][8], rel=1e-13)
+
+
+def test_compress_is_the_same_state_as_reference():
+    """SVD signs differ between LAPACK and the oracle's Jacobi SVD; the state does not."""
+    z = load_golden("mpsops_debug")
+    ln = _mps(z, "leftnorm")
+    ref = _mps(z, "compressed")
+    mine = po.compress(ln, 2)
+    np.testing.assert_array_equal(mine.dims, ref.dims)
+    f = po.inner_product(mine, ref) / np.sqrt(po.inner_product(mine, mine) * po.inner_product(ref, ref))
+    assert abs(f) == pytest.approx(1.0, abs=1e-12)
+    assert po.inner_product(ln, mine) == pytest.approx(z["scalars"][6], rel=1e-10)
+
+
+def _walk_oracle(z, trace=True):
+    meta = z["meta"]
+    trial = po.MPS(z["trial_ln_dims"], z["trial_ln_data"])
+    w0 = po.MPS(z["walker0_init_dims"], z["walker0_init_data"])
+    L, N = meta["L"], meta["Nw"]
+    ci, cj, cJ = po.chain_couplings(L)
+    walkers = np.tile(w0.data, (N, 1))
+    return po.walk(trial, walkers, w0.dims, z["init_weight"], z["init_overlap"], np.zeros(N), ci=ci, cj=cj,
+                   cJ=cJ, Jvals=np.array([1.0]), U=z["U"], S=z["S"], VT=z["VT"], grid=z["grid"],
+                   dtau=meta["dtau"], nsteps=meta["steps"], Ndesired=N, capacity=max(1000, 3 * N),
+                   seed=meta["seed"], skip=meta["setup_draws"], trace=trace)
+
+
+@pytest.mark.parametrize("case", WALK_CASES)
+def test_walk_trajectory_matches_reference(case):
+    z = load_golden(case)
+    meta = z["meta"]
+    res = _walk_oracle(z)
+    assert res.status == 0
+    assert res.E0 == pytest.approx(meta["E0"], rel=1e-12)
+    np.testing.assert_array_equal(res.n, z["stat_n"])
+    np.testing.assert_allclose(res.sumw, z["stat_sumw"], rtol=1e-12)
+    np.testing.assert_allclose(res.EP, z["stat_EP"], rtol=1e-12)
+    np.testing.assert_allclose(res.ET, z["stat_ET"], rtol=1e-10, atol=1e-10)
+    # the fluctuation metric is a difference of nearly equal sums: absolute scale E^2
+    np.testing.assert_allclose(res.omega, z["stat_omega"], rtol=0, atol=1e-9 * np.max(np.abs(z["stat_EP"])) ** 2)
+    for s in range(1, meta["steps"] + 1):
+        p = f"step{s:03d}_"
+        n = len(z[p + "weight"])
+        np.testing.assert_allclose(res.weight[s - 1, :n], z[p + "weight"], rtol=1e-12)
+        np.testing.assert_allclose(res.overlap[s - 1, :n], z[p + "overlap"], rtol=1e-12)
+        np.testing.assert_allclose(res.energy[s - 1, :n], z[p + "energy"], rtol=1e-12)
+        np.testing.assert_array_equal(res.parent[s - 1, :len(z[p + "parent"])], z[p + "parent"])
+        tr = res.trace[s - 1, :n].reshape(-1, 21)
+        np.testing.assert_array_equal(tr[:, 18].astype(int), z[p + "trace_index"])
+        np.testing.assert_array_equal(tr[:, 17], z[p + "trace_u"])
+        np.testing.assert_allclose(tr[:, :16], z[p + "trace_C"], rtol=0, atol=1e-13)
+    last = f"step{meta['steps']:03d}_tensors"
+    # walkers after the last branching are copies of pre-branching ones
+    par = z[f"step{meta['steps']:03d}_parent"]
+    np.testing.assert_allclose(res.walkers, z[last][par], rtol=0, atol=1e-12)
+    draws = int(np.sum(z["stat_draws"]))
+    assert res.draws == draws
+
+
+def test_ed_pins_reference_value():
+    """main.cpp:153: E_FCI of the L=10 spin-1/2 chain = -4.25803520728288."""
+    from oracle import ed
+    assert ed.ground_energy(10) == pytest.approx(-4.25803520728288, abs=1e-11)
+
+
+def test_dmrg_trials_are_variational():
+    from oracle import ed
+    z = load_golden("trials")
+    for L, D in [(8, 4), (10, 8), (16, 16)]:
+        e = float(z[f"L{L}D{D}_energy"])
+        e0 = ed.ground_energy(L)
+        assert e0 <= e + 1e-10
+        assert e - e0 < 1e-2
