@@ -135,6 +135,50 @@ int mpsqmc_get_trace(mpsqmc_ctx *ctx, double *trace, int *n_walkers);
 int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms,
                        int *kernel_launches);
 
+/* ---------------------------------------------------------------------------------------------
+ * Local energies without any device allocation.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: code whose device memory is owned by someone else
+ * (a framework's caching allocator, a fixed arena handed over by the application) or that runs
+ * where allocating is not allowed.  The caller passes device pointers to its own inputs and
+ * outputs; the environment scratch the kernel needs lives in one file-scope device array of
+ * MPSQMC_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until the process
+ * exits.  The function calls no cudaMalloc, cudaFree or allocating library routine.
+ *
+ * Computes, for w < n_walkers, energies[w] = <Psi_T|H|phi_w> / overlaps[w] (the local energy of
+ * the walk) for H = sum_c J_c S_i.S_j - h sum_k S^z_k on a nearest-neighbour chain, on `stream`
+ * (a cudaStream_t, NULL = legacy default stream), asynchronously: results are valid once the
+ * stream has been synchronised.
+ *   trial:   device, reference layout for trial_dims;
+ *   walkers: device, walker w at walkers + w * walker_stride, reference layout for walker_dims;
+ *   overlaps, energies: device, n_walkers doubles each.
+ * Limits: L <= MPSQMC_NOALLOC_MAX_L, d = 2, and the environment scratch of one CTA,
+ * 8 * max(trial_dims) * max(walker_dims) doubles, must fit in the array; larger problems are
+ * rejected with MPSQMC_E_UNSUPPORTED and a message in mpsqmc_last_error().
+ * The first call on a device (with that device current) looks up the array's device address
+ * and raises the kernel's shared-memory limit; make that first call before any stream capture.
+ * Every call reuses the same array and leaves its contents behind; each call writes every
+ * scratch element before reading it.  Calls that overlap on the GPU (different streams, or
+ * different host threads without ordering) race on the array. */
+#define MPSQMC_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
+#define MPSQMC_NOALLOC_MAX_L 128
+
+typedef struct {
+  int L;                   /* chain length */
+  int d;                   /* local dimension (2) */
+  const int *trial_dims;   /* host [L+1] */
+  const int *walker_dims;  /* host [L+1] */
+  int nC;                  /* couplings (nearest-neighbour, ordered by site) */
+  const int *ci, *cj;      /* host [nC] */
+  const double *cJ;        /* host [nC] */
+  double h;                /* field */
+} mpsqmc_energy_layout;
+
+int mpsqmc_local_energy_noalloc(const mpsqmc_energy_layout *layout, const double *trial,
+                                const double *walkers, long walker_stride,
+                                const double *overlaps, int n_walkers, double *energies,
+                                int device, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

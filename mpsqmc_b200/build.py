@@ -37,7 +37,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    cmd = [nvcc, *NVCC_FLAGS, os.path.join(CSRC, "capi.cu"), "-o", LIB + ".tmp"]
+    units = [os.path.join(CSRC, f) for f in ("capi.cu", "noalloc.cu")]
+    cmd = [nvcc, *NVCC_FLAGS, *units, "-o", LIB + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

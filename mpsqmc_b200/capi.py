@@ -21,7 +21,7 @@ EXPORTED = [
     "mpsqmc_create", "mpsqmc_destroy", "mpsqmc_last_error", "mpsqmc_version", "mpsqmc_walker_size",
     "mpsqmc_set_walkers", "mpsqmc_get_walkers", "mpsqmc_set_rng", "mpsqmc_get_rng_draws",
     "mpsqmc_energy", "mpsqmc_walk", "mpsqmc_last_step_walkers", "mpsqmc_set_trace",
-    "mpsqmc_get_trace", "mpsqmc_last_timing",
+    "mpsqmc_get_trace", "mpsqmc_last_timing", "mpsqmc_local_energy_noalloc",
 ]
 
 
@@ -42,6 +42,15 @@ class Config(C.Structure):
         ("G", C.c_int), ("grid", C.POINTER(C.c_double)),
         ("Ndesired", C.c_int), ("capacity", C.c_int),
         ("walker_dims", C.POINTER(C.c_int)), ("device", C.c_int),
+    ]
+
+
+class EnergyLayout(C.Structure):
+    """mpsqmc_energy_layout: host-side description of the problem for the no-allocation entry point."""
+    _fields_ = [
+        ("L", C.c_int), ("d", C.c_int), ("trial_dims", C.POINTER(C.c_int)),
+        ("walker_dims", C.POINTER(C.c_int)), ("nC", C.c_int), ("ci", C.POINTER(C.c_int)),
+        ("cj", C.POINTER(C.c_int)), ("cJ", C.POINTER(C.c_double)), ("h", C.c_double),
     ]
 
 
@@ -90,6 +99,8 @@ def load(build_if_missing: bool = True):
         "mpsqmc_set_trace": (C.c_int, [P, C.c_int]),
         "mpsqmc_get_trace": (C.c_int, [P, dp, ip]),
         "mpsqmc_last_timing": (C.c_int, [P, dp, dp, ip]),
+        "mpsqmc_local_energy_noalloc": (C.c_int, [C.POINTER(EnergyLayout), P, P, C.c_long, P, C.c_int, P,
+                                                  C.c_int, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -210,3 +221,17 @@ class Engine:
         k, t, n = C.c_double(0), C.c_double(0), C.c_int(0)
         check(self.lib.mpsqmc_last_timing(self._ctx, C.byref(k), C.byref(t), C.byref(n)))
         return dict(step_kernel_ms=k.value, total_ms=t.value, launches=n.value)
+
+
+def local_energy_noalloc(*, L, trial_dims, walker_dims, ci, cj, cJ, h, trial_ptr, walkers_ptr, walker_stride,
+                         overlaps_ptr, n_walkers, energies_ptr, device=0, stream=None):
+    """Call mpsqmc_local_energy_noalloc on caller-owned device buffers (raw device addresses).
+
+    The call allocates nothing on the device; results are valid after the stream is synchronised."""
+    lib = load()
+    keep = [np.ascontiguousarray(a, dtype=t) for a, t in ((trial_dims, np.int32), (walker_dims, np.int32),
+                                                           (ci, np.int32), (cj, np.int32), (cJ, np.float64))]
+    lay = EnergyLayout(L=L, d=2, trial_dims=_ip(keep[0]), walker_dims=_ip(keep[1]), nC=len(keep[2]),
+                       ci=_ip(keep[2]), cj=_ip(keep[3]), cJ=_dp(keep[4]), h=h)
+    return lib.mpsqmc_local_energy_noalloc(C.byref(lay), trial_ptr, walkers_ptr, walker_stride, overlaps_ptr,
+                                           n_walkers, energies_ptr, device, stream)

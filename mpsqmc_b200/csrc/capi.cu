@@ -27,6 +27,15 @@ int fail(int code, const std::string &msg) {
   return code;
 }
 
+}  // namespace
+
+// Lets the other translation unit of the library (noalloc.cu) report through mpsqmc_last_error.
+namespace mq_host {
+__attribute__((visibility("hidden"))) void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace mq_host
+
+namespace {
+
 #define CK(call)                                                                             \
   do {                                                                                       \
     cudaError_t e_ = (call);                                                                 \

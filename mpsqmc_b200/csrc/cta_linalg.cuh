@@ -32,7 +32,7 @@ __device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double
 // Each warp owns 16x16 output blocks (2x2 DMMA tiles); element bounds are checked, so any
 // M, N, K >= 0 is valid.  Output element (m, n) is always written by the same thread for a
 // given (M, N), so two calls with the same M, N may accumulate into C without a barrier.
-__device__ __noinline__ void cta_gemm(int M, int N, int K, double alpha, const double *A, int lda,
+static __device__ __noinline__ void cta_gemm(int M, int N, int K, double alpha, const double *A, int lda,
                                       bool ta, const double *B, int ldb, bool tb, double beta,
                                       double *C, int ldc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -123,7 +123,7 @@ __device__ __forceinline__ double dlapy2(double x, double y) {
 // diagonal is zero or m - i == 1).  On exit A holds Q (m x n, orthonormal columns) and R
 // (n x n, ld ldr, upper triangular) holds the triangular factor.  tau, w: >= n doubles of
 // shared memory, red: >= kWarps doubles.  Ends with a barrier.
-__device__ __noinline__ void cta_householder_qr(int m, int n, double *A, int lda, double *R, int ldr,
+static __device__ __noinline__ void cta_householder_qr(int m, int n, double *A, int lda, double *R, int ldr,
                                                 double *tau, double *w, double *red) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ double s_scale;

@@ -132,7 +132,7 @@ __device__ __forceinline__ void store_site(double *dst, const double *src, int l
 //   Lenv (al x bl, ld pa) -> Lenv' = sum_s B[s]^T Lenv T[s]               (ar x br)
 //   Fcur[0..3] (done, Sx, iSy, Sz; ld maxA) -> Fnxt[0..3]
 // Bond coupling into the site: Jprev (0 if none).  first: Fcur is zero (site 0).
-__device__ void env_update(const Dev &p, Smem &s, const double *B, int al, int ar, int bl, int br,
+static __device__ void env_update(const Dev &p, Smem &s, const double *B, int al, int ar, int bl, int br,
                            const double *T, int cs, int ss, const double *Fcur, double *Fnxt,
                            double Jprev, bool first) {
   const int d = kMaxD, lda = p.maxA, fstride = p.maxA * p.maxB;
@@ -195,6 +195,10 @@ __device__ void env_update(const Dev &p, Smem &s, const double *B, int al, int a
     __syncthreads();
   }
 }
+
+// Translation units that only need the device helpers above define MQ_DEVICE_ONLY, so that
+// the kernels below are compiled once, in capi.cu.
+#ifndef MQ_DEVICE_ONLY
 
 // ---------------------------------------------------------------------------------------------
 // The walker-step kernel
@@ -860,5 +864,7 @@ __global__ void finish_branch_kernel(StepDev *sd, int *n_cur, int *slot_of, cons
     *n_cur = nn;
   }
 }
+
+#endif  // MQ_DEVICE_ONLY
 
 }  // namespace mq
