@@ -82,14 +82,14 @@ struct mpsqmc_ctx {
   int L = 0, d = 2, nC = 0, G = 0, nJ = 0, Ndesired = 0, capacity = 0;
   double dtau = 0.0, h = 0.0;
   std::vector<int> aT, bW;
-  std::vector<long> toff, woff, roff;
+  std::vector<long> toff, woff, roff, nroff;
   long wsize = 0, wstride = 0, scr_stride = 0, foff = 0;
   int maxA = 1, maxB = 1, pa = 4, pb = 4, pq = 4;
   size_t smem_bytes = 0;
   int sm_count = 1, max_ctas = 1;
   // device memory
   int *d_aT = nullptr, *d_bW = nullptr;
-  long *d_toff = nullptr, *d_woff = nullptr, *d_roff = nullptr;
+  long *d_toff = nullptr, *d_woff = nullptr, *d_roff = nullptr, *d_nroff = nullptr;
   double *d_trial = nullptr, *d_walkers = nullptr;
   int *d_slot_of = nullptr, *d_slot_new = nullptr, *d_free = nullptr, *d_copy_src = nullptr,
       *d_copy_dst = nullptr, *d_parent = nullptr, *d_flag_pos = nullptr, *d_ncur = nullptr;
@@ -157,6 +157,7 @@ mq::Dev make_dev(mpsqmc_ctx *c) {
   p.scratch = c->d_scratch;
   p.scr_stride = c->scr_stride;
   p.roff = c->d_roff;
+  p.nroff = c->d_nroff;
   p.foff = c->foff;
   p.trace = c->trace_on ? c->d_trace : nullptr;
   p.err = c->d_err;
@@ -176,7 +177,7 @@ int check_err(mpsqmc_ctx *c) {
 }
 
 void free_all(mpsqmc_ctx *c) {
-  void *ptrs[] = {c->d_aT, c->d_bW, c->d_toff, c->d_woff, c->d_roff, c->d_trial, c->d_walkers,
+  void *ptrs[] = {c->d_aT, c->d_bW, c->d_toff, c->d_woff, c->d_roff, c->d_nroff, c->d_trial, c->d_walkers,
                   c->d_slot_of, c->d_slot_new, c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
                   c->d_flag_pos, c->d_ncur, c->d_weight, c->d_overlap, c->d_ehist, c->d_energy,
                   c->d_ovout, c->d_wtout, c->d_sw, c->d_uni, c->d_ubr, c->d_bond_c, c->d_bond_j,
@@ -268,7 +269,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   c->wstride = (wo + 31) & ~31L;
   c->maxA = *std::max_element(c->aT.begin(), c->aT.end());
   c->maxB = *std::max_element(c->bW.begin(), c->bW.end());
-  c->pa = mq::padld(c->maxA);
+  c->pa = mq::padld(std::max(c->maxA, c->maxB));  // slots also hold walker-row matrices
   c->pb = mq::padld(c->maxB);
   c->pq = mq::padld(d * c->maxB);
   c->smem_bytes = sizeof(double) * (size_t)mq::smem_doubles(c->maxA, c->maxB, c->G, c->pa, c->pb, c->pq,
@@ -278,6 +279,11 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   for (int k = 0; k <= L; ++k) {
     c->roff[k] = ro;
     ro += ((long)c->aT[k] * c->bW[k] + 3) & ~3L;
+  }
+  c->nroff.resize(L + 1);
+  for (int k = 0; k <= L; ++k) {
+    c->nroff[k] = ro;
+    ro += ((long)c->bW[k] * c->bW[k] + 3) & ~3L;
   }
   c->foff = ro;
   c->scr_stride = ro + 2L * 4 * c->maxA * c->maxB;
@@ -316,7 +322,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   const int cap = c->capacity;
   int rc = 0;
   rc |= dalloc(&c->d_aT, L + 1) | dalloc(&c->d_bW, L + 1) | dalloc(&c->d_toff, L) | dalloc(&c->d_woff, L) |
-        dalloc(&c->d_roff, L + 1) | dalloc(&c->d_trial, to) | dalloc(&c->d_walkers, (size_t)cap * c->wstride) |
+        dalloc(&c->d_roff, L + 1) | dalloc(&c->d_nroff, L + 1) | dalloc(&c->d_trial, to) | dalloc(&c->d_walkers, (size_t)cap * c->wstride) |
         dalloc(&c->d_slot_of, cap) | dalloc(&c->d_slot_new, cap) | dalloc(&c->d_free, cap) |
         dalloc(&c->d_copy_src, cap) | dalloc(&c->d_copy_dst, cap) | dalloc(&c->d_parent, cap) |
         dalloc(&c->d_flag_pos, cap) | dalloc(&c->d_ncur, 1) | dalloc(&c->d_weight, cap) |
@@ -334,6 +340,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   bool ok = up(c->d_aT, c->aT.data(), sizeof(int) * (L + 1)) && up(c->d_bW, c->bW.data(), sizeof(int) * (L + 1)) &&
             up(c->d_toff, c->toff.data(), sizeof(long) * L) && up(c->d_woff, c->woff.data(), sizeof(long) * L) &&
             up(c->d_roff, c->roff.data(), sizeof(long) * (L + 1)) &&
+            up(c->d_nroff, c->nroff.data(), sizeof(long) * (L + 1)) &&
             up(c->d_trial, cfg->trial, sizeof(double) * to) &&
             up(c->d_bond_c, bond_c.data(), sizeof(int) * (L - 1)) &&
             up(c->d_bond_j, bond_j.data(), sizeof(int) * (L - 1)) &&

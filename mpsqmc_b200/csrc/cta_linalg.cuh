@@ -26,15 +26,94 @@ __device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double
       : "d"(a), "d"(b));
 }
 
+// Check-free path for M, N, K multiples of 16: each warp computes 16x16 blocks; the K loop runs
+// in chunks of four k-steps whose 16 fragment loads are issued one chunk ahead of the DMMAs.
+template <bool TA, bool TB>
+static __device__ __forceinline__ void gemm16(int M, int N, int K, double alpha, const double *A, int lda,
+                                              const double *B, int ldb, double beta, double *C, int ldc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int bm = M >> 4, bn = N >> 4;
+  const long sa = TA ? 4 : 4L * lda, sb = TB ? 4L * ldb : 4;
+  for (int blk = warp; blk < bm * bn; blk += kWarps) {
+    const int m0 = (blk % bm) << 4, n0 = (blk / bm) << 4;
+    const int ma = m0 + g, mb = m0 + 8 + g, na = n0 + g, nb = n0 + 8 + g;
+    const double *pa0 = TA ? A + (long)lda * ma + t : A + ma + (long)lda * t;
+    const double *pa1 = TA ? A + (long)lda * mb + t : A + mb + (long)lda * t;
+    const double *pb0 = TB ? B + na + (long)ldb * t : B + t + (long)ldb * na;
+    const double *pb1 = TB ? B + nb + (long)ldb * t : B + t + (long)ldb * nb;
+    double acc[2][2][2] = {{{0.0, 0.0}, {0.0, 0.0}}, {{0.0, 0.0}, {0.0, 0.0}}};
+    double a0[4], a1[4], b0[4], b1[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a0[u] = pa0[u * sa];
+      a1[u] = pa1[u * sa];
+      b0[u] = pb0[u * sb];
+      b1[u] = pb1[u * sb];
+    }
+    for (int k0 = 0; k0 < K; k0 += 16) {
+      double c0[4], c1[4], d0[4], d1[4];
+      const bool more = k0 + 16 < K;
+      const long off = (long)(k0 / 4 + 4);
+      if (more) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          c0[u] = pa0[(off + u) * sa];
+          c1[u] = pa1[(off + u) * sa];
+          d0[u] = pb0[(off + u) * sb];
+          d1[u] = pb1[(off + u) * sb];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        dmma884(acc[0][0][0], acc[0][0][1], a0[u], b0[u]);
+        dmma884(acc[0][1][0], acc[0][1][1], a0[u], b1[u]);
+        dmma884(acc[1][0][0], acc[1][0][1], a1[u], b0[u]);
+        dmma884(acc[1][1][0], acc[1][1][1], a1[u], b1[u]);
+      }
+      if (more) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          a0[u] = c0[u];
+          a1[u] = c1[u];
+          b0[u] = d0[u];
+          b1[u] = d1[u];
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          double *c = C + (m0 + 8 * i + g) + (long)ldc * (n0 + 8 * j + 2 * t + e);
+          const double v = alpha * acc[i][j][e];
+          *c = (beta == 0.0) ? v : v + beta * (*c);
+        }
+  }
+}
+
 // C (M x N, ldc) = alpha * op(A) * op(B) + beta * C, op(A) M x K, op(B) K x N.
 //   ta == false: A[m + lda*k];  ta == true: A[k + lda*m]
 //   tb == false: B[k + ldb*n];  tb == true: B[n + ldb*k]
-// Each warp owns 16x16 output blocks (2x2 DMMA tiles); element bounds are checked, so any
-// M, N, K >= 0 is valid.  Output element (m, n) is always written by the same thread for a
-// given (M, N), so two calls with the same M, N may accumulate into C without a barrier.
+// Each warp owns 16x16 output blocks (2x2 DMMA tiles).  When M, N and K are multiples of 16 the
+// check-free gemm16 path runs; otherwise element bounds are checked, so any M, N, K >= 0 is
+// valid.  Output element (m, n) is always written by the same thread for a given (M, N), so two
+// calls with the same M, N may accumulate into C without a barrier.
 static __device__ __noinline__ void cta_gemm(int M, int N, int K, double alpha, const double *A, int lda,
                                       bool ta, const double *B, int ldb, bool tb, double beta,
                                       double *C, int ldc) {
+  if (((M | N | K) & 15) == 0) {
+    if (ta) {
+      if (tb) gemm16<true, true>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+      else gemm16<true, false>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    } else {
+      if (tb) gemm16<false, true>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+      else gemm16<false, false>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    }
+    return;
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int bm = (M + 15) >> 4, bn = (N + 15) >> 4;
@@ -121,87 +200,91 @@ __device__ __forceinline__ double dlapy2(double x, double y) {
 // Householder QR of A (m x n, m >= n, ld lda, shared memory) in LAPACK's conventions
 // (dgeqr2 + dorg2r, with dlarfg's beta = -sign(alpha)*||x||, tau = 0 when the column below the
 // diagonal is zero or m - i == 1).  On exit A holds Q (m x n, orthonormal columns) and R
-// (n x n, ld ldr, upper triangular) holds the triangular factor.  tau, w: >= n doubles of
-// shared memory, red: >= kWarps doubles.  Ends with a barrier.
+// (n x n, ld ldr, upper triangular) holds the triangular factor.  tau: >= n doubles of shared
+// memory; w and red are not used.  Starts and ends with a barrier.
+//
+// Column j belongs to warp j % kWarps for the whole factorisation: the owner builds reflector j
+// and every warp applies published reflectors to its own columns, so one barrier per column
+// and pass is enough (a warp updates its columns in program order).
 static __device__ __noinline__ void cta_householder_qr(int m, int n, double *A, int lda, double *R, int ldr,
                                                 double *tau, double *w, double *red) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  __shared__ double s_scale;
+  (void)w;
+  (void)red;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned full = 0xffffffffu;
+  __syncthreads();
+  // dgeqr2
   for (int i = 0; i < n; ++i) {
     double *col = A + (long)lda * i;
-    double part = 0.0;
-    for (int r = i + 1 + tid; r < m; r += kThreads) part += col[r] * col[r];
-    const double ss = cta_sum(part, red);
-    if (tid == 0) {
-      double ti = 0.0, sc = 1.0;
-      if (m - i > 1 && ss > 0.0) {
-        const double alpha = col[i];
-        const double mag = dlapy2(alpha, sqrt(ss));
+    if (warp == i % kWarps) {
+      double part = 0.0;
+      for (int r = i + 1 + lane; r < m; r += 32) part += col[r] * col[r];
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(full, part, o);
+      const double alpha = col[i];
+      double ti = 0.0;
+      if (m - i > 1 && part > 0.0) {
+        const double mag = dlapy2(alpha, sqrt(part));
         const double beta = (alpha >= 0.0) ? -mag : mag;
         ti = (beta - alpha) / beta;
-        sc = 1.0 / (alpha - beta);
-        col[i] = beta;
+        const double sc = 1.0 / (alpha - beta);
+        for (int r = i + 1 + lane; r < m; r += 32) col[r] *= sc;
+        __syncwarp();
+        if (lane == 0) col[i] = beta;
       }
-      tau[i] = ti;
-      s_scale = sc;
+      if (lane == 0) tau[i] = ti;
     }
     __syncthreads();
     const double ti = tau[i];
     if (ti != 0.0) {
-      const double sc = s_scale;
-      for (int r = i + 1 + tid; r < m; r += kThreads) col[r] *= sc;
-      __syncthreads();
-      // w_j = v^T A(i:m, j), v = (1, col[i+1..m))
-      for (int j = i + 1 + warp; j < n; j += kWarps) {
-        const double *cj = A + (long)lda * j;
+      const int first = i + 1 + (((warp - (i + 1)) % kWarps) + kWarps) % kWarps;
+      for (int j = first; j < n; j += kWarps) {
+        double *cj = A + (long)lda * j;
+        const double head = cj[i];
         double s = 0.0;
         for (int r = i + 1 + lane; r < m; r += 32) s += col[r] * cj[r];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) w[j] = s + cj[i];
-      }
-      __syncthreads();
-      const int rows = m - i, cols = n - i - 1;
-      for (int q = tid; q < rows * cols; q += kThreads) {
-        const int r = i + q % rows, j = i + 1 + q / rows;
-        const double v = (r == i) ? 1.0 : col[r];
-        A[r + (long)lda * j] -= ti * v * w[j];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(full, s, o);
+        const double f = ti * (s + head);
+        for (int r = i + 1 + lane; r < m; r += 32) cj[r] -= f * col[r];
+        if (lane == 0) cj[i] = head - f;
+        __syncwarp();
       }
     }
-    __syncthreads();
   }
-  for (int q = tid; q < n * n; q += kThreads) {
+  __syncthreads();
+  for (int q = threadIdx.x; q < n * n; q += kThreads) {
     const int r = q % n, c = q / n;
     R[r + (long)ldr * c] = (r <= c) ? A[r + (long)lda * c] : 0.0;
   }
   __syncthreads();
-  // dorg2r, k = n
+  // dorg2r, k = n: Q = H_0 ... H_{n-1} applied to the first n unit columns
   for (int i = n - 1; i >= 0; --i) {
-    double *col = A + (long)lda * i;
+    const double *col = A + (long)lda * i;
     const double ti = tau[i];
-    if (i < n - 1 && ti != 0.0) {
-      for (int j = i + 1 + warp; j < n; j += kWarps) {
-        const double *cj = A + (long)lda * j;
+    if (ti != 0.0 && i < n - 1) {
+      const int first = i + 1 + (((warp - (i + 1)) % kWarps) + kWarps) % kWarps;
+      for (int j = first; j < n; j += kWarps) {
+        double *cj = A + (long)lda * j;
+        const double head = cj[i];
         double s = 0.0;
         for (int r = i + 1 + lane; r < m; r += 32) s += col[r] * cj[r];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) w[j] = s + cj[i];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(full, s, o);
+        const double f = ti * (s + head);
+        for (int r = i + 1 + lane; r < m; r += 32) cj[r] -= f * col[r];
+        if (lane == 0) cj[i] = head - f;
+        __syncwarp();
       }
-      __syncthreads();
-      const int rows = m - i, cols = n - i - 1;
-      for (int q = tid; q < rows * cols; q += kThreads) {
-        const int r = i + q % rows, j = i + 1 + q / rows;
-        const double v = (r == i) ? 1.0 : col[r];
-        A[r + (long)lda * j] -= ti * v * w[j];
-      }
-      __syncthreads();
-    }
-    for (int r = tid; r < m; r += kThreads) {
-      if (r > i) col[r] *= -ti;
-      else if (r == i) col[r] = 1.0 - ti;
-      else col[r] = 0.0;
     }
     __syncthreads();
+    if (warp == i % kWarps) {
+      double *ci = A + (long)lda * i;
+      for (int r = lane; r < m; r += 32) {
+        if (r > i) ci[r] *= -ti;
+        else if (r == i) ci[r] = 1.0 - ti;
+        else ci[r] = 0.0;
+      }
+    }
   }
+  __syncthreads();
 }
 
 }  // namespace mq

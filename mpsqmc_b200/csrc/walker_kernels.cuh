@@ -3,16 +3,16 @@
 // One CTA owns one walker at a time (persistent grid striding over walkers) and runs the whole
 // timestep of MPSQMC2::PropagateSeparately (MPSQMC2.cpp:518-611) for it:
 //
-//   phase A  right sweep (LQ, site L-1 .. 1): right-canonical form with the orthogonality centre
-//            on site 0, right environments R[k] = <Psi_T|phi> contracted over sites k..L-1,
-//            overlap and sign fix (Walker::setOverlap, Walker.cpp:54-66, at MPSQMC2.cpp:534);
+//   phase A  right environments (site L-1 .. 1) of the walker as stored: R[k] = <Psi_T|phi> and
+//            N[k] = <phi|phi> contracted over sites k..L-1; overlap, norm and sign fix with the
+//            centre on site 0 (Walker::setOverlap, Walker.cpp:54-66, at MPSQMC2.cpp:534);
 //   phase B  left-to-right sweep over the bonds.  For a bond (i, i+1) that carries a coupling:
 //            the 16 numbers C_kl = <Psi_T|(sqrt(s_k)U_k)_i (sqrt(s_l)V_l)_j|phi> from the left
 //            environment, 4 left branches, 4 right branches and 16 closures (the reference gets
 //            them from 16 full-chain InnerProducts against stored trial copies, 540-549); the
 //            grid PDF, weight update and CDF sample (551-588); the auxiliary-field site
 //            operators (MPSstate.cpp:575-633); renormalisation and new overlap (592).  The centre
-//            then moves to i+1 by one Householder QR.  Compact-MPO left environments built from
+//            moves to i+1 by one Householder QR; the new norm closes against N[i+2].  Compact-MPO left environments built from
 //            the final site tensors give <Psi_T|H|phi> at the end of the sweep, i.e. the local
 //            energy of Walker::calcIndividualProjectedEnergy (Walker.cpp:72-77).
 //
@@ -58,6 +58,7 @@ struct Dev {
   double *scratch;     // per-CTA global scratch
   long scr_stride;
   const long *roff;    // right-environment offsets [L+1] inside a CTA's scratch
+  const long *nroff;   // norm-environment offsets [L+1] inside a CTA's scratch
   long foff;           // compact-MPO environments (2 x 4 x maxA*maxB) inside the scratch
   double *trace;       // optional [N][nC][kTraceStride]
   int *err;            // device error word (bit flags)
@@ -215,72 +216,63 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
   for (int w = blockIdx.x; w < N; w += gridDim.x) {
     const int slot = p.slot_of[w];
     double *W = p.walkers + (long)slot * p.wstride;
-    // ---------------- phase A: right sweep --------------------------------------------------
+    // ---------------- phase A: right environments ------------------------------------------
+    // The walker is read as stored (between steps: left-canonical).  For k = L-1 .. 1:
+    //   R[k] = sum_s B_k[s] R[k+1] A_k[s]^T        (a_k x b_k, trial-walker overlap)
+    //   N[k] = sum_s A_k[s] N[k+1] A_k[s]^T        (b_k x b_k, walker norm)
+    // so that <Psi_T|phi> and ||phi||^2 of any state that differs from phi only on sites < k
+    // close against R[k] and N[k].  Then the centre is site 0: normalise, overlap, sign fix
+    // (Walker::setOverlap at MPSQMC2.cpp:534).
     {
-      double *R = scr + p.roff[L];
-      if (tid == 0) R[0] = 1.0;
-      load_site(s.Cen, p.pb, s.sbC, W + p.woff[L - 1], p.bW[L - 1], p.bW[L]);
-      __syncthreads();
+      if (tid == 0) {
+        scr[p.roff[L]] = 1.0;
+        scr[p.nroff[L]] = 1.0;
+      }
       for (int k = L - 1; k >= 1; --k) {
         const int al = p.aT[k], ar = p.aT[k + 1], bl = p.bW[k], br = p.bW[k + 1];
-        const int bll = p.bW[k - 1];
-        // LQ of the centre (bl x br*d) through QR of its transpose (br*d x bl)
-        for (int q = tid; q < bl * br * d; q += kThreads) {
-          const int r = q % bl, rest = q / bl, c = rest % br, sg = rest / br;
-          s.QRb[(c + br * sg) + p.pq * r] = s.Cen[sg * s.sbC + r + p.pb * c];
-        }
+        load_site(s.Nxt, p.pb, s.sbC, W + p.woff[k], bl, br);
         __syncthreads();
-        cta_householder_qr(br * d, bl, s.QRb, p.pq, s.Rf, p.pb, s.tau, s.wv, s.red);
-        // site k <- Q'^T : A_k[sg](r, c) = Q'(c + br*sg, r)
-        double *Wk = W + p.woff[k];
-        for (int q = tid; q < bl * br * d; q += kThreads) {
-          const int r = q % bl, rest = q / bl, c = rest % br, sg = rest / br;
-          Wk[q] = s.QRb[(c + br * sg) + p.pq * r];
-        }
-        // R[k] = sum_s B_k[s] (R[k+1] Q_k[s]^T)       (al x bl)
-        const double *Rn = scr + p.roff[k + 1];
-        double *Rk = scr + p.roff[k];
+        const double *Rn = scr + p.roff[k + 1], *Nn = scr + p.nroff[k + 1];
+        double *Rk = scr + p.roff[k], *Nk = scr + p.nroff[k];
         const double *Bk = p.trial + p.toff[k];
-        for (int sg = 0; sg < d; ++sg)
-          cta_gemm(ar, bl, br, 1.0, Rn, ar, false, s.QRb + br * sg, p.pq, false, 0.0,
+        for (int sg = 0; sg < d; ++sg) {
+          // Y[s] = R[k+1] A_k[s]^T (ar x bl),  Z[s] = N[k+1] A_k[s]^T (br x bl)
+          cta_gemm(ar, bl, br, 1.0, Rn, ar, false, s.Nxt + sg * s.sbC, p.pb, true, 0.0,
                    s.Xb + sg * s.sbX, p.pa);
-        // next centre: A_{k-1}[s] * R'^T   (bll x bl)
-        load_site(s.Nxt, p.pb, s.sbC, W + p.woff[k - 1], bll, bl);
+          cta_gemm(br, bl, br, 1.0, Nn, br, false, s.Nxt + sg * s.sbC, p.pb, true, 0.0,
+                   s.Pb + sg * s.sbX, p.pa);
+        }
         __syncthreads();
-        cta_gemm(al, bl, ar, 1.0, Bk, al, false, s.Xb, p.pa, false, 0.0, Rk, al);
-        for (int sg = 1; sg < d; ++sg)
-          cta_gemm(al, bl, ar, 1.0, Bk + (long)sg * al * ar, al, false, s.Xb + sg * s.sbX, p.pa,
-                   false, 1.0, Rk, al);
-        for (int sg = 0; sg < d; ++sg)
-          cta_gemm(bll, bl, bl, 1.0, s.Nxt + sg * s.sbC, p.pb, false, s.Rf, p.pb, true, 0.0,
-                   s.Cen + sg * s.sbC, p.pb);
+        for (int sg = 0; sg < d; ++sg) {
+          cta_gemm(al, bl, ar, 1.0, Bk + (long)sg * al * ar, al, false, s.Xb + sg * s.sbX, p.pa, false,
+                   sg == 0 ? 0.0 : 1.0, Rk, al);
+          cta_gemm(bl, bl, br, 1.0, s.Nxt + sg * s.sbC, p.pb, false, s.Pb + sg * s.sbX, p.pa, false,
+                   sg == 0 ? 0.0 : 1.0, Nk, bl);
+        }
         __syncthreads();
       }
-      // centre on site 0 (1 x b1): normalise, overlap with R[1], sign fix
+      // centre = site 0 (1 x b1): ||phi||^2 = sum_s C[s] N[1] C[s]^T, ov = sum_s B_0[s] R[1] C[s]^T
       {
         const int a1 = p.aT[1], b1 = p.bW[1];
-        double part = 0.0;
-        for (int q = tid; q < b1 * d; q += kThreads) {
-          const double v = s.Cen[(q / b1) * s.sbC + p.pb * (q % b1)];
-          part += v * v;
-        }
-        const double nrm = sqrt(cta_sum(part, s.red));
-        const double inv = 1.0 / nrm;
-        for (int q = tid; q < b1 * d; q += kThreads) s.Cen[(q / b1) * s.sbC + p.pb * (q % b1)] *= inv;
+        load_site(s.Cen, p.pb, s.sbC, W + p.woff[0], 1, b1);
         __syncthreads();
-        // ov = sum_s B_0[s] (1 x a1) R[1] (a1 x b1) C[s]^T (b1 x 1)
-        const double *R1 = scr + p.roff[1];
+        const double *R1 = scr + p.roff[1], *N1 = scr + p.nroff[1];
         const double *B0 = p.trial + p.toff[0];
-        part = 0.0;
+        double v2[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int q = tid; q < b1 * b1 * d; q += kThreads) {
+          const int a = q % b1, rest = q / b1, b = rest % b1, sg = rest / b1;
+          v2[0] += s.Cen[sg * s.sbC + p.pb * a] * N1[a + b1 * b] * s.Cen[sg * s.sbC + p.pb * b];
+        }
         for (int q = tid; q < a1 * b1 * d; q += kThreads) {
           const int a = q % a1, rest = q / a1, b = rest % b1, sg = rest / b1;
-          part += B0[a + a1 * sg] * R1[a + a1 * b] * s.Cen[sg * s.sbC + p.pb * b];
+          v2[1] += B0[a + a1 * sg] * R1[a + a1 * b] * s.Cen[sg * s.sbC + p.pb * b];
         }
-        double ov = cta_sum(part, s.red);
-        if (ov < 0.0) {  // ChangePhase on site 0 (MPSstate.cpp:307-315)
-          for (int q = tid; q < b1 * d; q += kThreads) s.Cen[(q / b1) * s.sbC + p.pb * (q % b1)] *= -1.0;
-          ov = -ov;
-        }
+        cta_sum4(v2, s.red);
+        const double nrm = sqrt(v2[0]);
+        double ov = v2[1] / nrm;
+        const double scale = (ov < 0.0) ? -1.0 / nrm : 1.0 / nrm;  // ChangePhase, MPSstate.cpp:307-315
+        if (ov < 0.0) ov = -ov;
+        for (int q = tid; q < b1 * d; q += kThreads) s.Cen[(q / b1) * s.sbC + p.pb * (q % b1)] *= scale;
         if (tid == 0) s.sc[0] = ov;
         __syncthreads();
       }
@@ -432,11 +424,16 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
       }
       __syncthreads();
       if (c >= 0) {
+        // ||B(x) phi||^2 = sum_s tr(C[s] N[i+2] C[s]^T): sites < i+1 are orthonormal now
+        const double *N2 = scr + p.nroff[i + 2];
+        for (int sg = 0; sg < d; ++sg)
+          cta_gemm(br, b2, b2, 1.0, s.Cen + sg * s.sbC, p.pb, false, N2, b2, false, 0.0, s.Xb + sg * s.sbX,
+                   p.pa);
+        __syncthreads();
         double part = 0.0;
         for (int q = tid; q < br * b2 * d; q += kThreads) {
           const int r = q % br, rest = q / br, cc = rest % b2, sg = rest / b2;
-          const double v = s.Cen[sg * s.sbC + r + p.pb * cc];
-          part += v * v;
+          part += s.Cen[sg * s.sbC + r + p.pb * cc] * s.Xb[sg * s.sbX + r + p.pa * cc];
         }
         const double nrm = sqrt(cta_sum(part, s.red));
         ov = num / nrm;
