@@ -197,6 +197,213 @@ __device__ __forceinline__ double dlapy2(double x, double y) {
   return w * sqrt(1.0 + r * r);
 }
 
+// Apply H = I - tau v v^T (v = (1, col[i+1..m)) stored below the diagonal of column i) to the
+// columns j > i that this warp owns (j = warp mod kWarps), all of them at once: partial dot
+// products for every owned column first, then one interleaved butterfly, then the updates.
+// MAXC bounds the owned columns (n <= MAXC * kWarps).
+template <int MAXC>
+static __device__ __forceinline__ void warp_apply_reflector(int m, int n, int i, const double *col,
+                                                            double tau, double *A, int lda) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int first = i + 1 + (((warp - (i + 1)) % kWarps) + kWarps) % kWarps;
+  double part[MAXC], head[MAXC];
+#pragma unroll
+  for (int c = 0; c < MAXC; ++c) {
+    const int j = first + c * kWarps;
+    part[c] = 0.0;
+    head[c] = 0.0;
+    if (j < n) {
+      const double *cj = A + (long)lda * j;
+      head[c] = cj[i];
+      for (int r = i + 1 + lane; r < m; r += 32) part[c] += col[r] * cj[r];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) part[c] += __shfl_xor_sync(0xffffffffu, part[c], o);
+#pragma unroll
+  for (int c = 0; c < MAXC; ++c) {
+    const int j = first + c * kWarps;
+    if (j < n) {
+      double *cj = A + (long)lda * j;
+      const double f = tau * (part[c] + head[c]);
+      for (int r = i + 1 + lane; r < m; r += 32) cj[r] -= f * col[r];
+      if (lane == 0) cj[i] = head[c] - f;
+    }
+  }
+  __syncwarp();
+}
+
+// Register-resident Householder QR (same conventions and results as cta_householder_qr below).
+// Column j belongs to warp j % kWarps; the warp keeps rows lane + 32*q (q < RPL) of its columns
+// (at most MAXC of them) in registers for the whole factorisation, so updates never go through
+// shared memory.  Reflector vectors are published in A below the diagonal (and tau[]), one
+// barrier per column in the factorisation; forming Q reads the published reflectors only and
+// needs no barrier.  Requires m <= 32*RPL and n <= kWarps*MAXC.
+template <int RPL, int MAXC>
+static __device__ __noinline__ void cta_qr_reg(int m, int n, double *__restrict__ A, int lda,
+                                               double *__restrict__ R, int ldr, double *__restrict__ tau) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned full = 0xffffffffu;
+  double x[MAXC][RPL];
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < MAXC; ++c) {
+    const int j = warp + c * kWarps;
+#pragma unroll
+    for (int q = 0; q < RPL; ++q) {
+      const int r = lane + 32 * q;
+      x[c][q] = (j < n && r < m) ? A[r + (long)lda * j] : 0.0;
+    }
+  }
+  // dgeqr2
+  for (int i = 0; i < n; ++i) {
+    const int ci = i / kWarps;  // slot of column i in its owner's registers
+    if (warp == i % kWarps) {
+      double part = 0.0, alpha = 0.0;
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c)
+        if (c == ci) {
+#pragma unroll
+          for (int q = 0; q < RPL; ++q) {
+            const int r = lane + 32 * q;
+            if (r > i && r < m) part += x[c][q] * x[c][q];
+            if (r == i) alpha = x[c][q];
+          }
+        }
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(full, part, o);
+      alpha = __shfl_sync(full, alpha, i & 31);
+      double ti = 0.0, beta = alpha, sc = 1.0;
+      if (m - i > 1 && part > 0.0) {
+        const double mag = dlapy2(alpha, sqrt(part));
+        beta = (alpha >= 0.0) ? -mag : mag;
+        ti = (beta - alpha) / beta;
+        sc = 1.0 / (alpha - beta);
+      }
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c)
+        if (c == ci) {
+#pragma unroll
+          for (int q = 0; q < RPL; ++q) {
+            const int r = lane + 32 * q;
+            if (r > i && r < m) {
+              if (ti != 0.0) x[c][q] *= sc;
+              A[r + (long)lda * i] = x[c][q];  // published reflector below the diagonal
+            }
+            if (r == i) x[c][q] = beta;
+          }
+        }
+      if (lane == 0) tau[i] = ti;
+    }
+    __syncthreads();
+    const double ti = tau[i];
+    if (ti != 0.0) {
+      double v[RPL];
+#pragma unroll
+      for (int q = 0; q < RPL; ++q) {
+        const int r = lane + 32 * q;
+        v[q] = (r > i && r < m) ? A[r + (long)lda * i] : (r == i ? 1.0 : 0.0);
+      }
+      double part[MAXC];
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) {
+        part[c] = 0.0;
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) part[c] += v[q] * x[c][q];
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c) part[c] += __shfl_xor_sync(full, part[c], o);
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) {
+        const int j = warp + c * kWarps;
+        if (j > i && j < n) {
+          const double f = ti * part[c];
+#pragma unroll
+          for (int q = 0; q < RPL; ++q) x[c][q] -= f * v[q];
+        }
+      }
+    }
+  }
+  // R: upper triangle of the reduced columns
+#pragma unroll
+  for (int c = 0; c < MAXC; ++c) {
+    const int j = warp + c * kWarps;
+    if (j < n) {
+#pragma unroll
+      for (int q = 0; q < RPL; ++q) {
+        const int r = lane + 32 * q;
+        if (r < n) R[r + (long)ldr * j] = (r <= j) ? x[c][q] : 0.0;
+      }
+    }
+  }
+  // dorg2r: columns start as unit vectors, H_i applied for i = n-1 .. 0
+#pragma unroll
+  for (int c = 0; c < MAXC; ++c) {
+    const int j = warp + c * kWarps;
+#pragma unroll
+    for (int q = 0; q < RPL; ++q) x[c][q] = (lane + 32 * q == j) ? 1.0 : 0.0;
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    const double ti = tau[i];
+    double v[RPL];
+#pragma unroll
+    for (int q = 0; q < RPL; ++q) {
+      const int r = lane + 32 * q;
+      v[q] = (r > i && r < m) ? A[r + (long)lda * i] : (r == i ? 1.0 : 0.0);
+    }
+    if (ti != 0.0) {
+      double part[MAXC];
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) {
+        part[c] = 0.0;
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) part[c] += v[q] * x[c][q];
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c) part[c] += __shfl_xor_sync(full, part[c], o);
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) {
+        const int j = warp + c * kWarps;
+        if (j > i && j < n) {
+          const double f = ti * part[c];
+#pragma unroll
+          for (int q = 0; q < RPL; ++q) x[c][q] -= f * v[q];
+        }
+      }
+    }
+    // column i := H_i e_i
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) {
+      const int j = warp + c * kWarps;
+      if (j == i) {
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+          const int r = lane + 32 * q;
+          x[c][q] = (r > i) ? -ti * v[q] : (r == i ? 1.0 - ti : 0.0);
+        }
+      }
+    }
+  }
+  __syncthreads();  // every warp has read the published reflectors
+#pragma unroll
+  for (int c = 0; c < MAXC; ++c) {
+    const int j = warp + c * kWarps;
+    if (j < n) {
+#pragma unroll
+      for (int q = 0; q < RPL; ++q) {
+        const int r = lane + 32 * q;
+        if (r < m) A[r + (long)lda * j] = x[c][q];
+      }
+    }
+  }
+  __syncthreads();
+}
+
 // Householder QR of A (m x n, m >= n, ld lda, shared memory) in LAPACK's conventions
 // (dgeqr2 + dorg2r, with dlarfg's beta = -sign(alpha)*||x||, tau = 0 when the column below the
 // diagonal is zero or m - i == 1).  On exit A holds Q (m x n, orthonormal columns) and R
@@ -210,6 +417,14 @@ static __device__ __noinline__ void cta_householder_qr(int m, int n, double *A, 
                                                 double *tau, double *w, double *red) {
   (void)w;
   (void)red;
+  if (m <= 64 && n <= 4 * kWarps) {
+    cta_qr_reg<2, 4>(m, n, A, lda, R, ldr, tau);
+    return;
+  }
+  if (m <= 128 && n <= 8 * kWarps) {
+    cta_qr_reg<4, 8>(m, n, A, lda, R, ldr, tau);
+    return;
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned full = 0xffffffffu;
   __syncthreads();
@@ -236,18 +451,8 @@ static __device__ __noinline__ void cta_householder_qr(int m, int n, double *A, 
     __syncthreads();
     const double ti = tau[i];
     if (ti != 0.0) {
-      const int first = i + 1 + (((warp - (i + 1)) % kWarps) + kWarps) % kWarps;
-      for (int j = first; j < n; j += kWarps) {
-        double *cj = A + (long)lda * j;
-        const double head = cj[i];
-        double s = 0.0;
-        for (int r = i + 1 + lane; r < m; r += 32) s += col[r] * cj[r];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(full, s, o);
-        const double f = ti * (s + head);
-        for (int r = i + 1 + lane; r < m; r += 32) cj[r] -= f * col[r];
-        if (lane == 0) cj[i] = head - f;
-        __syncwarp();
-      }
+      if (n <= 4 * kWarps) warp_apply_reflector<4>(m, n, i, col, ti, A, lda);
+      else warp_apply_reflector<8>(m, n, i, col, ti, A, lda);
     }
   }
   __syncthreads();
@@ -261,18 +466,8 @@ static __device__ __noinline__ void cta_householder_qr(int m, int n, double *A, 
     const double *col = A + (long)lda * i;
     const double ti = tau[i];
     if (ti != 0.0 && i < n - 1) {
-      const int first = i + 1 + (((warp - (i + 1)) % kWarps) + kWarps) % kWarps;
-      for (int j = first; j < n; j += kWarps) {
-        double *cj = A + (long)lda * j;
-        const double head = cj[i];
-        double s = 0.0;
-        for (int r = i + 1 + lane; r < m; r += 32) s += col[r] * cj[r];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(full, s, o);
-        const double f = ti * (s + head);
-        for (int r = i + 1 + lane; r < m; r += 32) cj[r] -= f * col[r];
-        if (lane == 0) cj[i] = head - f;
-        __syncwarp();
-      }
+      if (n <= 4 * kWarps) warp_apply_reflector<4>(m, n, i, col, ti, A, lda);
+      else warp_apply_reflector<8>(m, n, i, col, ti, A, lda);
     }
     __syncthreads();
     if (warp == i % kWarps) {
