@@ -154,6 +154,7 @@ mq::Dev make_dev(mpsqmc_ctx *c) {
     p.opSz[k] = c->opSz[k];
   }
   p.h = c->h;
+  for (int sg = 0; sg < mq::kMaxD; ++sg) p.onesite[sg] = std::exp(0.5 * c->h * c->dtau * op_sz(c->d, sg, sg));
   p.scratch = c->d_scratch;
   p.scr_stride = c->scr_stride;
   p.roff = c->d_roff;
@@ -490,10 +491,24 @@ int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
     const int step = ++c->step_count;
     mq::Dev p = make_dev(c);
     mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, c->d_ncur, 0, c->nC, c->d_uni);
+    const bool field = c->h != 0.0;
+    if (field) {  // single-site propagator before the couplings (MPSQMC2.cpp:533)
+      mq::onesite_kernel<<<grid_for(c, N), 256, 0, c->stream>>>(p);
+      launches += 1;
+    }
     CK(cudaEventRecord(c->ev[0], c->stream));
     mq::walker_step_kernel<<<grid_for(c, N), mq::kThreads, c->smem_bytes, c->stream>>>(p);
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev[1], c->stream));
+    if (field) {
+      // single-site propagator after the couplings, setOverlap, and the local energy of the
+      // resulting state (MPSQMC2.cpp:597-598, then 698)
+      mq::onesite_kernel<<<grid_for(c, N), 256, 0, c->stream>>>(p);
+      mq::set_overlap_kernel<<<grid_for(c, N), mq::kThreads, c->smem_bytes, c->stream>>>(p);
+      mq::energy_kernel<<<grid_for(c, N), mq::kThreads, c->smem_bytes, c->stream>>>(p);
+      CK(cudaGetLastError());
+      launches += 3;
+    }
     mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, step, 1, c->d_flag_pos, c->d_sw);
     mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, &c->d_sd->n_flag, 0, 1, c->d_ubr);
     mq::branch_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->d_flag_pos, c->d_sw, c->d_ubr, c->d_slot_new,

@@ -55,6 +55,7 @@ struct Dev {
   const double *grid;  // [G][4]
   double opSx[4], opISy[4], opSz[4];  // [sigma + d*tau]
   double h;
+  double onesite[kMaxD];  // diagonal of exp(0.5 h dtau S^z) (TrotterHeisenberg.cpp:80-88)
   double *scratch;     // per-CTA global scratch
   long scr_stride;
   const long *roff;    // right-environment offsets [L+1] inside a CTA's scratch
@@ -578,6 +579,20 @@ __global__ void __launch_bounds__(kThreads, 1) energy_kernel(Dev p) {
       p.wt_out[w] = p.weight[slot];
     }
     __syncthreads();
+  }
+}
+
+// ApplyOneSiteTrotterTermEverywhere (MPSstate.cpp:635-659): every site's sigma block scaled by
+// the diagonal single-site propagator.  One CTA per walker (grid-stride).
+__global__ void onesite_kernel(Dev p) {
+  const int N = *p.n_cur;
+  for (int w = blockIdx.x; w < N; w += gridDim.x) {
+    double *W = p.walkers + (long)p.slot_of[w] * p.wstride;
+    for (int k = 0; k < p.L; ++k) {
+      const int blk = p.bW[k] * p.bW[k + 1];
+      double *site = W + p.woff[k];
+      for (int q = threadIdx.x; q < blk * kMaxD; q += blockDim.x) site[q] *= p.onesite[q / blk];
+    }
   }
 }
 

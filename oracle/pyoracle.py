@@ -319,9 +319,11 @@ def load_npy_dir(path: str) -> dict:
 
 
 def harness_walk(trial_path: str, DW: int, Nw: int, dtau: float, steps: int, trace=True,
-                 tensors=False, seed: int | None = None) -> dict:
+                 tensors=False, seed: int | None = None, field: float = 0.0) -> dict:
     with tempfile.TemporaryDirectory() as tmp:
-        extra = {"MPSQMC_REF_SEED": str(seed)} if seed is not None else None
+        extra = {"MPSQMC_REF_SEED": str(seed)} if seed is not None else {}
+        if field:
+            extra["MPSQMC_REF_FIELD"] = repr(float(field))
         args = ["walk", trial_path, DW, Nw, dtau, steps, tmp] + (["trace"] if trace else []) + \
                (["tensors"] if tensors else [])
         run_harness(*args, env_extra=extra)

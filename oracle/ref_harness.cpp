@@ -111,9 +111,15 @@ void save_mps(const std::string &prefix, MPSstate *m) {
   save_d(prefix + "_data.npy", data);
 }
 
+// Chain of main.cpp:36-41; the field h comes from $MPSQMC_REF_FIELD (default 0, as main.cpp).
+double field_from_env() {
+  const char *f = getenv("MPSQMC_REF_FIELD");
+  return f ? atof(f) : 0.0;
+}
+
 void build_chain(HeisenbergMPO &mpo, int L) {
   for (int i = 0; i < L - 1; ++i) mpo.sCoupling(i, i + 1, 1.0);
-  mpo.sField(0.0);
+  mpo.sField(field_from_env());
 }
 
 int trial_length(const char *file) {
@@ -451,7 +457,7 @@ int mode_walk(int argc, char **argv) {
      << ", \"dtau\": " << fmt17(dtau) << ", \"steps\": " << steps
      << ", \"seed\": " << mpsqmc_compat::mt_last_seed() << ", \"setup_draws\": " << setup_draws
      << ", \"E0\": " << fmt17(E0) << ", \"nCouplings\": " << q.nCouplings
-     << ", \"G\": " << grid.gNPoints() << "}";
+     << ", \"G\": " << grid.gNPoints() << ", \"h\": " << fmt17(field_from_env()) << "}";
   write_json(out + "/meta.json", js.str());
   return 0;
 }

@@ -25,7 +25,7 @@ def load_golden(name: str) -> dict:
 
 
 WALK_CASES = ["walk_L16D16_DW16", "walk_L10D8_DW4", "walk_L10D8_DW2_branch", "walk_L10D8_DW1_branch",
-              "walk_debug_DW2"]
+              "walk_debug_DW2", "walk_L10D8_DW4_field"]
 
 
 @pytest.fixture(scope="session")

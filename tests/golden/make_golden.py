@@ -78,11 +78,11 @@ def gen_mpsops():
     save("mpsops_debug", **D)
 
 
-def gen_walk(name, trial: po.MPS, DW, Nw, dtau, steps, tensors=True):
+def gen_walk(name, trial: po.MPS, DW, Nw, dtau, steps, tensors=True, field=0.0):
     with tempfile.TemporaryDirectory() as t:
         path = os.path.join(t, "trial.mps")
         po.write_mps(path, trial)
-        D = po.harness_walk(path, DW, Nw, dtau, steps, trace=True, tensors=tensors, seed=SEED)
+        D = po.harness_walk(path, DW, Nw, dtau, steps, trace=True, tensors=tensors, seed=SEED, field=field)
     meta = D.pop("meta")
     keep = {}
     last = f"step{steps:03d}_"
@@ -114,7 +114,15 @@ def main():
     gen_walk("walk_L10D8_DW1_branch", T(10, 8), 1, 32, 0.5, 8)
     dbg = po.read_mps(os.path.join(REF_DIR, "debug.mps"))
     gen_walk("walk_debug_DW2", dbg, 2, 32, 0.01, 3)
+    gen_walk("walk_L10D8_DW4_field", T(10, 8), 4, 16, 0.05, 3, field=0.7)
 
 
 if __name__ == "__main__":
-    main()
+    only = sys.argv[1:]
+    if only:  # regenerate selected walk fixtures only, e.g. walk_L10D8_DW4_field
+        z = np.load(os.path.join(OUT, "trials.npz"))
+        T = lambda L, D: po.MPS(z[f"L{L}D{D}_dims"], z[f"L{L}D{D}_data"])
+        if "walk_L10D8_DW4_field" in only:
+            gen_walk("walk_L10D8_DW4_field", T(10, 8), 4, 16, 0.05, 3, field=0.7)
+    else:
+        main()

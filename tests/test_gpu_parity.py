@@ -25,7 +25,7 @@ def engine_for(z, capacity=None):
     meta = z["meta"]
     L, N = meta["L"], meta["Nw"]
     ci, cj, cJ = pb.chain(L)
-    eng = Engine(L=L, ci=ci, cj=cj, cJ=cJ, h=0.0, dtau=meta["dtau"], trial_dims=z["trial_ln_dims"],
+    eng = Engine(L=L, ci=ci, cj=cj, cJ=cJ, h=meta.get("h", 0.0), dtau=meta["dtau"], trial_dims=z["trial_ln_dims"],
                  trial=z["trial_ln_data"], Jvals=[1.0], U=z["U"], S=z["S"], VT=z["VT"], grid=z["grid"],
                  Ndesired=N, capacity=capacity or max(1000, 3 * N), walker_dims=z["walker0_init_dims"])
     walkers = np.tile(z["walker0_init_data"], (N, 1))

@@ -101,7 +101,7 @@ def _walk_oracle(z, trace=True):
     return po.walk(trial, walkers, w0.dims, z["init_weight"], z["init_overlap"], np.zeros(N), ci=ci, cj=cj,
                    cJ=cJ, Jvals=np.array([1.0]), U=z["U"], S=z["S"], VT=z["VT"], grid=z["grid"],
                    dtau=meta["dtau"], nsteps=meta["steps"], Ndesired=N, capacity=max(1000, 3 * N),
-                   seed=meta["seed"], skip=meta["setup_draws"], trace=trace)
+                   seed=meta["seed"], skip=meta["setup_draws"], trace=trace, h=meta.get("h", 0.0))
 
 
 @pytest.mark.parametrize("case", WALK_CASES)
