@@ -115,8 +115,14 @@ int mpsqmc_energy(mpsqmc_ctx *ctx, double *E_P);
 /* Run `nsteps` iterations of the body of MPSQMC2::Walk (MPSQMC2.cpp:465-511): propagation of
  * every walker (PropagateSeparately, 518-611), weight sum, E_T, local energies and history
  * (688-747), threshold population control (613-686).  stats may be NULL or hold nsteps
- * entries. */
+ * entries.  Each step runs as one CUDA graph launch (captured on first use). */
 int mpsqmc_walk(mpsqmc_ctx *ctx, int nsteps, mpsqmc_step_stats *stats);
+
+/* Set the number of completed steps.  The next step is completed_steps + 1; it divides the
+ * energy history in the fluctuation metric (MPSQMC2.cpp:708).  MPSQMC2::Walk restarts its step
+ * loop at 1 on every call (MPSQMC2.cpp:465): call mpsqmc_set_step(ctx, 0) before mpsqmc_walk to
+ * get that behaviour; by default the count continues across mpsqmc_walk calls. */
+int mpsqmc_set_step(mpsqmc_ctx *ctx, int completed_steps);
 
 /* Per-walker data of the most recent step, in the logical order used during that step (before
  * branching): weight, overlap and local energy after propagation; parent[k] is the pre-branch

@@ -21,7 +21,7 @@ EXPORTED = [
     "mpsqmc_create", "mpsqmc_destroy", "mpsqmc_last_error", "mpsqmc_version", "mpsqmc_walker_size",
     "mpsqmc_set_walkers", "mpsqmc_get_walkers", "mpsqmc_set_rng", "mpsqmc_get_rng_draws",
     "mpsqmc_energy", "mpsqmc_walk", "mpsqmc_last_step_walkers", "mpsqmc_set_trace",
-    "mpsqmc_get_trace", "mpsqmc_last_timing", "mpsqmc_local_energy_noalloc",
+    "mpsqmc_get_trace", "mpsqmc_last_timing", "mpsqmc_local_energy_noalloc", "mpsqmc_set_step",
 ]
 
 
@@ -99,6 +99,7 @@ def load(build_if_missing: bool = True):
         "mpsqmc_set_trace": (C.c_int, [P, C.c_int]),
         "mpsqmc_get_trace": (C.c_int, [P, dp, ip]),
         "mpsqmc_last_timing": (C.c_int, [P, dp, dp, ip]),
+        "mpsqmc_set_step": (C.c_int, [P, C.c_int]),
         "mpsqmc_local_energy_noalloc": (C.c_int, [C.POINTER(EnergyLayout), P, P, C.c_long, P, C.c_int, P,
                                                   C.c_int, P]),
     }
@@ -198,6 +199,9 @@ class Engine:
         return [dict(step=s.step, n_walkers=s.n_walkers, n_after=s.n_after, sum_weight=s.sum_weight,
                      avg_weight=s.avg_weight, E_P=s.E_P, E_T=s.E_T, omega=s.omega, scaling=s.scaling,
                      draws=s.draws) for s in st[:nsteps]]
+
+    def set_step(self, completed_steps: int):
+        check(self.lib.mpsqmc_set_step(self._ctx, completed_steps))
 
     def last_step_walkers(self):
         nb, na = C.c_int(0), C.c_int(0)

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -108,6 +109,12 @@ struct mpsqmc_ctx {
   int last_launches = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   double opSx[4], opISy[4], opSz[4];
+  // one timestep captured as a CUDA graph (re-captured when the trace setting changes)
+  bool use_graph = true;
+  cudaGraphExec_t graph_exec = nullptr;
+  bool graph_trace = false;
+  mq::StepDev *h_sd = nullptr;  // pinned copies read back after every step
+  int *h_err = nullptr;
 };
 
 namespace {
@@ -186,6 +193,9 @@ void free_all(mpsqmc_ctx *c) {
                   c->d_err, c->d_mt, c->d_sd};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  if (c->h_sd) cudaFreeHost(c->h_sd);
+  if (c->h_err) cudaFreeHost(c->h_err);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -335,6 +345,9 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
         dalloc(&c->d_scratch, (size_t)c->max_ctas * c->scr_stride) | dalloc(&c->d_err, 1) |
         dalloc(&c->d_mt, 1) | dalloc(&c->d_sd, 1);
   if (rc) return bail(MPSQMC_E_CUDA);
+  if (cudaMallocHost((void **)&c->h_sd, sizeof(mq::StepDev)) != cudaSuccess ||
+      cudaMallocHost((void **)&c->h_err, sizeof(int)) != cudaSuccess)
+    return bail(fail(MPSQMC_E_CUDA, "pinned host buffers"));
   auto up = [&](void *dst, const void *src, size_t bytes) {
     return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
   };
@@ -420,6 +433,7 @@ int mpsqmc_set_walkers(mpsqmc_ctx *c, int N, const double *walkers, const double
   std::memset(&sd, 0, sizeof sd);
   sd.n_cur = N;
   sd.n_free = c->capacity - N;
+  sd.step = c->step_count;
   CK(cudaMemcpyAsync(c->d_sd, &sd, sizeof sd, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_ncur, &N, sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
@@ -464,7 +478,7 @@ int mpsqmc_energy(mpsqmc_ctx *c, double *E_P) {
   mq::Dev p = make_dev(c);
   mq::energy_kernel<<<grid_for(c, c->n_cur), mq::kThreads, c->smem_bytes, c->stream>>>(p);
   CK(cudaGetLastError());
-  mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 1, 0, c->d_flag_pos, c->d_sw);
+  mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 0, c->d_flag_pos, c->d_sw);
   CK(cudaGetLastError());
   mq::StepDev sd;
   CK(cudaMemcpyAsync(&sd, c->d_sd, sizeof sd, cudaMemcpyDeviceToHost, c->stream));
@@ -472,6 +486,67 @@ int mpsqmc_energy(mpsqmc_ctx *c, double *E_P) {
   int rc = check_err(c);
   if (rc) return rc;
   *E_P = sd.EP;
+  return 0;
+}
+
+// Issue one timestep on c->stream (also used under stream capture): every grid has its fixed
+// maximal size and every kernel reads the current walker count from device memory.
+static int enqueue_step(mpsqmc_ctx *c, int *launches) {
+  mq::Dev p = make_dev(c);
+  const int grid = c->max_ctas;
+  mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, c->d_ncur, 0, c->nC, c->d_uni);
+  const bool field = c->h != 0.0;
+  int n = 7;
+  if (field) {  // single-site propagator before the couplings (MPSQMC2.cpp:533)
+    mq::onesite_kernel<<<grid, 256, 0, c->stream>>>(p);
+    n += 1;
+  }
+  // external event records: they become event-record nodes under capture, so they time the
+  // step kernel inside the graph
+  CK(cudaEventRecordWithFlags(c->ev[0], c->stream, cudaEventRecordExternal));
+  mq::walker_step_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+  CK(cudaEventRecordWithFlags(c->ev[1], c->stream, cudaEventRecordExternal));
+  if (field) {
+    // single-site propagator after the couplings, setOverlap, and the local energy of the
+    // resulting state (MPSQMC2.cpp:597-598, then 698)
+    mq::onesite_kernel<<<grid, 256, 0, c->stream>>>(p);
+    mq::set_overlap_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+    mq::energy_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+    n += 3;
+  }
+  mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 1, c->d_flag_pos, c->d_sw);
+  mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, &c->d_sd->n_flag, 0, 1, c->d_ubr);
+  mq::branch_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->d_flag_pos, c->d_sw, c->d_ubr, c->d_slot_new,
+                                               c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
+                                               c->capacity);
+  mq::copy_walkers_kernel<<<4 * c->sm_count, 256, 0, c->stream>>>(p, c->d_sd, c->d_copy_src, c->d_copy_dst);
+  mq::finish_branch_kernel<<<1, 1024, 0, c->stream>>>(c->d_sd, c->d_ncur, c->d_slot_of, c->d_slot_new, c->d_err,
+                                                      c->capacity);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->h_sd, c->d_sd, sizeof(mq::StepDev), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  *launches = n;
+  return 0;
+}
+
+static int build_graph(mpsqmc_ctx *c, int *launches) {
+  if (c->graph_exec) {
+    cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_step(c, launches);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(MPSQMC_E_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(MPSQMC_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  c->graph_trace = c->trace_on;
   return 0;
 }
 
@@ -483,48 +558,28 @@ int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
   if (c->trace_on && !c->d_trace) {
     if (dalloc(&c->d_trace, (size_t)c->capacity * c->nC * mq::kTraceStride)) return MPSQMC_E_CUDA;
   }
+  int per_step = 0;
+  if (c->use_graph && (!c->graph_exec || c->graph_trace != c->trace_on)) {
+    int rc = build_graph(c, &per_step);
+    if (rc) return rc;
+  }
+  if (c->use_graph) per_step = (c->h != 0.0) ? 11 : 7;
   double kernel_ms = 0.0;
   int launches = 0;
   CK(cudaEventRecord(c->ev[2], c->stream));
   for (int s = 0; s < nsteps; ++s) {
     const int N = c->n_cur;
     const int step = ++c->step_count;
-    mq::Dev p = make_dev(c);
-    mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, c->d_ncur, 0, c->nC, c->d_uni);
-    const bool field = c->h != 0.0;
-    if (field) {  // single-site propagator before the couplings (MPSQMC2.cpp:533)
-      mq::onesite_kernel<<<grid_for(c, N), 256, 0, c->stream>>>(p);
-      launches += 1;
+    if (c->use_graph) {
+      CK(cudaGraphLaunch(c->graph_exec, c->stream));
+    } else {
+      int rc = enqueue_step(c, &per_step);
+      if (rc) return rc;
     }
-    CK(cudaEventRecord(c->ev[0], c->stream));
-    mq::walker_step_kernel<<<grid_for(c, N), mq::kThreads, c->smem_bytes, c->stream>>>(p);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(c->ev[1], c->stream));
-    if (field) {
-      // single-site propagator after the couplings, setOverlap, and the local energy of the
-      // resulting state (MPSQMC2.cpp:597-598, then 698)
-      mq::onesite_kernel<<<grid_for(c, N), 256, 0, c->stream>>>(p);
-      mq::set_overlap_kernel<<<grid_for(c, N), mq::kThreads, c->smem_bytes, c->stream>>>(p);
-      mq::energy_kernel<<<grid_for(c, N), mq::kThreads, c->smem_bytes, c->stream>>>(p);
-      CK(cudaGetLastError());
-      launches += 3;
-    }
-    mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, step, 1, c->d_flag_pos, c->d_sw);
-    mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, &c->d_sd->n_flag, 0, 1, c->d_ubr);
-    mq::branch_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->d_flag_pos, c->d_sw, c->d_ubr, c->d_slot_new,
-                                                 c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
-                                                 c->capacity);
-    mq::copy_walkers_kernel<<<std::min(N * 4, 4 * c->sm_count), 256, 0, c->stream>>>(p, c->d_sd, c->d_copy_src,
-                                                                                     c->d_copy_dst);
-    mq::finish_branch_kernel<<<1, 1024, 0, c->stream>>>(c->d_sd, c->d_ncur, c->d_slot_of, c->d_slot_new, c->d_err,
-                                                        c->capacity);
-    CK(cudaGetLastError());
-    launches += 7;
-    mq::StepDev sd;
-    int err = 0;
-    CK(cudaMemcpyAsync(&sd, c->d_sd, sizeof sd, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(&err, c->d_err, sizeof err, cudaMemcpyDeviceToHost, c->stream));
+    launches += per_step;
     CK(cudaStreamSynchronize(c->stream));
+    const mq::StepDev sd = *c->h_sd;
+    const int err = *c->h_err;
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
     kernel_ms += ms;
@@ -557,6 +612,15 @@ int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
   c->last_kernel_ms = kernel_ms;
   c->last_total_ms = tot;
   c->last_launches = launches;
+  return 0;
+}
+
+int mpsqmc_set_step(mpsqmc_ctx *c, int completed_steps) {
+  if (!c || completed_steps < 0) return fail(MPSQMC_E_ARG, "bad arguments");
+  CK(cudaSetDevice(c->device));
+  c->step_count = completed_steps;
+  CK(cudaMemcpy((char *)c->d_sd + offsetof(mq::StepDev, step), &completed_steps, sizeof(int),
+                cudaMemcpyHostToDevice));
   return 0;
 }
 

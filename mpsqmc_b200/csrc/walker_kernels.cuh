@@ -711,9 +711,11 @@ __device__ double block_sum_d(double v, double *buf) {  // blockDim.x == 1024
 
 // Weight sum, E_T, E_P, energy history, fluctuation metric (MPSQMC2.cpp:468-487, 688-747),
 // then the branching flags of SeparatePopulationControl (613-648).
+// The step number (1-based, for e_j = Ehist_j / step) is sd->step + 1; finish_branch_kernel
+// advances sd->step, so a captured step graph needs no per-step argument.
 __global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Ndesired, double dtau,
-                                                     int step, int update_history, int *flag_pos,
-                                                     double *sw_out) {
+                                                     int update_history, int *flag_pos, double *sw_out) {
+  const int step = sd->step + 1;
   __shared__ double dbuf[32];
   __shared__ int ibuf[32];
   const int N = sd->n_cur;
@@ -873,6 +875,7 @@ __global__ void finish_branch_kernel(StepDev *sd, int *n_cur, int *slot_of, cons
   for (int q = threadIdx.x; q < nn; q += blockDim.x) slot_of[q] = slot_of_new[q];
   if (threadIdx.x == 0) {
     sd->n_cur = nn;
+    sd->step += 1;
     *n_cur = nn;
   }
 }
