@@ -33,8 +33,33 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(s) <= t for s in deps)
 
 
+HOST = os.path.join(HERE, "host")
+HOST_LIB = os.path.join(HERE, "libmpsqmc_host.so")
+
+
+def host_sources() -> list[str]:
+    src = os.path.join(HOST, "src")
+    return sorted(os.path.join(src, f) for f in os.listdir(src) if f.endswith(".cpp"))
+
+
+def build_host(force: bool = False) -> str:
+    """The reference-compatible C++ classes (host/include) over the engine, as libmpsqmc_host.so."""
+    deps = host_sources() + [os.path.join(HOST, "include", f) for f in os.listdir(os.path.join(HOST, "include"))]
+    if not force and os.path.exists(HOST_LIB) and all(os.path.getmtime(d) <= os.path.getmtime(HOST_LIB) for d in deps):
+        return HOST_LIB
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-I", os.path.join(HOST, "include"), *host_sources(),
+           "-L", HERE, "-lmpsqmc_b200", "-Wl,-rpath,$ORIGIN", "-o", HOST_LIB + ".tmp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host library build failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(HOST_LIB + ".tmp", HOST_LIB)
+    return HOST_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
+        build_host()
         return LIB
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     units = [os.path.join(CSRC, f) for f in ("capi.cu", "noalloc.cu")]
@@ -47,6 +72,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.replace(LIB + ".tmp", LIB)
     if verbose:
         print(r.stderr)
+    build_host(force=True)
     return LIB
 
 
