@@ -151,7 +151,8 @@ def main():
     cfg = {"workload": f"{wl.name}: L={wl.L} Heisenberg chain, D_T={wl.DT}, D_W={wl.DW}, {wl.Nw} walkers/GPU, "
                        f"dtau={wl.dtau}, Marsaglia(4) grid, FP64",
            "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.DW, "dtau": wl.dtau,
-           "l2": "population (1.8 GB) larger than L2; no flush", "parallelism": f"replicas x{world}"}
+           "l2": f"population ({wl.Nw * wl.walker.data.size * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
+           "parallelism": f"replicas x{world}"}
 
     if args.impl == "reference":
         if rank != 0:
@@ -187,9 +188,15 @@ def main():
     eng.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
     eng.set_rng(wl.seed + 7919 * rank, 0)
     eng.walk(args.warmup)
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
     with ClockSampler(local) as clk:
         stats = eng.walk(args.steps)
+        torch.cuda.synchronize()
         tim = eng.last_timing()
+    if pg is not None:
+        pg.barrier()
     ws_done = sum(s["n_walkers"] for s in stats)
     t_ms = tim["total_ms"]
     k_ms = tim["step_kernel_ms"]

@@ -116,7 +116,7 @@ def test_dropin_walk_runs_main_call_sequence(tmp_path):
                        text=True, env={**os.environ, "MPSQMC_SEED": "20131015"}, timeout=300)
     assert r.returncode == 0, r.stderr
     assert "GPU engine unavailable" not in r.stderr and "MPSQMC::Walk" not in r.stderr
-    meta = json.loads(str(load_golden("walk_L10D8_DW4")["meta"]))
+    meta = load_golden("walk_L10D8_DW4")["meta"]
     E0 = float(r.stdout.split("Energy at start = ")[1].split()[0])
     assert E0 == pytest.approx(meta["E0"], rel=1e-10)    # same trial, same compressed walkers
     lines = (tmp_path / "output" / "Heisenberg1D" / "ener_L10DT8DW4.txt").read_text().splitlines()
