@@ -39,6 +39,8 @@ def parse():
     ap.add_argument("--walkers", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--sweep", default="auto", choices=["auto", "nearest", "general"],
+                    help="walker-step kernel (auto: nearest-neighbour for chains)")
     return ap.parse_args()
 
 
@@ -152,7 +154,7 @@ def main():
                        f"dtau={wl.dtau}, Marsaglia(4) grid, FP64",
            "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.DW, "dtau": wl.dtau,
            "l2": f"population ({wl.Nw * wl.walker.data.size * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
-           "parallelism": f"replicas x{world}"}
+           "parallelism": f"replicas x{world}", "sweep": args.sweep}
 
     if args.impl == "reference":
         if rank != 0:
@@ -184,6 +186,9 @@ def main():
     inputs = wl.inputs()
     walkers = wl.walkers()
     eng = Engine(device=local, **inputs)
+    from mpsqmc_b200.capi import OPT_SWEEP
+    sweep = {"auto": 0, "nearest": 1, "general": 2}[args.sweep]
+    eng.set_option(OPT_SWEEP, sweep)
     N = walkers.shape[0]
     eng.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
     eng.set_rng(wl.seed + 7919 * rank, 0)
@@ -222,6 +227,7 @@ def main():
     e2e = None
     if not args.no_e2e:
         eng2 = Engine(device=local, **inputs)
+        eng2.set_option(OPT_SWEEP, sweep)
         host_w = np.ascontiguousarray(walkers)
         t0 = time.perf_counter()
         eng2.set_walkers(host_w, np.ones(N), None, np.zeros(N), normalize=True)

@@ -44,7 +44,7 @@ typedef struct {
   int d;                 /* local dimension; the kernels implement d = 2 */
   int nC;                /* number of couplings */
   const int *ci;         /* first site of each coupling */
-  const int *cj;         /* second site of each coupling (only cj = ci + 1 is implemented) */
+  const int *cj;         /* second site of each coupling (any cj > ci) */
   const double *cJ;      /* coupling strength of each coupling */
   double h;              /* magnetic field (HeisenbergMPO::gField) */
   double dtau;           /* imaginary time step */
@@ -140,6 +140,15 @@ int mpsqmc_get_trace(mpsqmc_ctx *ctx, double *trace, int *n_walkers);
  * (summed over steps), and the number of kernel launches the call made. */
 int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms,
                        int *kernel_launches);
+
+/* Engine options.  No counterpart in the reference (its choices are compile-time).  A new value
+ * takes effect from the next mpsqmc_walk step; unknown options or values give MPSQMC_E_ARG. */
+#define MPSQMC_OPT_SWEEP 1        /* walker-step kernel: */
+#define MPSQMC_SWEEP_AUTO 0       /*   nearest-neighbour sweep when every coupling is (i, i+1), else general */
+#define MPSQMC_SWEEP_NEAREST 1    /*   nearest-neighbour sweep (MPSQMC_E_UNSUPPORTED for longer couplings) */
+#define MPSQMC_SWEEP_GENERAL 2    /*   couplings (i, j) of any range, e.g. 2D lattices on a snake path */
+int mpsqmc_set_option(mpsqmc_ctx *ctx, int option, long value);
+int mpsqmc_get_option(mpsqmc_ctx *ctx, int option, long *value);
 
 /* ---------------------------------------------------------------------------------------------
  * Local energies without any device allocation.  No counterpart in the reference.

@@ -15,6 +15,8 @@ from . import build as _build
 OK = 0
 E_ARG, E_CUDA, E_NODEVICE, E_UNSUPPORTED, E_CAPACITY, E_NUMERIC, E_EXTINCT = -1, -2, -3, -4, -5, -6, -7
 TRACE_STRIDE = 21
+OPT_SWEEP = 1
+SWEEP_AUTO, SWEEP_NEAREST, SWEEP_GENERAL = 0, 1, 2
 
 # Every symbol include/mpsqmc_gpu.h declares.
 EXPORTED = [
@@ -22,6 +24,7 @@ EXPORTED = [
     "mpsqmc_set_walkers", "mpsqmc_get_walkers", "mpsqmc_set_rng", "mpsqmc_get_rng_draws",
     "mpsqmc_energy", "mpsqmc_walk", "mpsqmc_last_step_walkers", "mpsqmc_set_trace",
     "mpsqmc_get_trace", "mpsqmc_last_timing", "mpsqmc_local_energy_noalloc", "mpsqmc_set_step",
+    "mpsqmc_set_option", "mpsqmc_get_option",
 ]
 
 
@@ -100,6 +103,8 @@ def load(build_if_missing: bool = True):
         "mpsqmc_get_trace": (C.c_int, [P, dp, ip]),
         "mpsqmc_last_timing": (C.c_int, [P, dp, dp, ip]),
         "mpsqmc_set_step": (C.c_int, [P, C.c_int]),
+        "mpsqmc_set_option": (C.c_int, [P, C.c_int, C.c_long]),
+        "mpsqmc_get_option": (C.c_int, [P, C.c_int, C.POINTER(C.c_long)]),
         "mpsqmc_local_energy_noalloc": (C.c_int, [C.POINTER(EnergyLayout), P, P, C.c_long, P, C.c_int, P,
                                                   C.c_int, P]),
     }
@@ -220,6 +225,14 @@ class Engine:
         buf = np.zeros((self.capacity, self.nC, TRACE_STRIDE))
         check(self.lib.mpsqmc_get_trace(self._ctx, _dp(buf), C.byref(n)))
         return buf[: n.value]
+
+    def set_option(self, option: int, value: int):
+        check(self.lib.mpsqmc_set_option(self._ctx, option, value))
+
+    def get_option(self, option: int) -> int:
+        v = C.c_long(0)
+        check(self.lib.mpsqmc_get_option(self._ctx, option, C.byref(v)))
+        return v.value
 
     def last_timing(self):
         k, t, n = C.c_double(0), C.c_double(0), C.c_int(0)

@@ -18,6 +18,7 @@
 
 #include "../../include/mpsqmc_gpu.h"
 #include "walker_kernels.cuh"
+#include "walker_general.cuh"
 
 namespace {
 
@@ -97,6 +98,13 @@ struct mpsqmc_ctx {
   double *d_weight = nullptr, *d_overlap = nullptr, *d_ehist = nullptr, *d_energy = nullptr,
          *d_ovout = nullptr, *d_wtout = nullptr, *d_sw = nullptr, *d_uni = nullptr, *d_ubr = nullptr;
   int *d_bond_c = nullptr, *d_bond_j = nullptr;
+  // couplings of any range and the energy channels of their compact MPO
+  bool nn = true;   // every coupling is (i, i+1)
+  int sweep = MPSQMC_SWEEP_AUTO;
+  long choff = 0;
+  int *d_cp_j = nullptr, *d_cp_q = nullptr, *d_site_c0 = nullptr, *d_ech_off = nullptr, *d_ech_slot = nullptr,
+      *d_ech_cont = nullptr, *d_eopen = nullptr;
+  double *d_ech_J = nullptr;
   double *d_bondJ = nullptr, *d_tabU = nullptr, *d_tabS = nullptr, *d_tabVT = nullptr, *d_grid = nullptr;
   double *d_scratch = nullptr, *d_trace = nullptr;
   int *d_err = nullptr;
@@ -169,8 +177,21 @@ mq::Dev make_dev(mpsqmc_ctx *c) {
   p.foff = c->foff;
   p.trace = c->trace_on ? c->d_trace : nullptr;
   p.err = c->d_err;
+  p.cp_j = c->d_cp_j;
+  p.cp_q = c->d_cp_q;
+  p.site_c0 = c->d_site_c0;
+  p.ech_off = c->d_ech_off;
+  p.ech_slot = c->d_ech_slot;
+  p.ech_J = c->d_ech_J;
+  p.ech_cont = c->d_ech_cont;
+  p.eopen = c->d_eopen;
+  p.choff = c->choff;
   return p;
 }
+
+// The general sweep (walker_general.cuh) runs when a coupling is longer than one bond, or on
+// request; the nearest-neighbour sweep otherwise.
+bool general_sweep(const mpsqmc_ctx *c) { return !c->nn || c->sweep == MPSQMC_SWEEP_GENERAL; }
 
 int grid_for(const mpsqmc_ctx *c, int n) { return std::max(1, std::min(n, c->max_ctas)); }
 
@@ -190,7 +211,8 @@ void free_all(mpsqmc_ctx *c) {
                   c->d_flag_pos, c->d_ncur, c->d_weight, c->d_overlap, c->d_ehist, c->d_energy,
                   c->d_ovout, c->d_wtout, c->d_sw, c->d_uni, c->d_ubr, c->d_bond_c, c->d_bond_j,
                   c->d_bondJ, c->d_tabU, c->d_tabS, c->d_tabVT, c->d_grid, c->d_scratch, c->d_trace,
-                  c->d_err, c->d_mt, c->d_sd};
+                  c->d_err, c->d_mt, c->d_sd, c->d_cp_j, c->d_cp_q, c->d_site_c0, c->d_ech_off,
+                  c->d_ech_slot, c->d_ech_cont, c->d_eopen, c->d_ech_J};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
@@ -229,15 +251,15 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   if (!cfg->trial_dims || !cfg->trial || !cfg->walker_dims) return fail(MPSQMC_E_ARG, "missing MPS data");
   if (!valid_dims(cfg->trial_dims, L, d) || !valid_dims(cfg->walker_dims, L, d))
     return fail(MPSQMC_E_ARG, "bond dimensions inconsistent with the chain");
-  std::vector<int> bond_c(L - 1, -1), bond_j(L - 1, -1);
+  // Couplings in the order MPSQMC2.cpp:286-299 lists them: by first site, then by second site.
+  std::vector<int> bond_c(L - 1, -1), bond_j(L - 1, -1), cp_j(cfg->nC), cp_q(cfg->nC), site_c0(L + 1, 0);
   std::vector<double> bondJ(L - 1, 0.0);
+  bool nn = true;
   for (int c = 0; c < cfg->nC; ++c) {
     const int i = cfg->ci[c], j = cfg->cj[c];
     if (i < 0 || j >= L || i >= j) return fail(MPSQMC_E_ARG, "coupling indices out of order");
-    if (j != i + 1)
-      return fail(MPSQMC_E_UNSUPPORTED, "only nearest-neighbour chain couplings are implemented");
-    if (bond_c[i] >= 0) return fail(MPSQMC_E_ARG, "duplicate coupling");
-    if (c > 0 && cfg->ci[c - 1] >= i) return fail(MPSQMC_E_ARG, "couplings must be ordered by site");
+    if (c > 0 && (cfg->ci[c - 1] > i || (cfg->ci[c - 1] == i && cfg->cj[c - 1] >= j)))
+      return fail(MPSQMC_E_ARG, "couplings must be ordered by first site, then by second site, without repeats");
     int q = -1;
     for (int t = 0; t < cfg->nJ; ++t)
       if (cfg->Jvals[t] == cfg->cJ[c]) {
@@ -245,9 +267,61 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
         break;
       }
     if (q < 0) return fail(MPSQMC_E_ARG, "coupling strength without Trotter tables");
-    bond_c[i] = c;
-    bond_j[i] = q;
-    bondJ[i] = cfg->cJ[c];
+    cp_j[c] = j;
+    cp_q[c] = q;
+    site_c0[i + 1] += 1;
+    if (j != i + 1) {
+      nn = false;
+    } else {
+      bond_c[i] = c;
+      bond_j[i] = q;
+      bondJ[i] = cfg->cJ[c];
+    }
+  }
+  for (int i = 0; i < L; ++i) site_c0[i + 1] += site_c0[i];
+  // Energy channels: a site i is open on the cut before site k when it couples to some j >= k.
+  // Site k closes the couplings (i, k) and opens its own channel if it has a partner beyond k.
+  // A slot freed on site k can be taken by the channel site k opens (the kernel reads closing
+  // channels before it writes the new one).
+  std::vector<int> last_partner(L, -1);
+  for (int c = 0; c < cfg->nC; ++c) last_partner[cfg->ci[c]] = std::max(last_partner[cfg->ci[c]], cfg->cj[c]);
+  std::vector<int> ech_off(L + 1, 0), ech_slot, ech_cont, eopen(L, -1), slot_of_site(L, -1), free_slots;
+  std::vector<double> ech_J;
+  std::vector<int> open_sites;
+  int nslots = 0;
+  for (int k = 0; k < L; ++k) {
+    ech_off[k] = (int)ech_slot.size();
+    std::vector<int> still;
+    for (int i : open_sites) {
+      double J = 0.0;
+      for (int c = site_c0[i]; c < site_c0[i + 1]; ++c)
+        if (cp_j[c] == k) J += cfg->cJ[c];
+      const bool cont = last_partner[i] > k;
+      ech_slot.push_back(slot_of_site[i]);
+      ech_J.push_back(J);
+      ech_cont.push_back(cont ? 1 : 0);
+      if (cont) still.push_back(i);
+      else free_slots.push_back(slot_of_site[i]);
+    }
+    open_sites.swap(still);
+    if (last_partner[k] > k) {
+      int sl;
+      if (!free_slots.empty()) {
+        sl = free_slots.back();
+        free_slots.pop_back();
+      } else {
+        sl = nslots++;
+      }
+      slot_of_site[k] = sl;
+      eopen[k] = sl;
+      open_sites.push_back(k);
+    }
+  }
+  ech_off[L] = (int)ech_slot.size();
+  if (ech_slot.empty()) {  // keep the device arrays non-empty
+    ech_slot.push_back(0);
+    ech_J.push_back(0.0);
+    ech_cont.push_back(0);
   }
 
   mpsqmc_ctx *c = new mpsqmc_ctx();
@@ -265,6 +339,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   c->capacity = cfg->capacity;
   c->dtau = cfg->dtau;
   c->h = cfg->h;
+  c->nn = nn;
   c->aT.assign(cfg->trial_dims, cfg->trial_dims + L + 1);
   c->bW.assign(cfg->walker_dims, cfg->walker_dims + L + 1);
   c->toff.resize(L);
@@ -297,7 +372,8 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
     ro += ((long)c->bW[k] * c->bW[k] + 3) & ~3L;
   }
   c->foff = ro;
-  c->scr_stride = ro + 2L * 4 * c->maxA * c->maxB;
+  c->choff = ro + 2L * 4 * c->maxA * c->maxB;
+  c->scr_stride = c->choff + (2L + 3L * nslots) * c->maxA * c->maxB;
   c->scr_stride = (c->scr_stride + 31) & ~31L;
   for (int s = 0; s < 2; ++s)
     for (int t = 0; t < 2; ++t) {
@@ -321,6 +397,10 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
       cudaFuncSetAttribute(mq::set_overlap_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)c->smem_bytes) != cudaSuccess ||
       cudaFuncSetAttribute(mq::energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)c->smem_bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(mq::walker_step_general_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)c->smem_bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(mq::energy_general_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)c->smem_bytes) != cudaSuccess)
     return bail(fail(MPSQMC_E_CUDA, "cudaFuncSetAttribute failed"));
   int occ = 1;
@@ -343,7 +423,9 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
         dalloc(&c->d_bond_j, L - 1) | dalloc(&c->d_bondJ, L - 1) | dalloc(&c->d_tabU, 16 * c->nJ) |
         dalloc(&c->d_tabS, 4 * c->nJ) | dalloc(&c->d_tabVT, 16 * c->nJ) | dalloc(&c->d_grid, 4 * c->G) |
         dalloc(&c->d_scratch, (size_t)c->max_ctas * c->scr_stride) | dalloc(&c->d_err, 1) |
-        dalloc(&c->d_mt, 1) | dalloc(&c->d_sd, 1);
+        dalloc(&c->d_mt, 1) | dalloc(&c->d_sd, 1) | dalloc(&c->d_cp_j, c->nC) | dalloc(&c->d_cp_q, c->nC) |
+        dalloc(&c->d_site_c0, L + 1) | dalloc(&c->d_ech_off, L + 1) | dalloc(&c->d_ech_slot, ech_slot.size()) |
+        dalloc(&c->d_ech_cont, ech_cont.size()) | dalloc(&c->d_eopen, L) | dalloc(&c->d_ech_J, ech_J.size());
   if (rc) return bail(MPSQMC_E_CUDA);
   if (cudaMallocHost((void **)&c->h_sd, sizeof(mq::StepDev)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_err, sizeof(int)) != cudaSuccess)
@@ -360,7 +442,14 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
             up(c->d_bond_j, bond_j.data(), sizeof(int) * (L - 1)) &&
             up(c->d_bondJ, bondJ.data(), sizeof(double) * (L - 1)) &&
             up(c->d_tabU, cfg->U, sizeof(double) * 16 * c->nJ) && up(c->d_tabS, cfg->S, sizeof(double) * 4 * c->nJ) &&
-            up(c->d_tabVT, cfg->VT, sizeof(double) * 16 * c->nJ) && up(c->d_grid, cfg->grid, sizeof(double) * 4 * c->G);
+            up(c->d_tabVT, cfg->VT, sizeof(double) * 16 * c->nJ) && up(c->d_grid, cfg->grid, sizeof(double) * 4 * c->G) &&
+            up(c->d_cp_j, cp_j.data(), sizeof(int) * c->nC) && up(c->d_cp_q, cp_q.data(), sizeof(int) * c->nC) &&
+            up(c->d_site_c0, site_c0.data(), sizeof(int) * (L + 1)) &&
+            up(c->d_ech_off, ech_off.data(), sizeof(int) * (L + 1)) &&
+            up(c->d_ech_slot, ech_slot.data(), sizeof(int) * ech_slot.size()) &&
+            up(c->d_ech_cont, ech_cont.data(), sizeof(int) * ech_cont.size()) &&
+            up(c->d_eopen, eopen.data(), sizeof(int) * L) &&
+            up(c->d_ech_J, ech_J.data(), sizeof(double) * ech_J.size());
   if (!ok) return bail(fail(MPSQMC_E_CUDA, "upload failed"));
   if (cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess || cudaMemset(c->d_sd, 0, sizeof(mq::StepDev)) != cudaSuccess ||
       cudaMemset(c->d_ncur, 0, sizeof(int)) != cudaSuccess)
@@ -476,7 +565,10 @@ int mpsqmc_energy(mpsqmc_ctx *c, double *E_P) {
   if (c->n_cur < 1) return fail(MPSQMC_E_ARG, "no walkers");
   CK(cudaSetDevice(c->device));
   mq::Dev p = make_dev(c);
-  mq::energy_kernel<<<grid_for(c, c->n_cur), mq::kThreads, c->smem_bytes, c->stream>>>(p);
+  if (general_sweep(c))
+    mq::energy_general_kernel<<<grid_for(c, c->n_cur), mq::kThreads, c->smem_bytes, c->stream>>>(p);
+  else
+    mq::energy_kernel<<<grid_for(c, c->n_cur), mq::kThreads, c->smem_bytes, c->stream>>>(p);
   CK(cudaGetLastError());
   mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 0, c->d_flag_pos, c->d_sw);
   CK(cudaGetLastError());
@@ -504,14 +596,21 @@ static int enqueue_step(mpsqmc_ctx *c, int *launches) {
   // external event records: they become event-record nodes under capture, so they time the
   // step kernel inside the graph
   CK(cudaEventRecordWithFlags(c->ev[0], c->stream, cudaEventRecordExternal));
-  mq::walker_step_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+  const bool gen = general_sweep(c);
+  if (gen)
+    mq::walker_step_general_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+  else
+    mq::walker_step_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
   CK(cudaEventRecordWithFlags(c->ev[1], c->stream, cudaEventRecordExternal));
   if (field) {
     // single-site propagator after the couplings, setOverlap, and the local energy of the
     // resulting state (MPSQMC2.cpp:597-598, then 698)
     mq::onesite_kernel<<<grid, 256, 0, c->stream>>>(p);
     mq::set_overlap_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
-    mq::energy_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+    if (gen)
+      mq::energy_general_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+    else
+      mq::energy_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
     n += 3;
   }
   mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 1, c->d_flag_pos, c->d_sw);
@@ -661,6 +760,37 @@ int mpsqmc_last_timing(mpsqmc_ctx *c, double *step_kernel_ms, double *total_ms, 
   if (total_ms) *total_ms = c->last_total_ms;
   if (kernel_launches) *kernel_launches = c->last_launches;
   return 0;
+}
+
+int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
+  if (!c) return fail(MPSQMC_E_ARG, "null context");
+  switch (option) {
+    case MPSQMC_OPT_SWEEP:
+      if (value != MPSQMC_SWEEP_AUTO && value != MPSQMC_SWEEP_NEAREST && value != MPSQMC_SWEEP_GENERAL)
+        return fail(MPSQMC_E_ARG, "unknown sweep");
+      if (value == MPSQMC_SWEEP_NEAREST && !c->nn)
+        return fail(MPSQMC_E_UNSUPPORTED, "the nearest-neighbour sweep needs every coupling to be (i, i+1)");
+      c->sweep = (int)value;
+      break;
+    default:
+      return fail(MPSQMC_E_ARG, "unknown option");
+  }
+  if (c->graph_exec) {  // the captured step no longer matches
+    cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+  }
+  return 0;
+}
+
+int mpsqmc_get_option(mpsqmc_ctx *c, int option, long *value) {
+  if (!c || !value) return fail(MPSQMC_E_ARG, "null argument");
+  switch (option) {
+    case MPSQMC_OPT_SWEEP:
+      *value = c->sweep;
+      return 0;
+    default:
+      return fail(MPSQMC_E_ARG, "unknown option");
+  }
 }
 
 }  // extern "C"

@@ -63,6 +63,15 @@ struct Dev {
   long foff;           // compact-MPO environments (2 x 4 x maxA*maxB) inside the scratch
   double *trace;       // optional [N][nC][kTraceStride]
   int *err;            // device error word (bit flags)
+  // couplings (i, j) of any range (walker_general.cuh)
+  const int *cp_j, *cp_q;  // per coupling: second site, distinct-J index
+  const int *site_c0;      // [L+1]: couplings whose first site is i are site_c0[i] .. site_c0[i+1]-1
+  const int *ech_off;      // [L+1]: energy-channel entries of site k are ech_off[k] .. ech_off[k+1]-1
+  const int *ech_slot;     // per entry: channel slot of an open site i < k
+  const double *ech_J;     // per entry: J_ik (0 if i and k are not coupled)
+  const int *ech_cont;     // per entry: 1 if site i still has a partner beyond k
+  const int *eopen;        // [L]: slot of the channel that site k opens, or -1
+  long choff;              // energy channels inside a CTA's scratch: 2 "done" + 3 per slot
 };
 
 enum : int { kErrNumeric = 1, kErrCapacity = 2 };

@@ -62,6 +62,42 @@ def chain(L: int, J: float = 1.0):
     return ci, ci + 1, np.full(L - 1, float(J))
 
 
+def snake_site(W: int, r: int, c: int) -> int:
+    """MPS position of lattice site (row r, column c) on the snake path: even rows left to
+    right, odd rows right to left."""
+    return r * W + (c if r % 2 == 0 else W - 1 - c)
+
+
+def snake(W: int, H: int, J: float = 1.0):
+    """Open W x H square lattice, nearest-neighbour couplings J, as MPS couplings (i < j) along
+    the snake path, ordered by first site then second site (MPSQMC2.cpp:286-299)."""
+    pairs = set()
+    for r in range(H):
+        for c in range(W):
+            s = snake_site(W, r, c)
+            if c + 1 < W:
+                t = snake_site(W, r, c + 1)
+                pairs.add((min(s, t), max(s, t)))
+            if r + 1 < H:
+                t = snake_site(W, r + 1, c)
+                pairs.add((min(s, t), max(s, t)))
+    pairs = sorted(pairs)
+    ci = np.array([p[0] for p in pairs], dtype=np.int32)
+    cj = np.array([p[1] for p in pairs], dtype=np.int32)
+    return ci, cj, np.full(len(pairs), float(J))
+
+
+def lattice(name: str, J: float = 1.0):
+    """Couplings by name: "chain:L" or "snake:WxH"."""
+    kind, _, shape = name.partition(":")
+    if kind == "chain":
+        return chain(int(shape), J)
+    if kind == "snake":
+        W, H = (int(x) for x in shape.split("x"))
+        return snake(W, H, J)
+    raise ValueError(f"unknown lattice {name!r}")
+
+
 def _erf_inv(z: float) -> float:
     if z == 0.0:
         return 0.0

@@ -44,3 +44,13 @@ def ground_energy(L: int, J: float = 1.0) -> float:
         return float(np.linalg.eigvalsh(H.toarray())[0])
     w = sla.eigsh(H, k=1, which="SA", tol=1e-14, return_eigenvectors=False)
     return float(w[0])
+
+
+def ground_energy_couplings(L: int, ci, cj, cJ) -> float:
+    """Ground energy of H = sum_c J_c S_ci.S_cj (any couplings, e.g. a 2D lattice on a snake path)
+    in the sector with L//2 up spins (it holds the ground state: S^z = 0, or -1/2 for odd L)."""
+    H = chain_hamiltonian(L, bonds=[(int(i), int(j), float(J)) for i, j, J in zip(ci, cj, cJ)])
+    if H.shape[0] < 64:
+        return float(np.linalg.eigvalsh(H.toarray())[0])
+    w = sla.eigsh(H, k=1, which="SA", tol=1e-14, return_eigenvectors=False)
+    return float(w[0])

@@ -319,11 +319,15 @@ def load_npy_dir(path: str) -> dict:
 
 
 def harness_walk(trial_path: str, DW: int, Nw: int, dtau: float, steps: int, trace=True,
-                 tensors=False, seed: int | None = None, field: float = 0.0) -> dict:
+                 tensors=False, seed: int | None = None, field: float = 0.0, lattice: str | None = None) -> dict:
+    """The reference's MPSQMC2 walk (oracle/_ref/ref_harness walk); lattice "snake:WxH" selects the
+    open square lattice on the snake path instead of the chain."""
     with tempfile.TemporaryDirectory() as tmp:
         extra = {"MPSQMC_REF_SEED": str(seed)} if seed is not None else {}
         if field:
             extra["MPSQMC_REF_FIELD"] = repr(float(field))
+        if lattice:
+            extra["MPSQMC_REF_LATTICE"] = lattice
         args = ["walk", trial_path, DW, Nw, dtau, steps, tmp] + (["trace"] if trace else []) + \
                (["tensors"] if tensors else [])
         run_harness(*args, env_extra=extra)

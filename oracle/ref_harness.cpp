@@ -117,8 +117,31 @@ double field_from_env() {
   return f ? atof(f) : 0.0;
 }
 
+// Couplings: the chain of main.cpp:36-41 by default; $MPSQMC_REF_LATTICE = "snake:WxH" gives
+// the open W x H square lattice along the snake path (even rows left to right, odd rows right
+// to left), J = 1 on every nearest-neighbour pair, set through HeisenbergMPO::sCoupling as
+// main.cpp:66-95 sets its periodic J1-J2 square lattice.
+int snake_site(int W, int r, int c) { return r * W + ((r % 2 == 0) ? c : W - 1 - c); }
+
 void build_chain(HeisenbergMPO &mpo, int L) {
-  for (int i = 0; i < L - 1; ++i) mpo.sCoupling(i, i + 1, 1.0);
+  const char *lat = getenv("MPSQMC_REF_LATTICE");
+  int W = 0, H = 0;
+  if (lat && sscanf(lat, "snake:%dx%d", &W, &H) == 2 && W * H == L) {
+    for (int r = 0; r < H; ++r)
+      for (int c = 0; c < W; ++c) {
+        const int s = snake_site(W, r, c);
+        if (c + 1 < W) {
+          const int t = snake_site(W, r, c + 1);
+          mpo.sCoupling(std::min(s, t), std::max(s, t), 1.0);
+        }
+        if (r + 1 < H) {
+          const int t = snake_site(W, r + 1, c);
+          mpo.sCoupling(std::min(s, t), std::max(s, t), 1.0);
+        }
+      }
+  } else {
+    for (int i = 0; i < L - 1; ++i) mpo.sCoupling(i, i + 1, 1.0);
+  }
   mpo.sField(field_from_env());
 }
 
@@ -343,6 +366,19 @@ int mode_walk(int argc, char **argv) {
   save_mps(out + "/trial_ln", q.Psi0[0]);
   save_mps(out + "/walker0_init", q.theWalkers[0]->gState());
   {
+    // the coupling list in the order PropagateSeparately walks it (MPSQMC2.cpp:286-299)
+    std::vector<int> ci(q.nCouplings), cj(q.nCouplings);
+    std::vector<double> cJ(q.nCouplings);
+    for (int c = 0; c < q.nCouplings; ++c) {
+      ci[c] = q.firstIndexCoupling[c];
+      cj[c] = q.secondIndexCoupling[c];
+      cJ[c] = q.theTrotter->gCoupling(ci[c], cj[c]);
+    }
+    save_i(out + "/coup_i.npy", ci);
+    save_i(out + "/coup_j.npy", cj);
+    save_d(out + "/coup_J.npy", cJ);
+  }
+  {
     const int d = 2, n = 4;
     std::vector<double> U(16), S(4), VT(16);
     const double J = 1.0;
@@ -457,7 +493,8 @@ int mode_walk(int argc, char **argv) {
      << ", \"dtau\": " << fmt17(dtau) << ", \"steps\": " << steps
      << ", \"seed\": " << mpsqmc_compat::mt_last_seed() << ", \"setup_draws\": " << setup_draws
      << ", \"E0\": " << fmt17(E0) << ", \"nCouplings\": " << q.nCouplings
-     << ", \"G\": " << grid.gNPoints() << ", \"h\": " << fmt17(field_from_env()) << "}";
+     << ", \"G\": " << grid.gNPoints() << ", \"h\": " << fmt17(field_from_env())
+     << ", \"lattice\": \"" << (getenv("MPSQMC_REF_LATTICE") ? getenv("MPSQMC_REF_LATTICE") : "chain") << "\"}";
   write_json(out + "/meta.json", js.str());
   return 0;
 }

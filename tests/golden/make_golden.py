@@ -78,11 +78,29 @@ def gen_mpsops():
     save("mpsops_debug", **D)
 
 
-def gen_walk(name, trial: po.MPS, DW, Nw, dtau, steps, tensors=True, field=0.0):
+def gen_trials_2d():
+    """Reference DMRG trials of open W x H lattices on the snake path."""
+    out = {}
+    for W, H, D in [(3, 3, 8), (4, 4, 16)]:
+        with tempfile.TemporaryDirectory() as t:
+            path = os.path.join(t, "trial.mps")
+            info = json.loads(po.run_harness("dmrg", W * H, D, path, env_extra={
+                "OMP_NUM_THREADS": "1", "MPSQMC_REF_SEED": str(SEED), "MPSQMC_REF_LATTICE": f"snake:{W}x{H}"}))
+            m = po.read_mps(path)
+        key = f"snake{W}x{H}D{D}"
+        out[key + "_dims"] = m.dims
+        out[key + "_data"] = m.data
+        out[key + "_energy"] = np.array(info["energy"])
+    save("trials2d", **out)
+    return out
+
+
+def gen_walk(name, trial: po.MPS, DW, Nw, dtau, steps, tensors=True, field=0.0, lattice=None):
     with tempfile.TemporaryDirectory() as t:
         path = os.path.join(t, "trial.mps")
         po.write_mps(path, trial)
-        D = po.harness_walk(path, DW, Nw, dtau, steps, trace=True, tensors=tensors, seed=SEED, field=field)
+        D = po.harness_walk(path, DW, Nw, dtau, steps, trace=True, tensors=tensors, seed=SEED, field=field,
+                            lattice=lattice)
     meta = D.pop("meta")
     keep = {}
     last = f"step{steps:03d}_"
@@ -115,6 +133,15 @@ def main():
     dbg = po.read_mps(os.path.join(REF_DIR, "debug.mps"))
     gen_walk("walk_debug_DW2", dbg, 2, 32, 0.01, 3)
     gen_walk("walk_L10D8_DW4_field", T(10, 8), 4, 16, 0.05, 3, field=0.7)
+    gen_2d()
+
+
+def gen_2d():
+    z = gen_trials_2d()
+    T = lambda k: po.MPS(z[k + "_dims"], z[k + "_data"])
+    gen_walk("walk_snake3x3_D8_DW4", T("snake3x3D8"), 4, 16, 0.05, 4, lattice="snake:3x3")
+    gen_walk("walk_snake3x3_D8_DW4_field", T("snake3x3D8"), 4, 16, 0.05, 3, field=0.5, lattice="snake:3x3")
+    gen_walk("walk_snake4x4_D16_DW8_branch", T("snake4x4D16"), 8, 16, 0.3, 5, lattice="snake:4x4")
 
 
 if __name__ == "__main__":
@@ -124,5 +151,7 @@ if __name__ == "__main__":
         T = lambda L, D: po.MPS(z[f"L{L}D{D}_dims"], z[f"L{L}D{D}_data"])
         if "walk_L10D8_DW4_field" in only:
             gen_walk("walk_L10D8_DW4_field", T(10, 8), 4, 16, 0.05, 3, field=0.7)
+        if "2d" in only:
+            gen_2d()
     else:
         main()

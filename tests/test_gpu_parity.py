@@ -11,9 +11,10 @@ produced the fixture; every quantity of the walk is compared:
 import numpy as np
 import pytest
 
-from conftest import WALK_CASES, load_golden
+from conftest import WALK_CASES, couplings, load_golden
 from mpsqmc_b200 import Engine
 from mpsqmc_b200 import problem as pb
+from mpsqmc_b200.capi import OPT_SWEEP, SWEEP_GENERAL
 from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu
@@ -21,16 +22,18 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-10
 
 
-def engine_for(z, capacity=None):
+def engine_for(z, capacity=None, sweep=None):
     meta = z["meta"]
     L, N = meta["L"], meta["Nw"]
-    ci, cj, cJ = pb.chain(L)
+    ci, cj, cJ = couplings(z)
     eng = Engine(L=L, ci=ci, cj=cj, cJ=cJ, h=meta.get("h", 0.0), dtau=meta["dtau"], trial_dims=z["trial_ln_dims"],
                  trial=z["trial_ln_data"], Jvals=[1.0], U=z["U"], S=z["S"], VT=z["VT"], grid=z["grid"],
                  Ndesired=N, capacity=capacity or max(1000, 3 * N), walker_dims=z["walker0_init_dims"])
     walkers = np.tile(z["walker0_init_data"], (N, 1))
     eng.set_walkers(walkers, z["init_weight"], z["init_overlap"], np.zeros(N), normalize=False)
     eng.set_rng(meta["seed"], meta["setup_draws"])
+    if sweep is not None:
+        eng.set_option(OPT_SWEEP, sweep)
     return eng
 
 
@@ -40,11 +43,14 @@ def fidelity(dims_a, a, dims_b, b):
     return ab / np.sqrt(po.inner_product(A, A) * po.inner_product(B, B))
 
 
+@pytest.mark.parametrize("sweep", [None, SWEEP_GENERAL], ids=["auto", "general"])
 @pytest.mark.parametrize("case", WALK_CASES)
-def test_walk_matches_reference(case):
+def test_walk_matches_reference(case, sweep):
+    """Chains run the nearest-neighbour sweep by default and, forced, the general sweep; 2D
+    lattices always run the general sweep."""
     z = load_golden(case)
     meta = z["meta"]
-    eng = engine_for(z)
+    eng = engine_for(z, sweep=sweep)
     assert eng.energy() == pytest.approx(meta["E0"], rel=RTOL)
     total_draws = 0
     for s in range(1, meta["steps"] + 1):
@@ -130,3 +136,12 @@ def test_capacity_overflow_is_an_error_not_a_crash():
     with pytest.raises(MpsqmcError) as ei:
         eng.walk(8)
     assert ei.value.code == E_CAPACITY
+
+
+def test_nearest_neighbour_sweep_refuses_long_couplings():
+    from mpsqmc_b200.capi import E_UNSUPPORTED, SWEEP_NEAREST, MpsqmcError
+    eng = engine_for(load_golden("walk_snake3x3_D8_DW4"))
+    with pytest.raises(MpsqmcError) as ei:
+        eng.set_option(OPT_SWEEP, SWEEP_NEAREST)
+    assert ei.value.code == E_UNSUPPORTED
+    assert eng.get_option(OPT_SWEEP) == 0
