@@ -147,6 +147,9 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
 #define MPSQMC_SWEEP_AUTO 0       /*   nearest-neighbour sweep when every coupling is (i, i+1), else general */
 #define MPSQMC_SWEEP_NEAREST 1    /*   nearest-neighbour sweep (MPSQMC_E_UNSUPPORTED for longer couplings) */
 #define MPSQMC_SWEEP_GENERAL 2    /*   couplings (i, j) of any range, e.g. 2D lattices on a snake path */
+#define MPSQMC_OPT_WORKSPACE 2    /* where a CTA's matrix work buffers live: */
+#define MPSQMC_WORKSPACE_AUTO 0   /*   shared memory when they fit, else global scratch (L2-cached) */
+#define MPSQMC_WORKSPACE_GLOBAL 1 /*   always global scratch (reads the option back as the placement in use) */
 int mpsqmc_set_option(mpsqmc_ctx *ctx, int option, long value);
 int mpsqmc_get_option(mpsqmc_ctx *ctx, int option, long *value);
 

@@ -17,6 +17,8 @@ E_ARG, E_CUDA, E_NODEVICE, E_UNSUPPORTED, E_CAPACITY, E_NUMERIC, E_EXTINCT = -1,
 TRACE_STRIDE = 21
 OPT_SWEEP = 1
 SWEEP_AUTO, SWEEP_NEAREST, SWEEP_GENERAL = 0, 1, 2
+OPT_WORKSPACE = 2
+WORKSPACE_AUTO, WORKSPACE_GLOBAL = 0, 1
 
 # Every symbol include/mpsqmc_gpu.h declares.
 EXPORTED = [

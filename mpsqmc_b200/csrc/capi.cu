@@ -85,7 +85,11 @@ struct mpsqmc_ctx {
   double dtau = 0.0, h = 0.0;
   std::vector<int> aT, bW;
   std::vector<long> toff, woff, roff, nroff;
-  long wsize = 0, wstride = 0, scr_stride = 0, foff = 0;
+  long wsize = 0, wstride = 0, scr_stride = 0, foff = 0, gwoff = -1;
+  long scr_base = 0;                    // scratch doubles per CTA before the matrix work buffers
+  long all_doubles = 0, big_doubles = 0;  // work buffers: all of them / the matrix ones
+  size_t smem_optin = 0;
+  bool global_work = false;             // matrix work buffers in global scratch
   int maxA = 1, maxB = 1, pa = 4, pb = 4, pq = 4;
   size_t smem_bytes = 0;
   int sm_count = 1, max_ctas = 1;
@@ -101,6 +105,7 @@ struct mpsqmc_ctx {
   // couplings of any range and the energy channels of their compact MPO
   bool nn = true;   // every coupling is (i, i+1)
   int sweep = MPSQMC_SWEEP_AUTO;
+  int workspace = MPSQMC_WORKSPACE_AUTO;
   long choff = 0;
   int *d_cp_j = nullptr, *d_cp_q = nullptr, *d_site_c0 = nullptr, *d_ech_off = nullptr, *d_ech_slot = nullptr,
       *d_ech_cont = nullptr, *d_eopen = nullptr;
@@ -186,6 +191,7 @@ mq::Dev make_dev(mpsqmc_ctx *c) {
   p.ech_cont = c->d_ech_cont;
   p.eopen = c->d_eopen;
   p.choff = c->choff;
+  p.gwoff = c->gwoff;
   return p;
 }
 
@@ -221,6 +227,33 @@ void free_all(mpsqmc_ctx *c) {
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+// Where the matrix work buffers of a CTA live: shared memory when they fit (and are not forced
+// out), else the CTA's global scratch.  Sets the scratch stride, the dynamic shared memory of
+// every walker kernel and the persistent grid size.
+int layout_workspace(mpsqmc_ctx *c, bool force_global) {
+  const bool global = force_global || sizeof(double) * (size_t)c->all_doubles > c->smem_optin;
+  c->scr_stride = (c->scr_base + 31) & ~31L;
+  c->gwoff = -1;
+  c->smem_bytes = sizeof(double) * (size_t)c->all_doubles;
+  if (global) {
+    c->gwoff = c->scr_stride;
+    c->scr_stride = (c->gwoff + c->big_doubles + 31) & ~31L;
+    c->smem_bytes = sizeof(double) * (size_t)(c->all_doubles - c->big_doubles);
+  }
+  c->global_work = global;
+  if (c->smem_bytes > c->smem_optin)
+    return fail(MPSQMC_E_UNSUPPORTED, "grid too large for the shared-memory budget of one CTA");
+  const void *kernels[] = {(const void *)mq::walker_step_kernel, (const void *)mq::set_overlap_kernel,
+                           (const void *)mq::energy_kernel, (const void *)mq::walker_step_general_kernel,
+                           (const void *)mq::energy_general_kernel};
+  for (const void *k : kernels)
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes));
+  int occ = 1;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mq::walker_step_kernel, mq::kThreads, c->smem_bytes));
+  c->max_ctas = std::max(1, occ) * c->sm_count;
+  return 0;
 }
 
 }  // namespace
@@ -358,8 +391,8 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   c->pa = mq::padld(std::max(c->maxA, c->maxB));  // slots also hold walker-row matrices
   c->pb = mq::padld(c->maxB);
   c->pq = mq::padld(d * c->maxB);
-  c->smem_bytes = sizeof(double) * (size_t)mq::smem_doubles(c->maxA, c->maxB, c->G, c->pa, c->pb, c->pq,
-                                                            nullptr, nullptr);
+  c->all_doubles =
+      mq::smem_doubles(c->maxA, c->maxB, c->G, c->pa, c->pb, c->pq, nullptr, nullptr, nullptr, &c->big_doubles);
   c->roff.resize(L + 1);
   long ro = 0;
   for (int k = 0; k <= L; ++k) {
@@ -373,8 +406,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   }
   c->foff = ro;
   c->choff = ro + 2L * 4 * c->maxA * c->maxB;
-  c->scr_stride = c->choff + (2L + 3L * nslots) * c->maxA * c->maxB;
-  c->scr_stride = (c->scr_stride + 31) & ~31L;
+  c->scr_base = c->choff + (2L + 3L * nslots) * c->maxA * c->maxB;
   for (int s = 0; s < 2; ++s)
     for (int t = 0; t < 2; ++t) {
       c->opSx[s + 2 * t] = op_sx(d, s, t);
@@ -389,23 +421,14 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   };
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) return bail(fail(MPSQMC_E_CUDA, "properties"));
-  if (c->smem_bytes > (size_t)prop.sharedMemPerBlockOptin)
-    return bail(fail(MPSQMC_E_UNSUPPORTED, "bond dimensions exceed the shared-memory budget of one CTA"));
   c->sm_count = prop.multiProcessorCount;
-  if (cudaFuncSetAttribute(mq::walker_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)c->smem_bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(mq::set_overlap_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)c->smem_bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(mq::energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)c->smem_bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(mq::walker_step_general_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)c->smem_bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(mq::energy_general_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)c->smem_bytes) != cudaSuccess)
-    return bail(fail(MPSQMC_E_CUDA, "cudaFuncSetAttribute failed"));
-  int occ = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mq::walker_step_kernel, mq::kThreads, c->smem_bytes);
-  c->max_ctas = std::max(1, occ) * c->sm_count;
+  c->smem_optin = prop.sharedMemPerBlockOptin;
+  if (c->maxB > mq::kThreads / 2)
+    return bail(fail(MPSQMC_E_UNSUPPORTED, "walker bond dimension above 128 (one QR column group per warp)"));
+  {
+    const int rc = layout_workspace(c, false);
+    if (rc) return bail(rc);
+  }
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(MPSQMC_E_CUDA, "stream"));
   for (auto &e : c->ev)
@@ -772,6 +795,19 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
         return fail(MPSQMC_E_UNSUPPORTED, "the nearest-neighbour sweep needs every coupling to be (i, i+1)");
       c->sweep = (int)value;
       break;
+    case MPSQMC_OPT_WORKSPACE: {
+      if (value != MPSQMC_WORKSPACE_AUTO && value != MPSQMC_WORKSPACE_GLOBAL)
+        return fail(MPSQMC_E_ARG, "unknown workspace placement");
+      CK(cudaSetDevice(c->device));
+      CK(cudaStreamSynchronize(c->stream));
+      const int rc = layout_workspace(c, value == MPSQMC_WORKSPACE_GLOBAL);
+      if (rc) return rc;
+      cudaFree(c->d_scratch);
+      c->d_scratch = nullptr;
+      if (dalloc(&c->d_scratch, (size_t)c->max_ctas * c->scr_stride)) return MPSQMC_E_CUDA;
+      c->workspace = (int)value;
+      break;
+    }
     default:
       return fail(MPSQMC_E_ARG, "unknown option");
   }
@@ -787,6 +823,9 @@ int mpsqmc_get_option(mpsqmc_ctx *c, int option, long *value) {
   switch (option) {
     case MPSQMC_OPT_SWEEP:
       *value = c->sweep;
+      return 0;
+    case MPSQMC_OPT_WORKSPACE:
+      *value = c->global_work ? MPSQMC_WORKSPACE_GLOBAL : MPSQMC_WORKSPACE_AUTO;
       return 0;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");

@@ -452,7 +452,8 @@ static __device__ __noinline__ void cta_householder_qr(int m, int n, double *A, 
     const double ti = tau[i];
     if (ti != 0.0) {
       if (n <= 4 * kWarps) warp_apply_reflector<4>(m, n, i, col, ti, A, lda);
-      else warp_apply_reflector<8>(m, n, i, col, ti, A, lda);
+      else if (n <= 8 * kWarps) warp_apply_reflector<8>(m, n, i, col, ti, A, lda);
+      else warp_apply_reflector<16>(m, n, i, col, ti, A, lda);
     }
   }
   __syncthreads();
@@ -467,7 +468,8 @@ static __device__ __noinline__ void cta_householder_qr(int m, int n, double *A, 
     const double ti = tau[i];
     if (ti != 0.0 && i < n - 1) {
       if (n <= 4 * kWarps) warp_apply_reflector<4>(m, n, i, col, ti, A, lda);
-      else warp_apply_reflector<8>(m, n, i, col, ti, A, lda);
+      else if (n <= 8 * kWarps) warp_apply_reflector<8>(m, n, i, col, ti, A, lda);
+      else warp_apply_reflector<16>(m, n, i, col, ti, A, lda);
     }
     __syncthreads();
     if (warp == i % kWarps) {

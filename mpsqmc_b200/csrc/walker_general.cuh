@@ -295,7 +295,7 @@ static __device__ double norm_from_centre(const Dev &p, Smem &s, const double *W
 __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p) {
   extern __shared__ double smem_raw[];
   Smem s;
-  smem_doubles(p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw);
+  carve(p, s, smem_raw);
   const int L = p.L, d = kMaxD, tid = threadIdx.x;
   const int N = *p.n_cur;
   double *scr = p.scratch + (long)blockIdx.x * p.scr_stride;
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p)
 __global__ void __launch_bounds__(kThreads, 1) energy_general_kernel(Dev p) {
   extern __shared__ double smem_raw[];
   Smem s;
-  smem_doubles(p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw);
+  carve(p, s, smem_raw);
   const int L = p.L, tid = threadIdx.x;
   const int N = *p.n_cur;
   double *scr = p.scratch + (long)blockIdx.x * p.scr_stride;

@@ -72,6 +72,7 @@ struct Dev {
   const int *ech_cont;     // per entry: 1 if site i still has a partner beyond k
   const int *eopen;        // [L]: slot of the channel that site k opens, or -1
   long choff;              // energy channels inside a CTA's scratch: 2 "done" + 3 per slot
+  long gwoff;              // matrix work buffers inside a CTA's scratch, or -1 (shared memory)
 };
 
 enum : int { kErrNumeric = 1, kErrCapacity = 2 };
@@ -87,23 +88,31 @@ struct Smem {
   int sbC, sbX;  // sigma-block strides of Cen/Nxt and of Xb/Pb
 };
 
+// Work buffers of one CTA.  The small ones always live in shared memory.  The matrix buffers
+// (environments, site tensors, branches, QR panel) follow them in shared memory when they fit;
+// for large bond dimensions they live in the CTA's global scratch instead (big != nullptr), where
+// the GEMMs read them through L1/L2.  Returns the doubles placed in shared memory; *big_doubles
+// (if given) receives the size of the matrix buffers.
 __host__ __device__ inline long smem_doubles(int maxA, int maxB, int G, int pa, int pb, int pq,
-                                              Smem *s, double *base) {
-  long off = 0;
+                                              Smem *s, double *base, double *big = nullptr,
+                                              long *big_doubles = nullptr) {
+  long off = 0, boff = 0;
+  double *dummy;
   auto take = [&](double *&p, long n) {
     if (s) p = base + off;
     off += (n + 3) & ~3L;
   };
-  double *dummy;
+  auto take_big = [&](double *&p, long n) {
+    const long r = (n + 3) & ~3L;
+    if (big) {
+      if (s) p = big + boff;
+    } else {
+      if (s) p = base + off;
+      off += r;
+    }
+    boff += r;
+  };
   const int d = kMaxD;
-  take(s ? s->Lenv : dummy, (long)pa * maxB);
-  take(s ? s->Cen : dummy, (long)pb * maxB * d);
-  take(s ? s->Nxt : dummy, (long)pb * maxB * d);
-  take(s ? s->Xb : dummy, (long)pa * maxB * d);
-  take(s ? s->Pb : dummy, (long)pa * maxB * kN2);
-  take(s ? s->Qt : dummy, (long)pa * maxB);
-  take(s ? s->QRb : dummy, (long)pq * maxB);
-  take(s ? s->Rf : dummy, (long)pb * maxB);
   take(s ? s->red : dummy, 4 * kWarps);
   take(s ? s->tau : dummy, maxB);
   take(s ? s->wv : dummy, maxB);
@@ -113,11 +122,27 @@ __host__ __device__ inline long smem_doubles(int maxA, int maxB, int G, int pa, 
   take(s ? s->O2 : dummy, 4);
   take(s ? s->pdf : dummy, G);
   take(s ? s->sc : dummy, 16);
+  take_big(s ? s->Lenv : dummy, (long)pa * maxB);
+  take_big(s ? s->Cen : dummy, (long)pb * maxB * d);
+  take_big(s ? s->Nxt : dummy, (long)pb * maxB * d);
+  take_big(s ? s->Xb : dummy, (long)pa * maxB * d);
+  take_big(s ? s->Pb : dummy, (long)pa * maxB * kN2);
+  take_big(s ? s->Qt : dummy, (long)pa * maxB);
+  take_big(s ? s->QRb : dummy, (long)pq * maxB);
+  take_big(s ? s->Rf : dummy, (long)pb * maxB);
+  if (big_doubles) *big_doubles = boff;
   if (s) {
     s->sbC = pb * maxB;
     s->sbX = pa * maxB;
   }
   return off;
+}
+
+// Carve the work buffers of the calling CTA (shared memory, plus its global scratch when the
+// matrix buffers do not fit on chip).
+__device__ __forceinline__ void carve(const Dev &p, Smem &s, double *smem_raw) {
+  double *big = (p.gwoff >= 0) ? p.scratch + (long)blockIdx.x * p.scr_stride + p.gwoff : nullptr;
+  smem_doubles(p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw, big);
 }
 
 // dst[sigma*sb + r + ld*c] = src[r + dl*(c + dr*sigma)]   (site storage -> padded smem)
@@ -217,7 +242,7 @@ static __device__ void env_update(const Dev &p, Smem &s, const double *B, int al
 __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
   extern __shared__ double smem_raw[];
   Smem s;
-  smem_doubles(p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw);
+  carve(p, s, smem_raw);
   const int L = p.L, d = kMaxD, tid = threadIdx.x;
   const int N = *p.n_cur;
   double *scr = p.scratch + (long)blockIdx.x * p.scr_stride;
@@ -497,7 +522,7 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
 __global__ void __launch_bounds__(kThreads, 1) set_overlap_kernel(Dev p) {
   extern __shared__ double smem_raw[];
   Smem s;
-  smem_doubles(p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw);
+  carve(p, s, smem_raw);
   const int L = p.L, d = kMaxD, tid = threadIdx.x;
   const int N = *p.n_cur;
   for (int w = blockIdx.x; w < N; w += gridDim.x) {
@@ -563,7 +588,7 @@ __global__ void __launch_bounds__(kThreads, 1) set_overlap_kernel(Dev p) {
 __global__ void __launch_bounds__(kThreads, 1) energy_kernel(Dev p) {
   extern __shared__ double smem_raw[];
   Smem s;
-  smem_doubles(p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw);
+  carve(p, s, smem_raw);
   const int L = p.L, tid = threadIdx.x;
   const int N = *p.n_cur;
   double *scr = p.scratch + (long)blockIdx.x * p.scr_stride;

@@ -14,7 +14,7 @@ import pytest
 from conftest import WALK_CASES, couplings, load_golden
 from mpsqmc_b200 import Engine
 from mpsqmc_b200 import problem as pb
-from mpsqmc_b200.capi import OPT_SWEEP, SWEEP_GENERAL
+from mpsqmc_b200.capi import OPT_SWEEP, OPT_WORKSPACE, SWEEP_GENERAL, WORKSPACE_GLOBAL
 from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu
@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-10
 
 
-def engine_for(z, capacity=None, sweep=None):
+def engine_for(z, capacity=None, sweep=None, workspace=None):
     meta = z["meta"]
     L, N = meta["L"], meta["Nw"]
     ci, cj, cJ = couplings(z)
@@ -34,6 +34,9 @@ def engine_for(z, capacity=None, sweep=None):
     eng.set_rng(meta["seed"], meta["setup_draws"])
     if sweep is not None:
         eng.set_option(OPT_SWEEP, sweep)
+    if workspace is not None:
+        eng.set_option(OPT_WORKSPACE, workspace)
+        assert eng.get_option(OPT_WORKSPACE) == workspace
     return eng
 
 
@@ -43,14 +46,20 @@ def fidelity(dims_a, a, dims_b, b):
     return ab / np.sqrt(po.inner_product(A, A) * po.inner_product(B, B))
 
 
-@pytest.mark.parametrize("sweep", [None, SWEEP_GENERAL], ids=["auto", "general"])
+MODES = {"auto": (None, None), "general": (SWEEP_GENERAL, None), "global-ws": (None, WORKSPACE_GLOBAL),
+         "general-global-ws": (SWEEP_GENERAL, WORKSPACE_GLOBAL)}
+
+
+@pytest.mark.parametrize("mode", list(MODES))
 @pytest.mark.parametrize("case", WALK_CASES)
-def test_walk_matches_reference(case, sweep):
+def test_walk_matches_reference(case, mode):
     """Chains run the nearest-neighbour sweep by default and, forced, the general sweep; 2D
-    lattices always run the general sweep."""
+    lattices always run the general sweep.  "global-ws" keeps the matrix work buffers in global
+    scratch (the placement large bond dimensions use) instead of shared memory."""
     z = load_golden(case)
     meta = z["meta"]
-    eng = engine_for(z, sweep=sweep)
+    sweep, ws = MODES[mode]
+    eng = engine_for(z, sweep=sweep, workspace=ws)
     assert eng.energy() == pytest.approx(meta["E0"], rel=RTOL)
     total_draws = 0
     for s in range(1, meta["steps"] + 1):
