@@ -150,6 +150,14 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
 #define MPSQMC_OPT_WORKSPACE 2    /* where a CTA's matrix work buffers live: */
 #define MPSQMC_WORKSPACE_AUTO 0   /*   shared memory when they fit, else global scratch (L2-cached) */
 #define MPSQMC_WORKSPACE_GLOBAL 1 /*   always global scratch (reads the option back as the placement in use) */
+#define MPSQMC_OPT_POPCONTROL_INTERVAL 3 /* population control every K >= 1 steps (default 1, as the
+                                          * reference); on the steps between, weights are only
+                                          * rescaled by Ndesired / sum(w) and no uniform is drawn */
+#define MPSQMC_OPT_RESAMPLING 4   /* population control rule: */
+#define MPSQMC_RESAMPLE_THRESHOLD 0 /* the reference's threshold branching (MPSQMC2.cpp:613-686) */
+#define MPSQMC_RESAMPLE_COMB 1    /*   comb: one uniform u, walker w gets the teeth k + u in
+                                   *   [S_w, S_w + s_w) of the running sum of scaled weights s,
+                                   *   each copy with weight 1 (about Ndesired walkers) */
 int mpsqmc_set_option(mpsqmc_ctx *ctx, int option, long value);
 int mpsqmc_get_option(mpsqmc_ctx *ctx, int option, long *value);
 

@@ -19,6 +19,9 @@ OPT_SWEEP = 1
 SWEEP_AUTO, SWEEP_NEAREST, SWEEP_GENERAL = 0, 1, 2
 OPT_WORKSPACE = 2
 WORKSPACE_AUTO, WORKSPACE_GLOBAL = 0, 1
+OPT_POPCONTROL_INTERVAL = 3
+OPT_RESAMPLING = 4
+RESAMPLE_THRESHOLD, RESAMPLE_COMB = 0, 1
 
 # Every symbol include/mpsqmc_gpu.h declares.
 EXPORTED = [

@@ -106,6 +106,9 @@ struct mpsqmc_ctx {
   bool nn = true;   // every coupling is (i, i+1)
   int sweep = MPSQMC_SWEEP_AUTO;
   int workspace = MPSQMC_WORKSPACE_AUTO;
+  int pc_interval = 1;                  // population control every pc_interval steps
+  int resample = MPSQMC_RESAMPLE_THRESHOLD;
+  int *d_ncop = nullptr;                // copies per walker in the branching step
   long choff = 0;
   int *d_cp_j = nullptr, *d_cp_q = nullptr, *d_site_c0 = nullptr, *d_ech_off = nullptr, *d_ech_slot = nullptr,
       *d_ech_cont = nullptr, *d_eopen = nullptr;
@@ -218,7 +221,7 @@ void free_all(mpsqmc_ctx *c) {
                   c->d_ovout, c->d_wtout, c->d_sw, c->d_uni, c->d_ubr, c->d_bond_c, c->d_bond_j,
                   c->d_bondJ, c->d_tabU, c->d_tabS, c->d_tabVT, c->d_grid, c->d_scratch, c->d_trace,
                   c->d_err, c->d_mt, c->d_sd, c->d_cp_j, c->d_cp_q, c->d_site_c0, c->d_ech_off,
-                  c->d_ech_slot, c->d_ech_cont, c->d_eopen, c->d_ech_J};
+                  c->d_ech_slot, c->d_ech_cont, c->d_eopen, c->d_ech_J, c->d_ncop};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
@@ -448,7 +451,8 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
         dalloc(&c->d_scratch, (size_t)c->max_ctas * c->scr_stride) | dalloc(&c->d_err, 1) |
         dalloc(&c->d_mt, 1) | dalloc(&c->d_sd, 1) | dalloc(&c->d_cp_j, c->nC) | dalloc(&c->d_cp_q, c->nC) |
         dalloc(&c->d_site_c0, L + 1) | dalloc(&c->d_ech_off, L + 1) | dalloc(&c->d_ech_slot, ech_slot.size()) |
-        dalloc(&c->d_ech_cont, ech_cont.size()) | dalloc(&c->d_eopen, L) | dalloc(&c->d_ech_J, ech_J.size());
+        dalloc(&c->d_ech_cont, ech_cont.size()) | dalloc(&c->d_eopen, L) | dalloc(&c->d_ech_J, ech_J.size()) |
+        dalloc(&c->d_ncop, cap);
   if (rc) return bail(MPSQMC_E_CUDA);
   if (cudaMallocHost((void **)&c->h_sd, sizeof(mq::StepDev)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_err, sizeof(int)) != cudaSuccess)
@@ -593,7 +597,8 @@ int mpsqmc_energy(mpsqmc_ctx *c, double *E_P) {
   else
     mq::energy_kernel<<<grid_for(c, c->n_cur), mq::kThreads, c->smem_bytes, c->stream>>>(p);
   CK(cudaGetLastError());
-  mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 0, c->d_flag_pos, c->d_sw);
+  mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 0, c->d_flag_pos, c->d_sw, 1,
+                                              mq::kResampleThreshold);
   CK(cudaGetLastError());
   mq::StepDev sd;
   CK(cudaMemcpyAsync(&sd, c->d_sd, sizeof sd, cudaMemcpyDeviceToHost, c->stream));
@@ -636,11 +641,12 @@ static int enqueue_step(mpsqmc_ctx *c, int *launches) {
       mq::energy_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
     n += 3;
   }
-  mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 1, c->d_flag_pos, c->d_sw);
+  mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 1, c->d_flag_pos, c->d_sw,
+                                              c->pc_interval, c->resample);
   mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, &c->d_sd->n_flag, 0, 1, c->d_ubr);
   mq::branch_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->d_flag_pos, c->d_sw, c->d_ubr, c->d_slot_new,
                                                c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
-                                               c->capacity);
+                                               c->capacity, c->d_ncop, c->pc_interval, c->resample);
   mq::copy_walkers_kernel<<<4 * c->sm_count, 256, 0, c->stream>>>(p, c->d_sd, c->d_copy_src, c->d_copy_dst);
   mq::finish_branch_kernel<<<1, 1024, 0, c->stream>>>(c->d_sd, c->d_ncur, c->d_slot_of, c->d_slot_new, c->d_err,
                                                       c->capacity);
@@ -808,6 +814,15 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
       c->workspace = (int)value;
       break;
     }
+    case MPSQMC_OPT_POPCONTROL_INTERVAL:
+      if (value < 1 || value > (1L << 30)) return fail(MPSQMC_E_ARG, "population-control interval must be >= 1");
+      c->pc_interval = (int)value;
+      break;
+    case MPSQMC_OPT_RESAMPLING:
+      if (value != MPSQMC_RESAMPLE_THRESHOLD && value != MPSQMC_RESAMPLE_COMB)
+        return fail(MPSQMC_E_ARG, "unknown resampling");
+      c->resample = (int)value;
+      break;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");
   }
@@ -826,6 +841,12 @@ int mpsqmc_get_option(mpsqmc_ctx *c, int option, long *value) {
       return 0;
     case MPSQMC_OPT_WORKSPACE:
       *value = c->global_work ? MPSQMC_WORKSPACE_GLOBAL : MPSQMC_WORKSPACE_AUTO;
+      return 0;
+    case MPSQMC_OPT_POPCONTROL_INTERVAL:
+      *value = c->pc_interval;
+      return 0;
+    case MPSQMC_OPT_RESAMPLING:
+      *value = c->resample;
       return 0;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");

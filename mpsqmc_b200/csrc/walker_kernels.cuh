@@ -743,13 +743,22 @@ __device__ double block_sum_d(double v, double *buf) {  // blockDim.x == 1024
   return s;
 }
 
+// Population control modes (mpsqmc_set_option): threshold branching of the reference, or comb
+// (systematic) resampling to Ndesired equal-weight walkers; either every `interval` steps, with
+// the weights only rescaled by Ndesired / sum(w) on the steps in between.
+enum : int { kResampleThreshold = 0, kResampleComb = 1 };
+
 // Weight sum, E_T, E_P, energy history, fluctuation metric (MPSQMC2.cpp:468-487, 688-747),
 // then the branching flags of SeparatePopulationControl (613-648).
 // The step number (1-based, for e_j = Ehist_j / step) is sd->step + 1; finish_branch_kernel
 // advances sd->step, so a captured step graph needs no per-step argument.
+// Uniforms needed by the branching (n_flag): one per walker whose scaled weight leaves
+// [0.25, 1.5] (threshold), one per resampling (comb), none on steps without population control.
 __global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Ndesired, double dtau,
-                                                     int update_history, int *flag_pos, double *sw_out) {
+                                                     int update_history, int *flag_pos, double *sw_out,
+                                                     int interval, int mode) {
   const int step = sd->step + 1;
+  const bool branch_now = (step % interval) == 0;
   __shared__ double dbuf[32];
   __shared__ int ibuf[32];
   const int N = sd->n_cur;
@@ -785,7 +794,7 @@ __global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Nde
     if (w < N) {
       s = p.wt_out[w] * scaling;
       sw_out[w] = s;
-      f = (s < 0.25 || s > 1.5) ? 1 : 0;
+      f = (branch_now && mode == kResampleThreshold && (s < 0.25 || s > 1.5)) ? 1 : 0;
     }
     int tot;
     const int ex = block_scan_excl<int>(f, ibuf, tot);
@@ -798,30 +807,46 @@ __global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Nde
     sd->ET = log(scaling) / dtau;
     sd->EP = numer / sumw;
     sd->omega = update_history ? (sE2 - sE * sE / N) / N : 0.0;
-    sd->n_flag = nflag_total;
+    sd->n_flag = (branch_now && mode == kResampleComb) ? 1 : nflag_total;
     if (!(isfinite(sumw) && sumw > 0.0 && isfinite(numer))) atomicOr(p.err, kErrNumeric);
   }
 }
 
-// Threshold branching (MPSQMC2.cpp:620-686) with a slot table: the first copy of a surviving
-// walker keeps its slot, extra copies take free slots, killed walkers free theirs.
+// Branching with a slot table: the first copy of a surviving walker keeps its slot, extra copies
+// take free slots, killed walkers free theirs.  Copies per walker:
+//   threshold (MPSQMC2.cpp:620-686): int(s + u) for flagged walkers, else 1;
+//   comb: the teeth k + u (k = 0, 1, ...) that fall in [S_w, S_w + s_w), S_w the running sum of
+//         the scaled weights in walker order (summed sequentially, as the oracle does), weight 1;
+//   steps without population control: one copy with the scaled weight.
 __global__ void __launch_bounds__(1024) branch_kernel(Dev p, StepDev *sd, const int *flag_pos,
                                                       const double *sw_in, const double *ubr,
                                                       int *slot_of_new, int *free_slots,
                                                       int *copy_src, int *copy_dst, int *parent,
-                                                      int capacity) {
+                                                      int capacity, int *ncop, int interval, int mode) {
   __shared__ int ibuf[32];
   const int N = sd->n_cur;
+  const bool comb = mode == kResampleComb && ((sd->step + 1) % interval) == 0;
   int nfree = sd->n_free;
   int new_total = 0, extra_total = 0, killed_total = 0;
+  if (comb) {
+    if (threadIdx.x == 0) {
+      const double u = ubr[0];
+      double S = 0.0;
+      for (int w = 0; w < N; ++w) {
+        const double s = sw_in[w];
+        ncop[w] = (int)(ceil(S + s - u) - ceil(S - u));
+        S += s;
+      }
+    }
+  } else {
+    for (int w = threadIdx.x; w < N; w += 1024)
+      ncop[w] = (flag_pos[w] >= 0) ? (int)(sw_in[w] + ubr[flag_pos[w]]) : 1;
+  }
+  __syncthreads();
   // pass 1: killed slots onto the free stack (in walker order)
   for (int base = 0; base < N; base += 1024) {
     const int w = base + threadIdx.x;
-    int nc = 1;
-    if (w < N) {
-      const double s = sw_in[w];
-      if (flag_pos[w] >= 0) nc = (int)(s + ubr[flag_pos[w]]);
-    }
+    const int nc = (w < N) ? ncop[w] : 1;
     int tot;
     const int k = block_scan_excl<int>((w < N && nc == 0) ? 1 : 0, ibuf, tot);
     if (w < N && nc == 0) free_slots[nfree + killed_total + k] = p.slot_of[w];
@@ -836,12 +861,10 @@ __global__ void __launch_bounds__(1024) branch_kernel(Dev p, StepDev *sd, const 
     double s = 0.0, neww = 0.0;
     if (w < N) {
       s = sw_in[w];
-      nc = 1;
+      nc = ncop[w];
       neww = s;
-      if (flag_pos[w] >= 0) {
-        nc = (int)(s + ubr[flag_pos[w]]);
-        neww = (s < 0.25) ? 1.0 : s / nc;
-      }
+      if (comb) neww = 1.0;
+      else if (flag_pos[w] >= 0) neww = (s < 0.25) ? 1.0 : s / nc;
     }
     int tot_new, tot_extra;
     const int pos = block_scan_excl<int>(nc, ibuf, tot_new);

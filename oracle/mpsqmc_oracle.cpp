@@ -975,21 +975,33 @@ int orc_walk(const orc_walk_config *cfg, const int *dimsT, const double *trial, 
       if (pw_overlap) pw_overlap[(size_t)s0 * cap + w] = overlaps[w];
       if (pw_energy) pw_energy[(size_t)s0 * cap + w] = energy[w];
     }
-    // SeparatePopulationControl, MPSQMC2.cpp:613-686.
+    // SeparatePopulationControl, MPSQMC2.cpp:613-686 (threshold), or the engine's comb and
+    // interval variants (orc_walk_config).
     int Nn = 0;
     std::vector<double> nw, no, nh;
     std::vector<int> par;
+    const int K = cfg->popctl_interval > 0 ? cfg->popctl_interval : 1;
+    const bool branch_now = (step % K) == 0;
+    const bool comb = branch_now && cfg->comb != 0;
+    const double ucomb = comb ? rng.uniform() : 0.0;
+    double Scomb = 0.0;
     for (int w = 0; w < N; ++w) {
       const double sw = weights[w] * scaling;
       int nCopies = 1;
       double newW = sw;
-      if (newW < 0.25) {
-        nCopies = (int)(sw + rng.uniform());
+      if (comb) {
+        nCopies = (int)(std::ceil(Scomb + sw - ucomb) - std::ceil(Scomb - ucomb));
+        Scomb += sw;
         newW = 1.0;
-      }
-      if (newW > 1.5) {
-        nCopies = (int)(sw + rng.uniform());
-        newW = sw / nCopies;
+      } else if (branch_now) {
+        if (newW < 0.25) {
+          nCopies = (int)(sw + rng.uniform());
+          newW = 1.0;
+        }
+        if (newW > 1.5) {
+          nCopies = (int)(sw + rng.uniform());
+          newW = sw / nCopies;
+        }
       }
       if (Nn + nCopies > cap) return -1;
       for (int c = 0; c < nCopies; ++c) {

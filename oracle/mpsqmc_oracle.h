@@ -73,6 +73,12 @@ typedef struct {
   double dtau, h;
   unsigned int seed;
   unsigned long long skip;
+  /* Population-control variants of the engine (no counterpart in the reference; 0, 0 is the
+   * reference): popctl_interval K > 1 branches on steps divisible by K and only rescales the
+   * weights by Ndesired / sum(w) in between; comb != 0 resamples with one uniform u, walker w
+   * getting the teeth k + u inside [S_w, S_w + s_w) of the sequential running sum S of the
+   * scaled weights s, each copy with weight 1. */
+  int popctl_interval, comb;
 } orc_walk_config;
 
 int orc_walk(const orc_walk_config *cfg, const int *dimsT, const double *trial, const int *ci,

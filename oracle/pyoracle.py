@@ -48,6 +48,7 @@ class WalkConfig(C.Structure):
         ("L", C.c_int), ("d", C.c_int), ("nC", C.c_int), ("nJ", C.c_int), ("G", C.c_int),
         ("Ndesired", C.c_int), ("capacity", C.c_int), ("nsteps", C.c_int), ("nthreads", C.c_int),
         ("dtau", C.c_double), ("h", C.c_double), ("seed", C.c_uint), ("skip", C.c_ulonglong),
+        ("popctl_interval", C.c_int), ("comb", C.c_int),
     ]
 
 
@@ -259,7 +260,7 @@ class WalkResult:
 
 def walk(trial: MPS, walkers: np.ndarray, dimsW, weights, overlaps, ehist, *, ci, cj, cJ, Jvals,
          U, S, VT, grid, dtau, nsteps, Ndesired, capacity, seed, skip=0, h=0.0, trace=False,
-         nthreads=0) -> WalkResult:
+         nthreads=0, popctl_interval=1, comb=False) -> WalkResult:
     """MPSQMC2::Walk on the CPU (restatement).  walkers: [N, size] float64."""
     N = walkers.shape[0]
     size = mps_size(dimsW, trial.d)
@@ -280,7 +281,7 @@ def walk(trial: MPS, walkers: np.ndarray, dimsW, weights, overlaps, ehist, *, ci
     draws = C.c_ulonglong(0)
     cfg = WalkConfig(L=trial.L, d=trial.d, nC=nC, nJ=len(Jvals), G=grid.shape[0], Ndesired=Ndesired,
                      capacity=capacity, nsteps=nsteps, nthreads=nthreads, dtau=dtau, h=h, seed=seed,
-                     skip=skip)
+                     skip=skip, popctl_interval=popctl_interval, comb=int(comb))
     ptr = lambda a: a.ctypes.data_as(C.c_void_p) if a is not None else None
     status = lib().orc_walk(C.byref(cfg), _i32(trial.dims), _f64(trial.data), _i32(ci), _i32(cj),
                             _f64(cJ), _f64(Jvals), _f64(U), _f64(S), _f64(VT), _f64(grid), _i32(dimsW),
