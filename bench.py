@@ -228,12 +228,15 @@ def main():
     if not args.no_e2e:
         eng2 = Engine(device=local, **inputs)
         eng2.set_option(OPT_SWEEP, sweep)
-        host_w = np.ascontiguousarray(walkers)
+        # the population in pinned host memory (both directions), as a serving caller would keep it
+        host_w = torch.empty(walkers.shape, dtype=torch.float64, pin_memory=True).numpy()
+        host_w[:] = walkers
+        back_w = torch.empty((eng2.capacity, eng2.walker_size), dtype=torch.float64, pin_memory=True).numpy()
         t0 = time.perf_counter()
         eng2.set_walkers(host_w, np.ones(N), None, np.zeros(N), normalize=True)
         eng2.set_rng(wl.seed + 7919 * rank, 0)
         st2 = eng2.walk(args.steps)
-        back = eng2.get_walkers()
+        back = eng2.get_walkers(out=back_w)
         t1 = time.perf_counter()
         ws2 = sum(s["n_walkers"] for s in st2)
         nbytes = host_w.nbytes

@@ -100,9 +100,22 @@ int mpsqmc_set_walkers(mpsqmc_ctx *ctx, int N, const double *walkers, const doub
                        const double *overlaps, const double *ehist, int normalize);
 
 /* Download the current population in logical order; *N receives the count.  Any pointer may
- * be NULL.  walkers must hold capacity*walker_size doubles (or the current N). */
+ * be NULL.  walkers must hold capacity*walker_size doubles (or the current N); walker w occupies
+ * walker_size doubles from w*walker_size, its own tensors first (see mpsqmc_get_walker_dims). */
 int mpsqmc_get_walkers(mpsqmc_ctx *ctx, int *N, double *walkers, double *weights,
                        double *overlaps, double *ehist);
+
+/* Walkers of individual bond dimensions (the reference's MPSstate keeps its own VirtualD,
+ * MPSstate.cpp:13-40, and InnerProduct handles differing dims, 264-267).  dims: [N][L+1], each
+ * row valid for the chain and elementwise <= the configuration's walker_dims; walker w's tensors
+ * (sum_s dims[w][s]*dims[w][s+1]*d doubles, reference layout) follow walker w-1's back to back.
+ * Otherwise as mpsqmc_set_walkers.  One launch of every kernel serves all sizes; walkers are
+ * handed to CTAs dynamically. */
+int mpsqmc_set_walkers_dims(mpsqmc_ctx *ctx, int N, const int *dims, const double *walkers,
+                            const double *weights, const double *overlaps, const double *ehist,
+                            int normalize);
+/* Bond dims of the current population in logical order: dims [N][L+1] (may be NULL). */
+int mpsqmc_get_walker_dims(mpsqmc_ctx *ctx, int *N, int *dims);
 
 /* Random stream: mt19937(seed) advanced by `skip` 32-bit outputs; every uniform is one output
  * divided by 2^32 (Random.cpp:28-59 with Boost's uniform_real_distribution). */

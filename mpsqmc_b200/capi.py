@@ -29,7 +29,7 @@ EXPORTED = [
     "mpsqmc_set_walkers", "mpsqmc_get_walkers", "mpsqmc_set_rng", "mpsqmc_get_rng_draws",
     "mpsqmc_energy", "mpsqmc_walk", "mpsqmc_last_step_walkers", "mpsqmc_set_trace",
     "mpsqmc_get_trace", "mpsqmc_last_timing", "mpsqmc_local_energy_noalloc", "mpsqmc_set_step",
-    "mpsqmc_set_option", "mpsqmc_get_option",
+    "mpsqmc_set_option", "mpsqmc_get_option", "mpsqmc_set_walkers_dims", "mpsqmc_get_walker_dims",
 ]
 
 
@@ -109,6 +109,8 @@ def load(build_if_missing: bool = True):
         "mpsqmc_last_timing": (C.c_int, [P, dp, dp, ip]),
         "mpsqmc_set_step": (C.c_int, [P, C.c_int]),
         "mpsqmc_set_option": (C.c_int, [P, C.c_int, C.c_long]),
+        "mpsqmc_set_walkers_dims": (C.c_int, [P, C.c_int, ip, dp, dp, dp, dp, C.c_int]),
+        "mpsqmc_get_walker_dims": (C.c_int, [P, ip, ip]),
         "mpsqmc_get_option": (C.c_int, [P, C.c_int, C.POINTER(C.c_long)]),
         "mpsqmc_local_energy_noalloc": (C.c_int, [C.POINTER(EnergyLayout), P, P, C.c_long, P, C.c_int, P,
                                                   C.c_int, P]),
@@ -181,11 +183,40 @@ class Engine:
         eh = None if ehist is None else np.ascontiguousarray(ehist, dtype=np.float64)
         check(self.lib.mpsqmc_set_walkers(self._ctx, N, _dp(w), _dp(wt), _dp(ov), _dp(eh), int(normalize)))
 
-    def get_walkers(self):
+    def set_walkers_dims(self, dims, walkers, weights, overlaps=None, ehist=None, normalize=True):
+        """Walkers of individual bond dims: dims [N, L+1]; walkers a list of 1-D tensor arrays (or
+        one packed array)."""
+        dm = np.ascontiguousarray(dims, dtype=np.int32)
+        N = dm.shape[0]
+        packed = np.ascontiguousarray(np.concatenate([np.ravel(x) for x in walkers])
+                                      if isinstance(walkers, (list, tuple)) else walkers, dtype=np.float64)
+        wt = np.ascontiguousarray(weights, dtype=np.float64)
+        ov = None if overlaps is None else np.ascontiguousarray(overlaps, dtype=np.float64)
+        eh = None if ehist is None else np.ascontiguousarray(ehist, dtype=np.float64)
+        check(self.lib.mpsqmc_set_walkers_dims(self._ctx, N, _ip(dm), _dp(packed), _dp(wt), _dp(ov), _dp(eh),
+                                               int(normalize)))
+
+    def get_walker_dims(self):
+        n = C.c_int(0)
+        check(self.lib.mpsqmc_get_walker_dims(self._ctx, C.byref(n), None))
+        dm = np.zeros((n.value, self.L + 1), dtype=np.int32)
+        check(self.lib.mpsqmc_get_walker_dims(self._ctx, C.byref(n), _ip(dm)))
+        return dm
+
+    def get_walkers(self, out=None):
+        """(walkers [N, walker_size], weights, overlaps, energy histories).  out: optional
+        float64 C-contiguous array of at least capacity rows (e.g. pinned host memory) that
+        receives the walkers; the returned walkers are a view of it."""
         n = C.c_int(0)
         check(self.lib.mpsqmc_get_walkers(self._ctx, C.byref(n), None, None, None, None))
         N = n.value
-        w = np.zeros((N, self.walker_size))
+        if out is not None:
+            if out.dtype != np.float64 or not out.flags.c_contiguous or out.shape[0] < N or \
+                    out.shape[1] != self.walker_size:
+                raise ValueError("out must be C-contiguous float64 [>= N, walker_size]")
+            w = out[:N]
+        else:
+            w = np.zeros((N, self.walker_size))
         wt, ov, eh = np.zeros(N), np.zeros(N), np.zeros(N)
         check(self.lib.mpsqmc_get_walkers(self._ctx, C.byref(n), _dp(w), _dp(wt), _dp(ov), _dp(eh)))
         return w, wt, ov, eh

@@ -109,6 +109,11 @@ struct mpsqmc_ctx {
   int pc_interval = 1;                  // population control every pc_interval steps
   int resample = MPSQMC_RESAMPLE_THRESHOLD;
   int *d_ncop = nullptr;                // copies per walker in the branching step
+  int *d_wdims = nullptr;               // per slot: the walker's bond dims [capacity][L+1]
+  long *d_wofs = nullptr;               // per slot: its site offsets [capacity][L]
+  int *d_ctr = nullptr;                 // work counters of the persistent kernels
+  double *d_stage = nullptr;            // mpsqmc_get_walkers: walkers gathered into logical order
+  int stage_walkers = 0;
   long choff = 0;
   int *d_cp_j = nullptr, *d_cp_q = nullptr, *d_site_c0 = nullptr, *d_ech_off = nullptr, *d_ech_slot = nullptr,
       *d_ech_cont = nullptr, *d_eopen = nullptr;
@@ -195,6 +200,9 @@ mq::Dev make_dev(mpsqmc_ctx *c) {
   p.eopen = c->d_eopen;
   p.choff = c->choff;
   p.gwoff = c->gwoff;
+  p.wdims = c->d_wdims;
+  p.wofs = c->d_wofs;
+  p.ctr = c->d_ctr;
   return p;
 }
 
@@ -221,7 +229,8 @@ void free_all(mpsqmc_ctx *c) {
                   c->d_ovout, c->d_wtout, c->d_sw, c->d_uni, c->d_ubr, c->d_bond_c, c->d_bond_j,
                   c->d_bondJ, c->d_tabU, c->d_tabS, c->d_tabVT, c->d_grid, c->d_scratch, c->d_trace,
                   c->d_err, c->d_mt, c->d_sd, c->d_cp_j, c->d_cp_q, c->d_site_c0, c->d_ech_off,
-                  c->d_ech_slot, c->d_ech_cont, c->d_eopen, c->d_ech_J, c->d_ncop};
+                  c->d_ech_slot, c->d_ech_cont, c->d_eopen, c->d_ech_J, c->d_ncop, c->d_wdims, c->d_wofs,
+                  c->d_ctr, c->d_stage};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
@@ -395,7 +404,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   c->pb = mq::padld(c->maxB);
   c->pq = mq::padld(d * c->maxB);
   c->all_doubles =
-      mq::smem_doubles(c->maxA, c->maxB, c->G, c->pa, c->pb, c->pq, nullptr, nullptr, nullptr, &c->big_doubles);
+      mq::smem_doubles(L, c->maxA, c->maxB, c->G, c->pa, c->pb, c->pq, nullptr, nullptr, nullptr, &c->big_doubles);
   c->roff.resize(L + 1);
   long ro = 0;
   for (int k = 0; k <= L; ++k) {
@@ -452,7 +461,8 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
         dalloc(&c->d_mt, 1) | dalloc(&c->d_sd, 1) | dalloc(&c->d_cp_j, c->nC) | dalloc(&c->d_cp_q, c->nC) |
         dalloc(&c->d_site_c0, L + 1) | dalloc(&c->d_ech_off, L + 1) | dalloc(&c->d_ech_slot, ech_slot.size()) |
         dalloc(&c->d_ech_cont, ech_cont.size()) | dalloc(&c->d_eopen, L) | dalloc(&c->d_ech_J, ech_J.size()) |
-        dalloc(&c->d_ncop, cap);
+        dalloc(&c->d_ncop, cap) | dalloc(&c->d_wdims, (size_t)cap * (L + 1)) | dalloc(&c->d_wofs, (size_t)cap * L) |
+        dalloc(&c->d_ctr, mq::kNumCtr);
   if (rc) return bail(MPSQMC_E_CUDA);
   if (cudaMallocHost((void **)&c->h_sd, sizeof(mq::StepDev)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_err, sizeof(int)) != cudaSuccess)
@@ -478,6 +488,16 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
             up(c->d_eopen, eopen.data(), sizeof(int) * L) &&
             up(c->d_ech_J, ech_J.data(), sizeof(double) * ech_J.size());
   if (!ok) return bail(fail(MPSQMC_E_CUDA, "upload failed"));
+  {  // every slot starts with the common walker dims
+    std::vector<int> wd((size_t)cap * (L + 1));
+    std::vector<long> wf((size_t)cap * L);
+    for (int q = 0; q < cap; ++q) {
+      std::copy(c->bW.begin(), c->bW.end(), wd.begin() + (size_t)q * (L + 1));
+      std::copy(c->woff.begin(), c->woff.end(), wf.begin() + (size_t)q * L);
+    }
+    if (!up(c->d_wdims, wd.data(), sizeof(int) * wd.size()) || !up(c->d_wofs, wf.data(), sizeof(long) * wf.size()))
+      return bail(fail(MPSQMC_E_CUDA, "upload failed"));
+  }
   if (cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess || cudaMemset(c->d_sd, 0, sizeof(mq::StepDev)) != cudaSuccess ||
       cudaMemset(c->d_ncur, 0, sizeof(int)) != cudaSuccess)
     return bail(fail(MPSQMC_E_CUDA, "memset failed"));
@@ -525,14 +545,47 @@ int mpsqmc_get_rng_draws(mpsqmc_ctx *c, uint64_t *draws) {
   return 0;
 }
 
-int mpsqmc_set_walkers(mpsqmc_ctx *c, int N, const double *walkers, const double *weights,
-                       const double *overlaps, const double *ehist, int normalize) {
+// Upload N walkers into slots 0..N-1.  dims == nullptr: every walker has the common dims and
+// walker_size doubles (stride walker_size); else walker w has dims[w*(L+1) ..] and its tensors
+// follow the previous walker's back to back.
+static int set_walkers_impl(mpsqmc_ctx *c, int N, const int *dims, const double *walkers, const double *weights,
+                            const double *overlaps, const double *ehist, int normalize) {
   if (!c || !walkers || !weights) return fail(MPSQMC_E_ARG, "null argument");
   if (N < 1 || N > c->capacity) return fail(MPSQMC_E_ARG, "walker count outside [1, capacity]");
+  const int L = c->L, d = c->d;
+  std::vector<int> wd((size_t)N * (L + 1));
+  std::vector<long> wf((size_t)N * L);
+  std::vector<long> src_off(N);
+  long pos = 0;
+  for (int w = 0; w < N; ++w) {
+    const int *dw = dims ? dims + (size_t)w * (L + 1) : c->bW.data();
+    if (dims) {
+      if (!valid_dims(dw, L, d)) return fail(MPSQMC_E_ARG, "walker bond dimensions inconsistent with the chain");
+      for (int k = 0; k <= L; ++k)
+        if (dw[k] > c->bW[k]) return fail(MPSQMC_E_ARG, "walker bond dimension above the configured walker_dims");
+    }
+    long o = 0;
+    for (int k = 0; k < L; ++k) {
+      wf[(size_t)w * L + k] = o;
+      o += (long)dw[k] * dw[k + 1] * d;
+    }
+    std::copy(dw, dw + L + 1, wd.begin() + (size_t)w * (L + 1));
+    src_off[w] = pos;
+    pos += dims ? o : c->wsize;
+  }
   CK(cudaSetDevice(c->device));
-  for (int w = 0; w < N; ++w)
-    CK(cudaMemcpyAsync(c->d_walkers + (size_t)w * c->wstride, walkers + (size_t)w * c->wsize,
-                       sizeof(double) * c->wsize, cudaMemcpyHostToDevice, c->stream));
+  if (dims) {
+    for (int w = 0; w < N; ++w) {
+      const long n = (w + 1 < N ? src_off[w + 1] : pos) - src_off[w];
+      CK(cudaMemcpyAsync(c->d_walkers + (size_t)w * c->wstride, walkers + src_off[w], sizeof(double) * n,
+                         cudaMemcpyHostToDevice, c->stream));
+    }
+  } else {
+    CK(cudaMemcpy2DAsync(c->d_walkers, sizeof(double) * c->wstride, walkers, sizeof(double) * c->wsize,
+                         sizeof(double) * c->wsize, N, cudaMemcpyHostToDevice, c->stream));
+  }
+  CK(cudaMemcpyAsync(c->d_wdims, wd.data(), sizeof(int) * wd.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_wofs, wf.data(), sizeof(long) * wf.size(), cudaMemcpyHostToDevice, c->stream));
   std::vector<int> slots(N), freel(c->capacity - N);
   for (int w = 0; w < N; ++w) slots[w] = w;
   for (int q = 0; q < c->capacity - N; ++q) freel[q] = c->capacity - 1 - q;
@@ -556,11 +609,38 @@ int mpsqmc_set_walkers(mpsqmc_ctx *c, int N, const double *walkers, const double
   c->n_cur = N;
   if (normalize) {
     mq::Dev p = make_dev(c);
+    CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(int) * mq::kNumCtr, c->stream));
     mq::set_overlap_kernel<<<grid_for(c, N), mq::kThreads, c->smem_bytes, c->stream>>>(p);
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(c->stream));
   return check_err(c);
+}
+
+int mpsqmc_set_walkers(mpsqmc_ctx *c, int N, const double *walkers, const double *weights,
+                       const double *overlaps, const double *ehist, int normalize) {
+  return set_walkers_impl(c, N, nullptr, walkers, weights, overlaps, ehist, normalize);
+}
+
+int mpsqmc_set_walkers_dims(mpsqmc_ctx *c, int N, const int *dims, const double *walkers, const double *weights,
+                            const double *overlaps, const double *ehist, int normalize) {
+  if (!dims) return fail(MPSQMC_E_ARG, "null dims");
+  return set_walkers_impl(c, N, dims, walkers, weights, overlaps, ehist, normalize);
+}
+
+int mpsqmc_get_walker_dims(mpsqmc_ctx *c, int *N, int *dims) {
+  if (!c) return fail(MPSQMC_E_ARG, "null context");
+  CK(cudaSetDevice(c->device));
+  const int n = c->n_cur, L = c->L;
+  if (N) *N = n;
+  if (!dims) return 0;
+  std::vector<int> slots(n), all((size_t)c->capacity * (L + 1));
+  CK(cudaMemcpy(slots.data(), c->d_slot_of, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(all.data(), c->d_wdims, sizeof(int) * all.size(), cudaMemcpyDeviceToHost));
+  for (int w = 0; w < n; ++w)
+    std::copy(all.begin() + (size_t)slots[w] * (L + 1), all.begin() + (size_t)(slots[w] + 1) * (L + 1),
+              dims + (size_t)w * (L + 1));
+  return 0;
 }
 
 int mpsqmc_get_walkers(mpsqmc_ctx *c, int *N, double *walkers, double *weights, double *overlaps,
@@ -580,10 +660,23 @@ int mpsqmc_get_walkers(mpsqmc_ctx *c, int *N, double *walkers, double *weights, 
   };
   int rc = gather(weights, c->d_weight) | gather(overlaps, c->d_overlap) | gather(ehist, c->d_ehist);
   if (rc) return rc;
-  if (walkers)
-    for (int w = 0; w < n; ++w)
-      CK(cudaMemcpy(walkers + (size_t)w * c->wsize, c->d_walkers + (size_t)slots[w] * c->wstride,
-                    sizeof(double) * c->wsize, cudaMemcpyDeviceToHost));
+  if (walkers && n > 0) {
+    // gather the slots into logical order on the device, then one copy per chunk
+    if (!c->d_stage) {
+      const long per = c->wsize;
+      c->stage_walkers = (int)std::max(1L, std::min<long>(c->capacity, (256L << 20) / (8 * per)));
+      if (dalloc(&c->d_stage, (size_t)c->stage_walkers * per)) return MPSQMC_E_CUDA;
+    }
+    mq::Dev p = make_dev(c);
+    for (int w0 = 0; w0 < n; w0 += c->stage_walkers) {
+      const int m = std::min(c->stage_walkers, n - w0);
+      mq::gather_walkers_kernel<<<std::min(m, 4 * c->sm_count), 256, 0, c->stream>>>(p, w0, m, c->wsize, c->d_stage);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(walkers + (size_t)w0 * c->wsize, c->d_stage, sizeof(double) * (size_t)m * c->wsize,
+                         cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+  }
   return 0;
 }
 
@@ -592,6 +685,7 @@ int mpsqmc_energy(mpsqmc_ctx *c, double *E_P) {
   if (c->n_cur < 1) return fail(MPSQMC_E_ARG, "no walkers");
   CK(cudaSetDevice(c->device));
   mq::Dev p = make_dev(c);
+  CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(int) * mq::kNumCtr, c->stream));
   if (general_sweep(c))
     mq::energy_general_kernel<<<grid_for(c, c->n_cur), mq::kThreads, c->smem_bytes, c->stream>>>(p);
   else
@@ -614,6 +708,7 @@ int mpsqmc_energy(mpsqmc_ctx *c, double *E_P) {
 static int enqueue_step(mpsqmc_ctx *c, int *launches) {
   mq::Dev p = make_dev(c);
   const int grid = c->max_ctas;
+  CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(int) * mq::kNumCtr, c->stream));
   mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, c->d_ncur, 0, c->nC, c->d_uni);
   const bool field = c->h != 0.0;
   int n = 7;

@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(mq::kThreads, 1)
                           double *out, int N) {
   extern __shared__ double smem_raw[];
   mq::Smem s;
-  mq::smem_doubles(p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw);
+  mq::smem_doubles(p.L, p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw);
   const int L = p.L, tid = threadIdx.x;
   double *Fbuf = p.scratch + (long)blockIdx.x * p.scr_stride;
   const int fst = 4 * p.maxA * p.maxB;
@@ -192,7 +192,7 @@ extern "C" int mpsqmc_local_energy_noalloc(const mpsqmc_energy_layout *lay, cons
       }
     p.scratch = st->scratch + kTablesDoubles;
     p.scr_stride = per_cta;
-    const size_t smem = sizeof(double) * (size_t)mq::smem_doubles(maxA, maxB, 1, p.pa, p.pb, p.pq, nullptr, nullptr);
+    const size_t smem = sizeof(double) * (size_t)mq::smem_doubles(p.L, maxA, maxB, 1, p.pa, p.pb, p.pq, nullptr, nullptr);
     if ((int)smem > st->smem_optin) {
       rc = err(MPSQMC_E_UNSUPPORTED, "bond dimensions exceed the shared-memory budget of one CTA");
     } else {

@@ -32,8 +32,8 @@ namespace mq {
 // Uses Nxt and Xb.  Ends with a barrier.
 static __device__ void right_env_step(const Dev &p, Smem &s, const double *W, double *scr, int k) {
   const int d = kMaxD;
-  const int al = p.aT[k], ar = p.aT[k + 1], bl = p.bW[k], br = p.bW[k + 1];
-  load_site(s.Nxt, p.pb, s.sbC, W + p.woff[k], bl, br);
+  const int al = p.aT[k], ar = p.aT[k + 1], bl = s.bW[k], br = s.bW[k + 1];
+  load_site(s.Nxt, p.pb, s.sbC, W + s.woff[k], bl, br);
   __syncthreads();
   const double *Rn = scr + p.roff[k + 1];
   double *Rk = scr + p.roff[k];
@@ -156,7 +156,7 @@ static __device__ void env_update_general(const Dev &p, Smem &s, int k, const do
 // (walker site in Nxt, R[j+1] at Rn): M[p + 4q] = <P_p, B_j[s'] R[j+1] A_j[t']^T>, q = s' + 2t'.
 static __device__ void closures(const Dev &p, Smem &s, int j, const double *Rn) {
   const int d = kMaxD, tid = threadIdx.x;
-  const int aj = p.aT[j], a2 = p.aT[j + 1], bj = p.bW[j], b2 = p.bW[j + 1];
+  const int aj = p.aT[j], a2 = p.aT[j + 1], bj = s.bW[j], b2 = s.bW[j + 1];
   const double *Bj = p.trial + p.toff[j];
   for (int tau = 0; tau < d; ++tau)
     cta_gemm(a2, bj, b2, 1.0, Rn, a2, false, s.Nxt + tau * s.sbC, p.pb, true, 0.0, s.Xb + tau * s.sbX, p.pa);
@@ -264,8 +264,8 @@ static __device__ double norm_from_centre(const Dev &p, Smem &s, const double *W
   if (tid == 0) scr[p.nroff[L]] = 1.0;
   __syncthreads();
   for (int k = L - 1; k > i; --k) {
-    const int bl = p.bW[k], br = p.bW[k + 1];
-    load_site(s.Nxt, p.pb, s.sbC, W + p.woff[k], bl, br);
+    const int bl = s.bW[k], br = s.bW[k + 1];
+    load_site(s.Nxt, p.pb, s.sbC, W + s.woff[k], bl, br);
     __syncthreads();
     const double *Nn = scr + p.nroff[k + 1];
     double *Nk = scr + p.nroff[k];
@@ -277,7 +277,7 @@ static __device__ double norm_from_centre(const Dev &p, Smem &s, const double *W
                sg == 0 ? 0.0 : 1.0, Nk, bl);
     __syncthreads();
   }
-  const int bl = p.bW[i], br = p.bW[i + 1];
+  const int bl = s.bW[i], br = s.bW[i + 1];
   const double *N1 = scr + p.nroff[i + 1];
   for (int sg = 0; sg < d; ++sg)
     cta_gemm(bl, br, br, 1.0, s.Cen + sg * s.sbC, p.pb, false, N1, br, false, 0.0, s.Xb + sg * s.sbX, p.pa);
@@ -302,8 +302,9 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p)
   const long fm = (long)p.maxA * p.maxB;
   double *Fdone[2] = {scr + p.choff, scr + p.choff + fm};
   double *Fch = scr + p.choff + 2 * fm;
-  for (int w = blockIdx.x; w < N; w += gridDim.x) {
+  for (int w = next_walker(s, p.ctr + kCtrStep); w < N; w = next_walker(s, p.ctr + kCtrStep)) {
     const int slot = p.slot_of[w];
+    load_walker_dims(p, s, slot);
     double *W = p.walkers + (long)slot * p.wstride;
     // right environments of the walker as stored
     if (tid == 0) scr[p.roff[L]] = 1.0;
@@ -312,8 +313,8 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p)
     // centre on site 0: overlap <Psi_T|phi> (the stored walker is normalised, overlap > 0)
     double ov;
     {
-      const int a1 = p.aT[1], b1 = p.bW[1];
-      load_site(s.Cen, p.pb, s.sbC, W + p.woff[0], 1, b1);
+      const int a1 = p.aT[1], b1 = s.bW[1];
+      load_site(s.Cen, p.pb, s.sbC, W + s.woff[0], 1, b1);
       __syncthreads();
       const double *R1 = scr + p.roff[1], *B0 = p.trial + p.toff[0];
       double part = 0.0;
@@ -330,7 +331,7 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p)
     int cur = 0;
     __syncthreads();
     for (int i = 0; i < L; ++i) {
-      const int al = p.aT[i], ar = p.aT[i + 1], bl = p.bW[i], br = p.bW[i + 1];
+      const int al = p.aT[i], ar = p.aT[i + 1], bl = s.bW[i], br = s.bW[i + 1];
       const double *Bi = p.trial + p.toff[i];
       for (int c = p.site_c0[i]; c < p.site_c0[i + 1]; ++c) {
         const int j = p.cp_j[c];
@@ -350,23 +351,23 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p)
         __syncthreads();
         // through the middle sites
         for (int m = i + 1; m < j; ++m) {
-          const int am = p.aT[m], am1 = p.aT[m + 1], bm = p.bW[m], bm1 = p.bW[m + 1];
-          load_site(s.Nxt, p.pb, s.sbC, W + p.woff[m], bm, bm1);
+          const int am = p.aT[m], am1 = p.aT[m + 1], bm = s.bW[m], bm1 = s.bW[m + 1];
+          load_site(s.Nxt, p.pb, s.sbC, W + s.woff[m], bm, bm1);
           __syncthreads();
           const double *Bm = p.trial + p.toff[m];
           for (int q = 0; q < kN2; ++q)
             transfer_in_place(p, s, Bm, am, am1, bm, bm1, s.Nxt, p.pb, s.sbC, s.Pb + q * s.sbX, p.pa);
         }
         // right branches at j, closures, sample
-        const int bj = p.bW[j], bj1 = p.bW[j + 1];
-        load_site(s.Nxt, p.pb, s.sbC, W + p.woff[j], bj, bj1);
+        const int bj = s.bW[j], bj1 = s.bW[j + 1];
+        load_site(s.Nxt, p.pb, s.sbC, W + s.woff[j], bj, bj1);
         __syncthreads();
         closures(p, s, j, scr + p.roff[j + 1]);
         const double num = sample_coupling(p, s, w, c, p.cp_q[c], ov, wt);
         apply_site_op(s.Cen, p.pb, s.sbC, bl, br, s.O1);
         apply_site_op(s.Nxt, p.pb, s.sbC, bj, bj1, s.O2);
         __syncthreads();
-        store_site(W + p.woff[j], s.Nxt, p.pb, s.sbC, bj, bj1);
+        store_site(W + s.woff[j], s.Nxt, p.pb, s.sbC, bj, bj1);
         if (rv < j + 1) rv = j + 1;
         ov = num;
         if (p.trace != nullptr) {
@@ -397,14 +398,14 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p)
         __syncthreads();
         cta_householder_qr(bl * d, br, s.QRb, p.pq, s.Rf, p.pb, s.tau, s.wv, s.red);
         {
-          double *Wi = W + p.woff[i];
+          double *Wi = W + s.woff[i];
           for (int q = tid; q < bl * br * d; q += kThreads) {
             const int r = q % bl, rest = q / bl, cc = rest % br, sg = rest / br;
             Wi[q] = s.QRb[(r + bl * sg) + p.pq * cc];
           }
         }
-        const int b2 = p.bW[i + 2];
-        load_site(s.Nxt, p.pb, s.sbC, W + p.woff[i + 1], br, b2);
+        const int b2 = s.bW[i + 2];
+        load_site(s.Nxt, p.pb, s.sbC, W + s.woff[i + 1], br, b2);
         __syncthreads();
         for (int sg = 0; sg < d; ++sg)
           cta_gemm(br, b2, br, 1.0, s.Rf, p.pb, false, s.Nxt + sg * s.sbC, p.pb, false, 0.0, s.Cen + sg * s.sbC,
@@ -426,7 +427,7 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p)
         const double scale = (ovr < 0.0) ? -1.0 / nrm : 1.0 / nrm;
         for (int q = tid; q < bl * d; q += kThreads) s.Cen[(q / bl) * s.sbC + (q % bl)] *= scale;
         __syncthreads();
-        store_site(W + p.woff[i], s.Cen, p.pb, s.sbC, bl, 1);
+        store_site(W + s.woff[i], s.Cen, p.pb, s.sbC, bl, 1);
         if (tid == 0) {
           const double ovf = fabs(ovr) / nrm;
           const double ew = en / ovr;
@@ -454,15 +455,16 @@ __global__ void __launch_bounds__(kThreads, 1) energy_general_kernel(Dev p) {
   const long fm = (long)p.maxA * p.maxB;
   double *Fdone[2] = {scr + p.choff, scr + p.choff + fm};
   double *Fch = scr + p.choff + 2 * fm;
-  for (int w = blockIdx.x; w < N; w += gridDim.x) {
+  for (int w = next_walker(s, p.ctr + kCtrEnergy); w < N; w = next_walker(s, p.ctr + kCtrEnergy)) {
     const int slot = p.slot_of[w];
+    load_walker_dims(p, s, slot);
     const double *W = p.walkers + (long)slot * p.wstride;
     if (tid == 0) s.Lenv[0] = 1.0;
     __syncthreads();
     int cur = 0;
     for (int k = 0; k < L; ++k) {
-      const int al = p.aT[k], ar = p.aT[k + 1], bl = p.bW[k], br = p.bW[k + 1];
-      env_update_general(p, s, k, p.trial + p.toff[k], al, ar, bl, br, W + p.woff[k], bl, bl * br, Fdone[cur],
+      const int al = p.aT[k], ar = p.aT[k + 1], bl = s.bW[k], br = s.bW[k + 1];
+      env_update_general(p, s, k, p.trial + p.toff[k], al, ar, bl, br, W + s.woff[k], bl, bl * br, Fdone[cur],
                          Fdone[1 - cur], Fch);
       cur = 1 - cur;
     }

@@ -35,9 +35,12 @@ struct Dev {
   int maxA, maxB;   // largest trial / walker bond dimension
   int pa, pb, pq;   // padded shared-memory leading dimensions
   const int *aT;    // trial bond dims [L+1]
-  const int *bW;    // walker bond dims [L+1]
+  const int *bW;    // largest walker bond dims [L+1] (the slot layout)
   const long *toff; // trial site offsets [L]
-  const long *woff; // walker site offsets [L]
+  const long *woff; // walker site offsets of the slot layout [L]
+  const int *wdims; // per slot: the walker's own bond dims [capacity][L+1] (<= bW)
+  const long *wofs; // per slot: the walker's site offsets [capacity][L]
+  int *ctr;         // work counters of the persistent kernels (zeroed before each launch)
   const double *trial;
   long wstride;     // doubles per walker slot
   double *walkers;
@@ -85,6 +88,9 @@ __host__ __device__ inline int padld(int x) {
 
 struct Smem {
   double *Lenv, *Cen, *Nxt, *Xb, *Pb, *Qt, *QRb, *Rf, *red, *tau, *wv, *M, *Cm, *O1, *O2, *pdf, *sc;
+  int *bW;      // bond dims of the walker being processed [L+1]
+  long *woff;   // its site offsets [L]
+  int *wsel;    // the walker index handed out by the work counter
   int sbC, sbX;  // sigma-block strides of Cen/Nxt and of Xb/Pb
 };
 
@@ -93,7 +99,7 @@ struct Smem {
 // for large bond dimensions they live in the CTA's global scratch instead (big != nullptr), where
 // the GEMMs read them through L1/L2.  Returns the doubles placed in shared memory; *big_doubles
 // (if given) receives the size of the matrix buffers.
-__host__ __device__ inline long smem_doubles(int maxA, int maxB, int G, int pa, int pb, int pq,
+__host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, int pa, int pb, int pq,
                                               Smem *s, double *base, double *big = nullptr,
                                               long *big_doubles = nullptr) {
   long off = 0, boff = 0;
@@ -122,6 +128,17 @@ __host__ __device__ inline long smem_doubles(int maxA, int maxB, int G, int pa, 
   take(s ? s->O2 : dummy, 4);
   take(s ? s->pdf : dummy, G);
   take(s ? s->sc : dummy, 16);
+  {
+    double *b, *o, *q;
+    take(b, (L + 2) / 2);
+    take(o, L);
+    take(q, 1);
+    if (s) {
+      s->bW = reinterpret_cast<int *>(b);
+      s->woff = reinterpret_cast<long *>(o);
+      s->wsel = reinterpret_cast<int *>(q);
+    }
+  }
   take_big(s ? s->Lenv : dummy, (long)pa * maxB);
   take_big(s ? s->Cen : dummy, (long)pb * maxB * d);
   take_big(s ? s->Nxt : dummy, (long)pb * maxB * d);
@@ -142,8 +159,27 @@ __host__ __device__ inline long smem_doubles(int maxA, int maxB, int G, int pa, 
 // matrix buffers do not fit on chip).
 __device__ __forceinline__ void carve(const Dev &p, Smem &s, double *smem_raw) {
   double *big = (p.gwoff >= 0) ? p.scratch + (long)blockIdx.x * p.scr_stride + p.gwoff : nullptr;
-  smem_doubles(p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw, big);
+  smem_doubles(p.L, p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw, big);
 }
+
+// Bond dims and site offsets of the walker in `slot` into shared memory.  Ends with a barrier.
+__device__ __forceinline__ void load_walker_dims(const Dev &p, Smem &s, int slot) {
+  for (int k = threadIdx.x; k <= p.L; k += kThreads) s.bW[k] = p.wdims[(long)slot * (p.L + 1) + k];
+  for (int k = threadIdx.x; k < p.L; k += kThreads) s.woff[k] = p.wofs[(long)slot * p.L + k];
+  __syncthreads();
+}
+
+// Dynamic scheduling of the persistent grid: the next logical walker from the kernel's work
+// counter (walkers of uneven bond dimension cost unevenly).  Starts with a barrier, so the
+// previous walker's shared data is no longer in use.
+__device__ __forceinline__ int next_walker(Smem &s, int *ctr) {
+  __syncthreads();
+  if (threadIdx.x == 0) *s.wsel = atomicAdd(ctr, 1);
+  __syncthreads();
+  return *s.wsel;
+}
+
+enum : int { kCtrStep = 0, kCtrSetOverlap = 1, kCtrEnergy = 2, kCtrCompress = 3, kNumCtr = 8 };
 
 // dst[sigma*sb + r + ld*c] = src[r + dl*(c + dr*sigma)]   (site storage -> padded smem)
 __device__ __forceinline__ void load_site(double *dst, int ld, int sb, const double *src, int dl,
@@ -248,8 +284,9 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
   double *scr = p.scratch + (long)blockIdx.x * p.scr_stride;
   double *Fbuf = scr + p.foff;
   const int fst = 4 * p.maxA * p.maxB;
-  for (int w = blockIdx.x; w < N; w += gridDim.x) {
+  for (int w = next_walker(s, p.ctr + kCtrStep); w < N; w = next_walker(s, p.ctr + kCtrStep)) {
     const int slot = p.slot_of[w];
+    load_walker_dims(p, s, slot);
     double *W = p.walkers + (long)slot * p.wstride;
     // ---------------- phase A: right environments ------------------------------------------
     // The walker is read as stored (between steps: left-canonical).  For k = L-1 .. 1:
@@ -264,8 +301,8 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
         scr[p.nroff[L]] = 1.0;
       }
       for (int k = L - 1; k >= 1; --k) {
-        const int al = p.aT[k], ar = p.aT[k + 1], bl = p.bW[k], br = p.bW[k + 1];
-        load_site(s.Nxt, p.pb, s.sbC, W + p.woff[k], bl, br);
+        const int al = p.aT[k], ar = p.aT[k + 1], bl = s.bW[k], br = s.bW[k + 1];
+        load_site(s.Nxt, p.pb, s.sbC, W + s.woff[k], bl, br);
         __syncthreads();
         const double *Rn = scr + p.roff[k + 1], *Nn = scr + p.nroff[k + 1];
         double *Rk = scr + p.roff[k], *Nk = scr + p.nroff[k];
@@ -288,8 +325,8 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
       }
       // centre = site 0 (1 x b1): ||phi||^2 = sum_s C[s] N[1] C[s]^T, ov = sum_s B_0[s] R[1] C[s]^T
       {
-        const int a1 = p.aT[1], b1 = p.bW[1];
-        load_site(s.Cen, p.pb, s.sbC, W + p.woff[0], 1, b1);
+        const int a1 = p.aT[1], b1 = s.bW[1];
+        load_site(s.Cen, p.pb, s.sbC, W + s.woff[0], 1, b1);
         __syncthreads();
         const double *R1 = scr + p.roff[1], *N1 = scr + p.nroff[1];
         const double *B0 = p.trial + p.toff[0];
@@ -320,10 +357,10 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
     __syncthreads();
     for (int i = 0; i < L - 1; ++i) {
       const int al = p.aT[i], ar = p.aT[i + 1], a2 = p.aT[i + 2];
-      const int bl = p.bW[i], br = p.bW[i + 1], b2 = p.bW[i + 2];
+      const int bl = s.bW[i], br = s.bW[i + 1], b2 = s.bW[i + 2];
       const double *Bi = p.trial + p.toff[i];
       const double *Bj = p.trial + p.toff[i + 1];
-      load_site(s.Nxt, p.pb, s.sbC, W + p.woff[i + 1], br, b2);
+      load_site(s.Nxt, p.pb, s.sbC, W + s.woff[i + 1], br, b2);
       __syncthreads();
       const int c = p.bond_c[i];
       double num = ov;  // overlap numerator after the bond (no coupling: unchanged)
@@ -451,7 +488,7 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
                  s.Cen + sg * s.sbC, p.pb);
       // site i <- Q
       {
-        double *Wi = W + p.woff[i];
+        double *Wi = W + s.woff[i];
         for (int q = tid; q < bl * br * d; q += kThreads) {
           const int r = q % bl, rest = q / bl, cc = rest % br, sg = rest / br;
           Wi[q] = s.QRb[(r + bl * sg) + p.pq * cc];
@@ -496,10 +533,10 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
     // last site: centre; overlap and energy (final setOverlap, MPSQMC2.cpp:598; Walker.cpp:76)
     {
       const int i = L - 1;
-      const int al = p.aT[i], bl = p.bW[i];
+      const int al = p.aT[i], bl = s.bW[i];
       env_update(p, s, p.trial + p.toff[i], al, 1, bl, 1, s.Cen, p.pb, s.sbC, Fbuf + cur * fst,
                  Fbuf + (1 - cur) * fst, p.bondJ[i - 1], false);
-      store_site(W + p.woff[i], s.Cen, p.pb, s.sbC, bl, 1);
+      store_site(W + s.woff[i], s.Cen, p.pb, s.sbC, bl, 1);
       const double ovf = s.Lenv[0];
       const double en = Fbuf[(1 - cur) * fst + 0];
       if (tid == 0) {
@@ -525,27 +562,28 @@ __global__ void __launch_bounds__(kThreads, 1) set_overlap_kernel(Dev p) {
   carve(p, s, smem_raw);
   const int L = p.L, d = kMaxD, tid = threadIdx.x;
   const int N = *p.n_cur;
-  for (int w = blockIdx.x; w < N; w += gridDim.x) {
+  for (int w = next_walker(s, p.ctr + kCtrSetOverlap); w < N; w = next_walker(s, p.ctr + kCtrSetOverlap)) {
     const int slot = p.slot_of[w];
+    load_walker_dims(p, s, slot);
     double *W = p.walkers + (long)slot * p.wstride;
-    load_site(s.Cen, p.pb, s.sbC, W + p.woff[0], p.bW[0], p.bW[1]);
+    load_site(s.Cen, p.pb, s.sbC, W + s.woff[0], s.bW[0], s.bW[1]);
     __syncthreads();
     for (int k = 0; k < L; ++k) {
-      const int bl = p.bW[k], br = p.bW[k + 1];
+      const int bl = s.bW[k], br = s.bW[k + 1];
       for (int q = tid; q < bl * br; q += kThreads) {
         const int r = q % bl, cc = q / bl;
         for (int sg = 0; sg < d; ++sg) s.QRb[(r + bl * sg) + p.pq * cc] = s.Cen[sg * s.sbC + r + p.pb * cc];
       }
       __syncthreads();
       cta_householder_qr(bl * d, br, s.QRb, p.pq, s.Rf, p.pb, s.tau, s.wv, s.red);
-      double *Wk = W + p.woff[k];
+      double *Wk = W + s.woff[k];
       for (int q = tid; q < bl * br * d; q += kThreads) {
         const int r = q % bl, rest = q / bl, cc = rest % br, sg = rest / br;
         Wk[q] = s.QRb[(r + bl * sg) + p.pq * cc];
       }
       if (k < L - 1) {
-        const int b2 = p.bW[k + 2];
-        load_site(s.Nxt, p.pb, s.sbC, W + p.woff[k + 1], br, b2);
+        const int b2 = s.bW[k + 2];
+        load_site(s.Nxt, p.pb, s.sbC, W + s.woff[k + 1], br, b2);
         __syncthreads();
         for (int sg = 0; sg < d; ++sg)
           cta_gemm(br, b2, br, 1.0, s.Rf, p.pb, false, s.Nxt + sg * s.sbC, p.pb, false, 0.0,
@@ -557,8 +595,8 @@ __global__ void __launch_bounds__(kThreads, 1) set_overlap_kernel(Dev p) {
     if (tid == 0) s.Lenv[0] = 1.0;
     __syncthreads();
     for (int k = 0; k < L; ++k) {
-      const int al = p.aT[k], ar = p.aT[k + 1], bl = p.bW[k], br = p.bW[k + 1];
-      const double *A = W + p.woff[k];
+      const int al = p.aT[k], ar = p.aT[k + 1], bl = s.bW[k], br = s.bW[k + 1];
+      const double *A = W + s.woff[k];
       const double *B = p.trial + p.toff[k];
       for (int sg = 0; sg < d; ++sg)
         cta_gemm(al, br, bl, 1.0, s.Lenv, p.pa, false, A + (long)sg * bl * br, bl, false, 0.0,
@@ -575,8 +613,8 @@ __global__ void __launch_bounds__(kThreads, 1) set_overlap_kernel(Dev p) {
     double ov = s.Lenv[0];
     __syncthreads();
     if (ov < 0.0) {
-      const int n0 = p.bW[0] * p.bW[1] * d;
-      for (int q = tid; q < n0; q += kThreads) W[p.woff[0] + q] *= -1.0;
+      const int n0 = s.bW[0] * s.bW[1] * d;
+      for (int q = tid; q < n0; q += kThreads) W[s.woff[0] + q] *= -1.0;
       ov = -ov;
     }
     if (tid == 0) p.overlap[slot] = ov;
@@ -594,15 +632,16 @@ __global__ void __launch_bounds__(kThreads, 1) energy_kernel(Dev p) {
   double *scr = p.scratch + (long)blockIdx.x * p.scr_stride;
   double *Fbuf = scr + p.foff;
   const int fst = 4 * p.maxA * p.maxB;
-  for (int w = blockIdx.x; w < N; w += gridDim.x) {
+  for (int w = next_walker(s, p.ctr + kCtrEnergy); w < N; w = next_walker(s, p.ctr + kCtrEnergy)) {
     const int slot = p.slot_of[w];
+    load_walker_dims(p, s, slot);
     const double *W = p.walkers + (long)slot * p.wstride;
     if (tid == 0) s.Lenv[0] = 1.0;
     __syncthreads();
     int cur = 0;
     for (int k = 0; k < L; ++k) {
-      const int al = p.aT[k], ar = p.aT[k + 1], bl = p.bW[k], br = p.bW[k + 1];
-      env_update(p, s, p.trial + p.toff[k], al, ar, bl, br, W + p.woff[k], bl, bl * br,
+      const int al = p.aT[k], ar = p.aT[k + 1], bl = s.bW[k], br = s.bW[k + 1];
+      env_update(p, s, p.trial + p.toff[k], al, ar, bl, br, W + s.woff[k], bl, bl * br,
                  Fbuf + cur * fst, Fbuf + (1 - cur) * fst, (k > 0) ? p.bondJ[k - 1] : 0.0, k == 0);
       cur = 1 - cur;
     }
@@ -621,10 +660,13 @@ __global__ void __launch_bounds__(kThreads, 1) energy_kernel(Dev p) {
 __global__ void onesite_kernel(Dev p) {
   const int N = *p.n_cur;
   for (int w = blockIdx.x; w < N; w += gridDim.x) {
-    double *W = p.walkers + (long)p.slot_of[w] * p.wstride;
+    const int slot = p.slot_of[w];
+    double *W = p.walkers + (long)slot * p.wstride;
+    const int *bW = p.wdims + (long)slot * (p.L + 1);
+    const long *woff = p.wofs + (long)slot * p.L;
     for (int k = 0; k < p.L; ++k) {
-      const int blk = p.bW[k] * p.bW[k + 1];
-      double *site = W + p.woff[k];
+      const int blk = bW[k] * bW[k + 1];
+      double *site = W + woff[k];
       for (int q = threadIdx.x; q < blk * kMaxD; q += blockDim.x) site[q] *= p.onesite[q / blk];
     }
   }
@@ -916,11 +958,24 @@ __global__ void copy_walkers_kernel(Dev p, const StepDev *sd, const int *copy_sr
     const double *a = p.walkers + (long)src * per;
     double *b = p.walkers + (long)dst * per;
     for (long e = threadIdx.x; e < per; e += blockDim.x) b[e] = a[e];
+    for (int k = threadIdx.x; k <= p.L; k += blockDim.x)
+      const_cast<int *>(p.wdims)[(long)dst * (p.L + 1) + k] = p.wdims[(long)src * (p.L + 1) + k];
+    for (int k = threadIdx.x; k < p.L; k += blockDim.x)
+      const_cast<long *>(p.wofs)[(long)dst * p.L + k] = p.wofs[(long)src * p.L + k];
     if (threadIdx.x == 0) {
       p.weight[dst] = p.weight[src];
       p.overlap[dst] = p.overlap[src];
       p.ehist[dst] = p.ehist[src];
     }
+  }
+}
+
+// Walkers [w0, w0 + m) in logical order into dst (stride per doubles each).
+__global__ void gather_walkers_kernel(Dev p, int w0, int m, long per, double *dst) {
+  for (int q = blockIdx.x; q < m; q += gridDim.x) {
+    const double *a = p.walkers + (long)p.slot_of[w0 + q] * p.wstride;
+    double *b = dst + (long)q * per;
+    for (long e = threadIdx.x; e < per; e += blockDim.x) b[e] = a[e];
   }
 }
 

@@ -809,11 +809,25 @@ int orc_walk(const orc_walk_config *cfg, const int *dimsT, const double *trial, 
              double *E0, double *st_sumw, double *st_EP, double *st_ET, double *st_omega, int *st_n,
              double *pw_weight, double *pw_overlap, double *pw_energy, int *pw_parent,
              double *trace, unsigned long long *draws_used) {
+  return orc_walk_dims(cfg, dimsT, trial, ci, cj, cJ, Jvals, Utab, Stab, VTtab, grid, dimsW, nullptr, walkers,
+                       weights, overlaps, ehist, n_walkers, E0, st_sumw, st_EP, st_ET, st_omega, st_n, pw_weight,
+                       pw_overlap, pw_energy, pw_parent, trace, draws_used);
+}
+
+int orc_walk_dims(const orc_walk_config *cfg, const int *dimsT, const double *trial, const int *ci,
+                  const int *cj, const double *cJ, const double *Jvals, const double *Utab,
+                  const double *Stab, const double *VTtab, const double *grid, const int *dimsW,
+                  int *wdims, double *walkers, double *weights, double *overlaps, double *ehist,
+                  int *n_walkers, double *E0, double *st_sumw, double *st_EP, double *st_ET,
+                  double *st_omega, int *st_n, double *pw_weight, double *pw_overlap, double *pw_energy,
+                  int *pw_parent, double *trace, unsigned long long *draws_used) {
   const int L = cfg->L, d = cfg->d, nC = cfg->nC, G = cfg->G, cap = cfg->capacity;
   const int n2 = d * d;
   if (L < 2 || nC < 1 || G < 1 || *n_walkers < 1 || *n_walkers > cap) return -2;
   const long szW = mps_size(L, d, dimsW);
   const long szT = mps_size(L, d, dimsT);
+  // walker w's own bond dims (MPSstate keeps its VirtualD, MPSstate.cpp:13-40)
+  auto dims_of = [&](int w) -> const int * { return wdims ? wdims + (size_t)w * (L + 1) : dimsW; };
   (void)szT;
   std::vector<int> jidx(nC, -1);
   for (int c = 0; c < nC; ++c)
@@ -857,7 +871,7 @@ int orc_walk(const orc_walk_config *cfg, const int *dimsT, const double *trial, 
   int N = *n_walkers;
   std::vector<double> energy(cap);
   auto energy_of = [&](int w) {
-    const MpsView Wv = make_view(L, d, dimsW, walkers + (size_t)w * szW);
+    const MpsView Wv = make_view(L, d, dims_of(w), walkers + (size_t)w * szW);
     return energy_numerator(mpo, T, Wv) / overlaps[w];
   };
   // Initial EnergyFunctionAndHistory(1, &E, false), MPSQMC2.cpp:447.
@@ -882,19 +896,20 @@ int orc_walk(const orc_walk_config *cfg, const int *dimsT, const double *trial, 
     for (int w = 0; w < N; ++w) {
       std::vector<double> w1, w2, w3, mem, Rm, qwork, work, pdf(G), C((size_t)n2 * n2);
       double *phi = walkers + (size_t)w * szW;
-      MpsView P = make_view(L, d, dimsW, phi);
+      const int *dW = dims_of(w);
+      MpsView P = make_view(L, d, dW, phi);
       auto set_overlap = [&]() {  // Walker::setOverlap, Walker.cpp:54-66
-        left_normalize(L, d, dimsW, phi, mem, Rm, qwork);
+        left_normalize(L, d, dW, phi, mem, Rm, qwork);
         double val = inner_product(T, P, w1, w2, w3);
         if (val < 0.0) {
-          const long n0 = (long)dimsW[0] * dimsW[1] * d;
+          const long n0 = (long)dW[0] * dW[1] * d;
           for (long q = 0; q < n0; ++q) phi[q] *= -1.0;
           val *= -1;
         }
         overlaps[w] = val;
       };
       if (field)
-        for (int s = 0; s < L; ++s) apply_site_op(d, dimsW[s], dimsW[s + 1], P.site[s], onesite.data(), work);
+        for (int s = 0; s < L; ++s) apply_site_op(d, dW[s], dW[s + 1], P.site[s], onesite.data(), work);
       set_overlap();
       MpsView term = T;
       for (int c = 0; c < nC; ++c) {
@@ -928,9 +943,9 @@ int orc_walk(const orc_walk_config *cfg, const int *dimsT, const double *trial, 
           cum += pdf[count];
         }
         const int q = jidx[c];
-        apply_grid_site(d, dimsW[i], dimsW[i + 1], P.site[i], Stab + (size_t)n2 * q,
+        apply_grid_site(d, dW[i], dW[i + 1], P.site[i], Stab + (size_t)n2 * q,
                         Utab + (size_t)n2 * n2 * q, false, grid + (size_t)n2 * count, work);
-        apply_grid_site(d, dimsW[j], dimsW[j + 1], P.site[j], Stab + (size_t)n2 * q,
+        apply_grid_site(d, dW[j], dW[j + 1], P.site[j], Stab + (size_t)n2 * q,
                         VTtab + (size_t)n2 * n2 * q, true, grid + (size_t)n2 * count, work);
         set_overlap();
         if (tr_step) {
@@ -944,7 +959,7 @@ int orc_walk(const orc_walk_config *cfg, const int *dimsT, const double *trial, 
         }
       }
       if (field)
-        for (int s = 0; s < L; ++s) apply_site_op(d, dimsW[s], dimsW[s + 1], P.site[s], onesite.data(), work);
+        for (int s = 0; s < L; ++s) apply_site_op(d, dW[s], dW[s + 1], P.site[s], onesite.data(), work);
       set_overlap();
     }
     double sumw = 0.0;
@@ -1014,6 +1029,12 @@ int orc_walk(const orc_walk_config *cfg, const int *dimsT, const double *trial, 
       Nn += nCopies;
     }
     std::memcpy(walkers, newbuf.data(), sizeof(double) * (size_t)Nn * szW);
+    if (wdims) {  // copies keep their parent's bond dims
+      std::vector<int> nd((size_t)Nn * (L + 1));
+      for (int w = 0; w < Nn; ++w)
+        std::memcpy(nd.data() + (size_t)w * (L + 1), wdims + (size_t)par[w] * (L + 1), sizeof(int) * (L + 1));
+      std::memcpy(wdims, nd.data(), sizeof(int) * nd.size());
+    }
     for (int w = 0; w < Nn; ++w) {
       weights[w] = nw[w];
       overlaps[w] = no[w];

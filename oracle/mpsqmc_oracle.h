@@ -81,6 +81,17 @@ typedef struct {
   int popctl_interval, comb;
 } orc_walk_config;
 
+/* As orc_walk, with walker w's own bond dims in wdims[w*(L+1) ..] (each <= dimsW elementwise;
+ * walker slots keep the stride of dimsW, tensors packed from the slot start).  wdims is updated
+ * by the branching (copies keep their parent's dims).  wdims == NULL: every walker has dimsW. */
+int orc_walk_dims(const orc_walk_config *cfg, const int *dimsT, const double *trial, const int *ci,
+                  const int *cj, const double *cJ, const double *Jvals, const double *Utab,
+                  const double *Stab, const double *VTtab, const double *grid, const int *dimsW,
+                  int *wdims, double *walkers, double *weights, double *overlaps, double *ehist,
+                  int *n_walkers, double *E0, double *st_sumw, double *st_EP, double *st_ET,
+                  double *st_omega, int *st_n, double *pw_weight, double *pw_overlap, double *pw_energy,
+                  int *pw_parent, double *trace, unsigned long long *draws_used);
+
 int orc_walk(const orc_walk_config *cfg, const int *dimsT, const double *trial, const int *ci,
              const int *cj, const double *cJ, const double *Jvals, const double *Utab,
              const double *Stab, const double *VTtab, const double *grid, const int *dimsW,

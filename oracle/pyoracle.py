@@ -83,6 +83,11 @@ def _declare(l):
                            _dp, _dp, _dp, _dp, C.POINTER(C.c_int), C.POINTER(C.c_double),
                            _dp, _dp, _dp, _dp, _ip, null_dp, null_dp, null_dp, null_dp, null_dp,
                            C.POINTER(C.c_ulonglong)]
+    l.orc_walk_dims.restype = C.c_int
+    l.orc_walk_dims.argtypes = [C.POINTER(WalkConfig), _ip, _dp, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip,
+                                null_dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                _dp, _dp, _dp, _dp, _ip, null_dp, null_dp, null_dp, null_dp, null_dp,
+                                C.POINTER(C.c_ulonglong)]
 
 
 # --------------------------------------------------------------------------------------------
@@ -256,16 +261,22 @@ class WalkResult:
     overlaps: np.ndarray
     ehist: np.ndarray
     draws: int
+    wdims: np.ndarray | None = None
 
 
 def walk(trial: MPS, walkers: np.ndarray, dimsW, weights, overlaps, ehist, *, ci, cj, cJ, Jvals,
          U, S, VT, grid, dtau, nsteps, Ndesired, capacity, seed, skip=0, h=0.0, trace=False,
-         nthreads=0, popctl_interval=1, comb=False) -> WalkResult:
-    """MPSQMC2::Walk on the CPU (restatement).  walkers: [N, size] float64."""
+         nthreads=0, popctl_interval=1, comb=False, wdims=None) -> WalkResult:
+    """MPSQMC2::Walk on the CPU (restatement).  walkers: [N, size(dimsW)] float64; with wdims
+    ([N, L+1]) walker w has its own bond dims and its tensors at the start of its row."""
     N = walkers.shape[0]
     size = mps_size(dimsW, trial.d)
     buf = np.zeros((capacity, size))
     buf[:N] = walkers
+    wd = None
+    if wdims is not None:
+        wd = np.zeros((capacity, trial.L + 1), dtype=np.int32)
+        wd[:N] = wdims
     w = np.zeros(capacity); w[:N] = weights
     o = np.zeros(capacity); o[:N] = overlaps
     eh = np.zeros(capacity); eh[:N] = ehist
@@ -283,13 +294,14 @@ def walk(trial: MPS, walkers: np.ndarray, dimsW, weights, overlaps, ehist, *, ci
                      capacity=capacity, nsteps=nsteps, nthreads=nthreads, dtau=dtau, h=h, seed=seed,
                      skip=skip, popctl_interval=popctl_interval, comb=int(comb))
     ptr = lambda a: a.ctypes.data_as(C.c_void_p) if a is not None else None
-    status = lib().orc_walk(C.byref(cfg), _i32(trial.dims), _f64(trial.data), _i32(ci), _i32(cj),
-                            _f64(cJ), _f64(Jvals), _f64(U), _f64(S), _f64(VT), _f64(grid), _i32(dimsW),
-                            buf, w, o, eh, C.byref(n), C.byref(E0), st[0], st[1], st[2], st[3], stn,
-                            ptr(pw[0]), ptr(pw[1]), ptr(pw[2]), ptr(par), ptr(tr), C.byref(draws))
+    status = lib().orc_walk_dims(C.byref(cfg), _i32(trial.dims), _f64(trial.data), _i32(ci), _i32(cj),
+                                 _f64(cJ), _f64(Jvals), _f64(U), _f64(S), _f64(VT), _f64(grid), _i32(dimsW),
+                                 ptr(wd), buf, w, o, eh, C.byref(n), C.byref(E0), st[0], st[1], st[2], st[3], stn,
+                                 ptr(pw[0]), ptr(pw[1]), ptr(pw[2]), ptr(par), ptr(tr), C.byref(draws))
     Nf = n.value
     return WalkResult(status, E0.value, st[0], st[1], st[2], st[3], stn, pw[0], pw[1], pw[2], par, tr,
-                      buf[:Nf].copy(), w[:Nf].copy(), o[:Nf].copy(), eh[:Nf].copy(), draws.value)
+                      buf[:Nf].copy(), w[:Nf].copy(), o[:Nf].copy(), eh[:Nf].copy(), draws.value,
+                      None if wd is None else wd[:Nf].copy())
 
 
 # --------------------------------------------------------------------------------------------
