@@ -117,6 +117,15 @@ int mpsqmc_set_walkers_dims(mpsqmc_ctx *ctx, int N, const int *dims, const doubl
 /* Bond dims of the current population in logical order: dims [N][L+1] (may be NULL). */
 int mpsqmc_get_walker_dims(mpsqmc_ctx *ctx, int *N, int *dims);
 
+/* MPSstate::CompressState(target_D[w]) (MPSstate.cpp:379-404; two-site SVD sweeps right then left,
+ * truncation at target_D and at Schmidt values < 1e-13, TwoSiteObject.cpp:71-184) on the device for
+ * every current walker w (logical order; target_D[w] <= 0 leaves walker w unchanged).  With
+ * normalize != 0 each walker then gets Walker::setOverlap, as SetupWalkers does after compressing
+ * (MPSQMC2.cpp:404-409).  The walkers' bond dims shrink accordingly (mpsqmc_get_walker_dims).
+ * Singular-vector signs are this implementation's: the states equal the reference's, the
+ * tensors may differ by signs on the bonds. */
+int mpsqmc_compress_walkers(mpsqmc_ctx *ctx, const int *target_D, int normalize);
+
 /* Random stream: mt19937(seed) advanced by `skip` 32-bit outputs; every uniform is one output
  * divided by 2^32 (Random.cpp:28-59 with Boost's uniform_real_distribution). */
 int mpsqmc_set_rng(mpsqmc_ctx *ctx, uint32_t seed, uint64_t skip);

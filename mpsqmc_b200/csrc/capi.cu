@@ -19,6 +19,7 @@
 #include "../../include/mpsqmc_gpu.h"
 #include "walker_kernels.cuh"
 #include "walker_general.cuh"
+#include "compress.cuh"
 
 namespace {
 
@@ -114,6 +115,9 @@ struct mpsqmc_ctx {
   int *d_ctr = nullptr;                 // work counters of the persistent kernels
   double *d_stage = nullptr;            // mpsqmc_get_walkers: walkers gathered into logical order
   int stage_walkers = 0;
+  double *d_cscr = nullptr;             // mpsqmc_compress_walkers: per-CTA scratch
+  long cstride = 0;
+  int *d_targets = nullptr;
   long choff = 0;
   int *d_cp_j = nullptr, *d_cp_q = nullptr, *d_site_c0 = nullptr, *d_ech_off = nullptr, *d_ech_slot = nullptr,
       *d_ech_cont = nullptr, *d_eopen = nullptr;
@@ -230,7 +234,7 @@ void free_all(mpsqmc_ctx *c) {
                   c->d_bondJ, c->d_tabU, c->d_tabS, c->d_tabVT, c->d_grid, c->d_scratch, c->d_trace,
                   c->d_err, c->d_mt, c->d_sd, c->d_cp_j, c->d_cp_q, c->d_site_c0, c->d_ech_off,
                   c->d_ech_slot, c->d_ech_cont, c->d_eopen, c->d_ech_J, c->d_ncop, c->d_wdims, c->d_wofs,
-                  c->d_ctr, c->d_stage};
+                  c->d_ctr, c->d_stage, c->d_cscr, c->d_targets};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
@@ -626,6 +630,34 @@ int mpsqmc_set_walkers_dims(mpsqmc_ctx *c, int N, const int *dims, const double 
                             const double *overlaps, const double *ehist, int normalize) {
   if (!dims) return fail(MPSQMC_E_ARG, "null dims");
   return set_walkers_impl(c, N, dims, walkers, weights, overlaps, ehist, normalize);
+}
+
+int mpsqmc_compress_walkers(mpsqmc_ctx *c, const int *target_D, int normalize) {
+  if (!c || !target_D) return fail(MPSQMC_E_ARG, "null argument");
+  const int n = c->n_cur;
+  if (n < 1) return fail(MPSQMC_E_ARG, "no walkers");
+  CK(cudaSetDevice(c->device));
+  if (!c->d_cscr) {
+    const long q2 = 2L * c->maxB;
+    const long wmax = c->woff[c->L - 1] + (long)c->bW[c->L - 1] * c->bW[c->L] * c->d;
+    c->cstride = ((wmax + 31) & ~31L) + 3 * q2 * q2;
+    c->cstride = (c->cstride + 31) & ~31L;
+    if (dalloc(&c->d_cscr, (size_t)c->max_ctas * c->cstride) || dalloc(&c->d_targets, c->capacity))
+      return MPSQMC_E_CUDA;
+  }
+  CK(cudaMemcpyAsync(c->d_targets, target_D, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(int) * mq::kNumCtr, c->stream));
+  mq::Dev p = make_dev(c);
+  mq::compress_kernel<<<grid_for(c, n), mq::kThreads, mq::compress_smem_bytes(c->L, c->maxB), c->stream>>>(
+      p, c->d_targets, c->d_cscr, c->cstride);
+  CK(cudaGetLastError());
+  if (normalize) {
+    CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(int) * mq::kNumCtr, c->stream));
+    mq::set_overlap_kernel<<<grid_for(c, n), mq::kThreads, c->smem_bytes, c->stream>>>(p);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return check_err(c);
 }
 
 int mpsqmc_get_walker_dims(mpsqmc_ctx *c, int *N, int *dims) {
