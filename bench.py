@@ -35,7 +35,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="chain64")
+    ap.add_argument("--workload", default="chain64", choices=["chain64", "snake6x6", "snake8x8"],
+                    help="chain64: the L=64 chain (default line); snake6x6 / snake8x8: the 2D lattices "
+                         "(walkers compressed on the device; no CPU baseline or e2e)")
     ap.add_argument("--walkers", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -144,20 +146,62 @@ def reference_cpu(wl, sample_walkers=None, steps=1, threads=None):
     return r
 
 
+def lattice_engine(wl, device):
+    """Engine for a 2D lattice workload.  Walkers start as copies of the trial compressed
+    (CompressState + setOverlap, as SetupWalkers does): on the device to uneven targets in one
+    population when D_T is among them, else one walker compressed on the host and replicated
+    (slots of the D_W layout)."""
+    from mpsqmc_b200 import Engine
+    from mpsqmc_b200 import problem as pb
+    ci, cj, cJ = wl.couplings()
+    trial = wl.trial()
+    U, S, VT = pb.trotter_tables(1.0, wl.dtau)
+    common = dict(L=wl.L, ci=ci, cj=cj, cJ=cJ, h=0.0, dtau=wl.dtau, trial_dims=trial.dims, trial=trial.data,
+                  Jvals=[1.0], U=U, S=S, VT=VT, grid=pb.grid_marsaglia(4, 4), Ndesired=wl.Nw, device=device)
+    N = wl.Nw
+    if max(wl.Ds) >= wl.DT:
+        eng = Engine(capacity=max(1000, 3 * N), walker_dims=trial.dims, **common)
+        eng.set_walkers(np.tile(trial.data, (N, 1)), np.ones(N), normalize=False)
+        eng.compress_walkers(wl.targets(), normalize=True)
+        dims = trial.dims
+    else:
+        # one walker compressed on the host (the engine's slots hold walkers up to D = 128)
+        w = pb.compress(trial, max(wl.Ds))
+        dims, w0 = w.dims, w.data
+        eng = Engine(capacity=max(1000, 3 * N), walker_dims=dims, **common)
+        eng.set_walkers(np.tile(w0, (N, 1)), np.ones(N), normalize=True)
+    inputs = dict(common, walker_dims=dims)
+    return eng, inputs
+
+
 def main():
     args = parse()
     rank, world, local, pg = dist_setup(args.gpus)
     from mpsqmc_b200 import workloads
 
-    wl = workloads.chain64(Nw=args.walkers or 2048)
-    cfg = {"workload": f"{wl.name}: L={wl.L} Heisenberg chain, D_T={wl.DT}, D_W={wl.DW}, {wl.Nw} walkers/GPU, "
-                       f"dtau={wl.dtau}, Marsaglia(4) grid, FP64",
-           "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.DW, "dtau": wl.dtau,
-           "l2": f"population ({wl.Nw * wl.walker.data.size * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
-           "parallelism": f"replicas x{world}", "sweep": args.sweep}
+    lattice = args.workload != "chain64"
+    if lattice:
+        wl = getattr(workloads, args.workload)(Nw=args.walkers) if args.walkers else getattr(workloads, args.workload)()
+        cfg = {"workload": f"{wl.name}: {wl.W}x{wl.H} open Heisenberg lattice on the snake path (L={wl.L}, "
+                           f"{len(wl.couplings()[0])} couplings), D_T={wl.DT}, D_W in {wl.Ds}, {wl.Nw} walkers/GPU, "
+                           f"dtau={wl.dtau}, Marsaglia(4) grid, FP64; seeded random left-normalised trial of the "
+                           f"D_T shape, walkers = trial compressed on the device",
+               "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.Ds, "dtau": wl.dtau,
+               "parallelism": f"replicas x{world}", "sweep": args.sweep}
+    else:
+        wl = workloads.chain64(Nw=args.walkers or 2048)
+        cfg = {"workload": f"{wl.name}: L={wl.L} Heisenberg chain, D_T={wl.DT}, D_W={wl.DW}, {wl.Nw} walkers/GPU, "
+                           f"dtau={wl.dtau}, Marsaglia(4) grid, FP64",
+               "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.DW, "dtau": wl.dtau,
+               "l2": f"population ({wl.Nw * wl.walker.data.size * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
+               "parallelism": f"replicas x{world}", "sweep": args.sweep}
 
     if args.impl == "reference":
         if rank != 0:
+            return
+        if lattice:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference classes need nC*16 trial copies "
+                              "and H*Psi_T per thread at this size; only chain64 has a CPU arm"}))
             return
         r = reference_cpu(wl, steps=1)
         if r is None:
@@ -183,14 +227,21 @@ def main():
     torch.cuda.set_device(local)
     from mpsqmc_b200 import Engine
 
-    inputs = wl.inputs()
-    walkers = wl.walkers()
-    eng = Engine(device=local, **inputs)
     from mpsqmc_b200.capi import OPT_SWEEP
     sweep = {"auto": 0, "nearest": 1, "general": 2}[args.sweep]
+    if lattice:
+        eng, inputs = lattice_engine(wl, local)
+        walkers = None
+        N = wl.Nw
+        args.no_e2e = True
+        args.no_cpu_baseline = True
+    else:
+        inputs = wl.inputs()
+        walkers = wl.walkers()
+        eng = Engine(device=local, **inputs)
+        N = walkers.shape[0]
+        eng.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
     eng.set_option(OPT_SWEEP, sweep)
-    N = walkers.shape[0]
-    eng.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
     eng.set_rng(wl.seed + 7919 * rank, 0)
     eng.walk(args.warmup)
     torch.cuda.synchronize()
@@ -216,9 +267,13 @@ def main():
         ws_all = float(ws_done)
     value = ws_all / (t_ms * 1e-3)
 
-    # roofline of the dominant kernel (walker_step_kernel): canonical FP64 work / kernel time
-    flops_ws = workloads.algorithmic_flops_per_walker_step(inputs["trial_dims"], inputs["walker_dims"],
-                                                           list(zip(inputs["ci"], inputs["cj"])))
+    # roofline of the dominant kernel (the walker-step kernel): canonical FP64 work / kernel time,
+    # averaged over the walkers' own bond dims
+    cpl = list(zip(inputs["ci"], inputs["cj"]))
+    dims_now = eng.get_walker_dims()
+    rows, counts = np.unique(dims_now, axis=0, return_counts=True)
+    flops_ws = float(sum(c * workloads.algorithmic_flops_per_walker_step(inputs["trial_dims"], r, cpl)
+                         for r, c in zip(rows, counts)) / counts.sum())
     achieved = flops_ws * ws_done / (k_ms * 1e-3) / 1e12
     peak = fp64_peak_tflops() if rank == 0 else None
 
@@ -255,7 +310,7 @@ def main():
     if rank == 0:
         prof_traffic = None
         tp = os.path.join(ROOT, "profiles", "walker_step_kernel_traffic.json")
-        if os.path.exists(tp):
+        if os.path.exists(tp) and not lattice and N == 2048:
             prof_traffic = json.load(open(tp)).get("bytes_per_launch")
         line = {
             "metric": METRIC, "value": value, "unit": "walker-steps/s", "n_gpus": world, "steps": args.steps,
@@ -264,7 +319,8 @@ def main():
             "energy": {"E_P_last": stats[-1]["E_P"], "E_T_last": stats[-1]["E_T"], "walkers_last": stats[-1]["n_after"]},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": prof_traffic,
-                         "kernel": "walker_step_kernel", "flops_per_walker_step": flops_ws,
+                         "kernel": "walker_step_general_kernel" if (lattice or args.sweep == "general")
+                         else "walker_step_kernel", "flops_per_walker_step": flops_ws,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor path)"},
             "cpu_baseline": cpu,
             "e2e": e2e,

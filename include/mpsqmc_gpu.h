@@ -119,7 +119,8 @@ int mpsqmc_get_walker_dims(mpsqmc_ctx *ctx, int *N, int *dims);
 
 /* MPSstate::CompressState(target_D[w]) (MPSstate.cpp:379-404; two-site SVD sweeps right then left,
  * truncation at target_D and at Schmidt values < 1e-13, TwoSiteObject.cpp:71-184) on the device for
- * every current walker w (logical order; target_D[w] <= 0 leaves walker w unchanged).  With
+ * every current walker w (logical order; target_D[w] <= 0, or >= the walker's largest bond
+ * dimension, leaves walker w unchanged, as SetupWalkers compresses only when DW < DT).  With
  * normalize != 0 each walker then gets Walker::setOverlap, as SetupWalkers does after compressing
  * (MPSQMC2.cpp:404-409).  The walkers' bond dims shrink accordingly (mpsqmc_get_walker_dims).
  * Singular-vector signs are this implementation's: the states equal the reference's, the

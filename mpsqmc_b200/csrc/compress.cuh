@@ -138,6 +138,11 @@ __global__ void __launch_bounds__(kThreads, 1) compress_kernel(Dev p, const int 
     long *go = const_cast<long *>(p.wofs) + (long)slot * L;
     for (int k = tid; k <= L; k += kThreads) dims[k] = gd[k];
     __syncthreads();
+    {  // SetupWalkers compresses only when the target is below the walker's bond dimension
+      int dmax = 1;
+      for (int k = 0; k <= L; ++k) dmax = max(dmax, dims[k]);
+      if (truncD >= dmax) continue;
+    }
     // unpack: site k of the walker (packed at go[k]) to the fixed offset p.woff[k]
     for (int k = 0; k < L; ++k) {
       const long n = (long)dims[k] * dims[k + 1] * d;

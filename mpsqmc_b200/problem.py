@@ -204,6 +204,36 @@ def write_mps(path: str, m: MPS) -> None:
     open(path, "w").write("\n".join(lines) + "\n")
 
 
+def left_normalize(m: MPS) -> MPS:
+    """Left-canonical form by QR sweeps (numpy's QR; the last site carries the norm, which is
+    divided out).  For synthetic inputs: the reference-exact LeftNormalize is the engine's
+    set_overlap and the oracle's."""
+    L, d = m.L, 2
+    dims = list(m.dims)
+    sites = []
+    off = 0
+    for k in range(L):
+        n = dims[k] * dims[k + 1] * d
+        sites.append(m.data[off:off + n].reshape((d, dims[k + 1], dims[k])).transpose(2, 0, 1))  # [r, s, c]
+        off += n
+    out = []
+    carry = np.ones((1, 1))
+    for k in range(L):
+        A = np.einsum("ab,bsc->asc", carry, sites[k])
+        a, s_, c = A.shape
+        if k < L - 1:
+            Q, R = np.linalg.qr(A.reshape(a * s_, c))
+            r = Q.shape[1]
+            out.append(Q.reshape(a, s_, r))
+            carry = R
+            dims[k + 1] = r
+        else:
+            A = A / np.linalg.norm(A)
+            out.append(A)
+    data = np.concatenate([t.transpose(1, 2, 0).ravel() for t in out])  # [s, c, r] -> r fastest
+    return MPS(np.asarray(dims, np.int32), data)
+
+
 def compress(m: MPS, D: int, cut: float = 1e-13) -> MPS:
     """Two-sweep two-site SVD truncation to bond dimension D (MPSstate.cpp:379-404 with
     TwoSiteObject.cpp:71-184): left-to-right with S pushed right, then right-to-left with S

@@ -70,10 +70,34 @@ def site_flops(a_l, a_r, b_l, b_r, d=2):
     return 2 * d * min(b_l * a_r * (a_l + b_r), a_l * b_r * (b_l + a_r))
 
 
-def algorithmic_flops_per_walker_step(aT, bW, couplings, d=2, mpo_nnz_bulk=8):
-    """Algorithmic FP work of one walker-step of the nearest-neighbour walk (canonical count):
-    per coupling (i, j), g = j - i: (5g + 4 + r_c) T_i + 16 closures of 2 a b + QR of the two
-    touched walker sites (4 m n^2 - 4/3 n^3 + 2 d n^3, m = d b_l, n = b_r); per step L T for the
+def mpo_nnz(L, couplings, h=0.0):
+    """Nonzero operator entries of each site's compact MPO for H = sum J S_i.S_j - h sum S^z:
+    done -> done, identity -> identity, the field, 3 per coupling closed on the site, 3 per
+    channel carried through it and 3 for the channel it opens.  8 per bulk site of the
+    nearest-neighbour chain."""
+    last = {}
+    for (i, j) in couplings:
+        last[i] = max(last.get(i, -1), j)
+    nnz = []
+    for k in range(L):
+        n = (1 if k > 0 else 0) + (1 if k < L - 1 else 0) + (1 if h != 0.0 else 0)
+        for i, lj in last.items():
+            if i < k <= lj:
+                if (i, k) in couplings:
+                    n += 3
+                if lj > k:
+                    n += 3
+        if last.get(k, -1) > k:
+            n += 3
+        nnz.append(n)
+    return nnz
+
+
+def algorithmic_flops_per_walker_step(aT, bW, couplings, d=2, h=0.0):
+    """Algorithmic FP work of one walker-step (canonical count): per coupling (i, j), g = j - i:
+    (5g + 4 + r_c) T_i, with r_c the right environments an earlier coupling of the step invalidated
+    (sites beyond j changed since they were built); 16 closures of 2 a b; QR of the two touched
+    walker sites (4 m n^2 - 4/3 n^3 + 2 d n^3, m = d b_l, n = b_r); per step L T for the
     right-environment sweep and sum_k nnz(W_k) T_k for the local energy."""
     aT, bW = list(aT), list(bW)
     L = len(aT) - 1
@@ -83,14 +107,59 @@ def algorithmic_flops_per_walker_step(aT, bW, couplings, d=2, mpo_nnz_bulk=8):
         m, n = d * bW[k], bW[k + 1]
         return 4 * m * n * n - (4.0 / 3.0) * n ** 3 + 2 * d * n ** 3
 
+    couplings = [tuple(int(x) for x in c) for c in couplings]
     f = 0.0
+    valid_from = 1  # right environments R[k], k >= valid_from, describe the current walker
     for (i, j) in couplings:
         g = j - i
-        f += (5 * g + 4) * T[i]
+        r_c = max(0, valid_from - (j + 1))
+        f += (5 * g + 4 + r_c) * T[i]
         f += 16 * 2 * aT[i + 1] * bW[i + 1]
         f += qr(i) + qr(j)
+        valid_from = j + 1
     f += sum(T)
-    for k in range(L):
-        nnz = mpo_nnz_bulk if 0 < k < L - 1 else 4
-        f += nnz * T[k]
+    cs = set(couplings)
+    for k, n in enumerate(mpo_nnz(L, cs, h)):
+        f += n * T[k]
     return f
+
+
+@dataclass
+class LatticeWorkload:
+    """A 2D open W x H Heisenberg lattice on the snake path with a D_T trial and walkers made on
+    the device by CompressState to per-walker bond dimensions (the 2D configurations)."""
+    name: str
+    W: int
+    H: int
+    DT: int
+    Ds: list
+    Nw: int
+    dtau: float
+    seed: int = 20131015
+
+    @property
+    def L(self):
+        return self.W * self.H
+
+    def couplings(self):
+        return pb.snake(self.W, self.H)
+
+    def targets(self):
+        rng = np.random.default_rng(self.seed + 1)
+        return rng.choice(np.asarray(self.Ds, dtype=np.int32), size=self.Nw)
+
+    def trial(self):
+        rng = np.random.default_rng(self.seed)
+        dims = pb.virtual_dims(self.L, self.DT)
+        data = rng.normal(size=int(sum(dims[k] * dims[k + 1] * 2 for k in range(self.L))))
+        return pb.left_normalize(pb.MPS(dims, data))
+
+
+def snake6x6(Nw: int = 1024) -> LatticeWorkload:
+    """6x6 open lattice, D_T = 128, walkers of D_W drawn uniformly from {16, 32, 64, 128}, dtau 0.005."""
+    return LatticeWorkload("snake6x6", 6, 6, 128, [16, 32, 64, 128], Nw, 0.005)
+
+
+def snake8x8(Nw: int = 4096) -> LatticeWorkload:
+    """8x8 open lattice, D_T = 256, D_W = 64, dtau 0.005."""
+    return LatticeWorkload("snake8x8", 8, 8, 256, [64], Nw, 0.005)
