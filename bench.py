@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--sweep", default="auto", choices=["auto", "nearest", "general"],
                     help="walker-step kernel (auto: nearest-neighbour for chains)")
+    ap.add_argument("--workspace", default="auto", choices=["auto", "global"],
+                    help="matrix work buffers: shared memory when they fit (auto) or global scratch")
     return ap.parse_args()
 
 
@@ -187,14 +189,16 @@ def main():
                            f"dtau={wl.dtau}, Marsaglia(4) grid, FP64; seeded random left-normalised trial of the "
                            f"D_T shape, walkers = trial compressed on the device",
                "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.Ds, "dtau": wl.dtau,
-               "parallelism": f"replicas x{world}", "sweep": args.sweep}
+               "parallelism": f"replicas x{world}", "sweep": args.sweep,
+               "workspace": args.workspace}
     else:
         wl = workloads.chain64(Nw=args.walkers or 2048)
         cfg = {"workload": f"{wl.name}: L={wl.L} Heisenberg chain, D_T={wl.DT}, D_W={wl.DW}, {wl.Nw} walkers/GPU, "
                            f"dtau={wl.dtau}, Marsaglia(4) grid, FP64",
                "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.DW, "dtau": wl.dtau,
                "l2": f"population ({wl.Nw * wl.walker.data.size * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
-               "parallelism": f"replicas x{world}", "sweep": args.sweep}
+               "parallelism": f"replicas x{world}", "sweep": args.sweep,
+               "workspace": args.workspace}
 
     if args.impl == "reference":
         if rank != 0:
@@ -242,6 +246,9 @@ def main():
         N = walkers.shape[0]
         eng.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
     eng.set_option(OPT_SWEEP, sweep)
+    if args.workspace == "global":
+        from mpsqmc_b200.capi import OPT_WORKSPACE, WORKSPACE_GLOBAL
+        eng.set_option(OPT_WORKSPACE, WORKSPACE_GLOBAL)
     eng.set_rng(wl.seed + 7919 * rank, 0)
     eng.walk(args.warmup)
     torch.cuda.synchronize()
