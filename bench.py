@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--sweep", default="auto", choices=["auto", "nearest", "general"],
-                    help="walker-step kernel (auto: nearest-neighbour for chains)")
+                    help="walker-step kernel (auto: the general sweep)")
     ap.add_argument("--workspace", default="auto", choices=["auto", "global"],
                     help="matrix work buffers: shared memory when they fit (auto) or global scratch")
     return ap.parse_args()
@@ -326,8 +326,8 @@ def main():
             "energy": {"E_P_last": stats[-1]["E_P"], "E_T_last": stats[-1]["E_T"], "walkers_last": stats[-1]["n_after"]},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": prof_traffic,
-                         "kernel": "walker_step_general_kernel" if (lattice or args.sweep == "general")
-                         else "walker_step_kernel", "flops_per_walker_step": flops_ws,
+                         "kernel": "walker_step_kernel" if args.sweep == "nearest" else "walker_step_general_kernel",
+                         "flops_per_walker_step": flops_ws,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor path)"},
             "cpu_baseline": cpu,
             "e2e": e2e,

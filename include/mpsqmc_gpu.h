@@ -167,7 +167,7 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
 /* Engine options.  No counterpart in the reference (its choices are compile-time).  A new value
  * takes effect from the next mpsqmc_walk step; unknown options or values give MPSQMC_E_ARG. */
 #define MPSQMC_OPT_SWEEP 1        /* walker-step kernel: */
-#define MPSQMC_SWEEP_AUTO 0       /*   nearest-neighbour sweep when every coupling is (i, i+1), else general */
+#define MPSQMC_SWEEP_AUTO 0       /*   the general sweep (the faster one, also on chains) */
 #define MPSQMC_SWEEP_NEAREST 1    /*   nearest-neighbour sweep (MPSQMC_E_UNSUPPORTED for longer couplings) */
 #define MPSQMC_SWEEP_GENERAL 2    /*   couplings (i, j) of any range, e.g. 2D lattices on a snake path */
 #define MPSQMC_OPT_WORKSPACE 2    /* where a CTA's matrix work buffers live: */

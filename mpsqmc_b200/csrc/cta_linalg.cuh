@@ -157,6 +157,138 @@ static __device__ __noinline__ void cta_gemm(int M, int N, int K, double alpha, 
   }
 }
 
+// Sixteen closures of two-site branch products, fused with the GEMM that forms them:
+//   out[k + 4 (s + 2 t)] = sum_{m < M, n < N} (A_s B_t)[m, n] P_k[m, n],   s, t in {0, 1}, k < 4,
+// A_s = A + s*sa (M x K, ld lda), B_t = B + t*sb (K x N, ld ldb), P_k = P + k*sp (ld ldp).
+// The products A_s B_t are never stored: each warp multiplies its 16x16 output blocks by the four
+// P blocks in the DMMA epilogue, and one CTA reduction writes the 16 sums to out (shared memory).
+// FAST requires M, N, K multiples of 16 (fragments loaded a chunk of four k-steps at a time);
+// otherwise every element access is bounds-checked.  red: >= 16*kWarps doubles.  Starts and ends with a
+// barrier inside the reduction.
+template <bool FAST>
+static __device__ __noinline__ void cta_closure16(int M, int N, int K, const double *A, int lda, long sa,
+                                                  const double *B, int ldb, long sb, const double *P, int ldp,
+                                                  long sp, double *red, double *out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int bm = (M + 15) >> 4, bn = (N + 15) >> 4;
+  double v[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = 0.0;
+  for (int blk = warp; blk < bm * bn; blk += kWarps) {
+    const int m0 = (blk % bm) << 4, n0 = (blk / bm) << 4;
+    const int ma = m0 + g, mb = m0 + 8 + g, na = n0 + g, nb = n0 + 8 + g;
+#pragma unroll 1
+    for (int s = 0; s < 2; ++s) {
+      const double *As = A + s * sa;
+      double acc[2][2][2][2], w[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) w[q] = 0.0;
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) acc[u][i][j][0] = acc[u][i][j][1] = 0.0;
+      if (FAST) {
+        // per chunk of four k-steps: all fragment loads first, then the 32 DMMAs
+        const double *pa0 = As + ma + (long)lda * t, *pa1 = As + mb + (long)lda * t;
+        const double *pb00 = B + t + (long)ldb * na, *pb01 = B + t + (long)ldb * nb;
+        const double *pb10 = pb00 + sb, *pb11 = pb01 + sb;
+        const long sA = 4L * lda;
+        for (int k0 = 0; k0 < K; k0 += 16) {
+          const int off = k0 / 4;
+          double a0[4], a1[4], b00[4], b01[4], b10[4], b11[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            a0[u] = pa0[(off + u) * sA];
+            a1[u] = pa1[(off + u) * sA];
+            b00[u] = pb00[4 * (off + u)];
+            b01[u] = pb01[4 * (off + u)];
+            b10[u] = pb10[4 * (off + u)];
+            b11[u] = pb11[4 * (off + u)];
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            dmma884(acc[0][0][0][0], acc[0][0][0][1], a0[u], b00[u]);
+            dmma884(acc[0][0][1][0], acc[0][0][1][1], a0[u], b01[u]);
+            dmma884(acc[0][1][0][0], acc[0][1][0][1], a1[u], b00[u]);
+            dmma884(acc[0][1][1][0], acc[0][1][1][1], a1[u], b01[u]);
+            dmma884(acc[1][0][0][0], acc[1][0][0][1], a0[u], b10[u]);
+            dmma884(acc[1][0][1][0], acc[1][0][1][1], a0[u], b11[u]);
+            dmma884(acc[1][1][0][0], acc[1][1][0][1], a1[u], b10[u]);
+            dmma884(acc[1][1][1][0], acc[1][1][1][1], a1[u], b11[u]);
+          }
+        }
+      } else {
+        for (int k0 = 0; k0 < K; k0 += 4) {
+          const int k = k0 + t;
+          const bool kin = k < K;
+          double a0 = 0.0, a1 = 0.0, b[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+          if (kin) {
+            if (ma < M) a0 = As[ma + (long)lda * k];
+            if (mb < M) a1 = As[mb + (long)lda * k];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              if (na < N) b[u][0] = B[u * sb + k + (long)ldb * na];
+              if (nb < N) b[u][1] = B[u * sb + k + (long)ldb * nb];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            dmma884(acc[u][0][0][0], acc[u][0][0][1], a0, b[u][0]);
+            dmma884(acc[u][0][1][0], acc[u][0][1][1], a0, b[u][1]);
+            dmma884(acc[u][1][0][0], acc[u][1][0][1], a1, b[u][0]);
+            dmma884(acc[u][1][1][0], acc[u][1][1][1], a1, b[u][1]);
+          }
+        }
+      }
+      // epilogue: dot the product blocks with the four P blocks
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int m = m0 + 8 * i + g, n = n0 + 8 * j + 2 * t + e;
+            if (FAST || (m < M && n < N)) {
+              const double *pp = P + m + (long)ldp * n;
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                const double pk = pp[k * sp];
+                w[k] += acc[0][i][j][e] * pk;
+                w[k + 4] += acc[1][i][j][e] * pk;
+              }
+            }
+          }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (s == 0) {
+          v[k] += w[k];
+          v[k + 8] += w[k + 4];
+        } else {
+          v[k + 4] += w[k];
+          v[k + 12] += w[k + 4];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 16; ++q)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < 16; ++q) red[q * kWarps + warp] = v[q];
+  __syncthreads();
+  if (threadIdx.x < 16) {
+    double sum = 0.0;
+    for (int w = 0; w < kWarps; ++w) sum += red[threadIdx.x * kWarps + w];
+    out[threadIdx.x] = sum;
+  }
+  __syncthreads();
+}
+
 // Sum of v over the CTA; result returned to every thread.  red: >= kWarps doubles of smem.
 __device__ __forceinline__ double cta_sum(double v, double *red) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

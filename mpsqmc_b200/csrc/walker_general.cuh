@@ -155,29 +155,17 @@ static __device__ void env_update_general(const Dev &p, Smem &s, int k, const do
 // Closures of the four left branches in Pb (cut j, a_j x b_j) with the right branches of site j
 // (walker site in Nxt, R[j+1] at Rn): M[p + 4q] = <P_p, B_j[s'] R[j+1] A_j[t']^T>, q = s' + 2t'.
 static __device__ void closures(const Dev &p, Smem &s, int j, const double *Rn) {
-  const int d = kMaxD, tid = threadIdx.x;
+  const int d = kMaxD;
   const int aj = p.aT[j], a2 = p.aT[j + 1], bj = s.bW[j], b2 = s.bW[j + 1];
   const double *Bj = p.trial + p.toff[j];
   for (int tau = 0; tau < d; ++tau)
     cta_gemm(a2, bj, b2, 1.0, Rn, a2, false, s.Nxt + tau * s.sbC, p.pb, true, 0.0, s.Xb + tau * s.sbX, p.pa);
   __syncthreads();
-  for (int sg = 0; sg < d; ++sg)
-    for (int tau = 0; tau < d; ++tau) {
-      cta_gemm(aj, bj, a2, 1.0, Bj + (long)sg * aj * a2, aj, false, s.Xb + tau * s.sbX, p.pa, false, 0.0,
-               s.Qt, p.pa);
-      __syncthreads();
-      double v[4] = {0.0, 0.0, 0.0, 0.0};
-      for (int q = tid; q < aj * bj; q += kThreads) {
-        const int r = q % aj, cc = q / aj;
-        const double qv = s.Qt[r + p.pa * cc];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) v[k] += s.Pb[k * s.sbX + r + p.pa * cc] * qv;
-      }
-      cta_sum4(v, s.red);
-      if (tid == 0)
-        for (int k = 0; k < 4; ++k) s.M[k + 4 * (sg + d * tau)] = v[k];
-    }
-  __syncthreads();
+  // M[k + 4 (s' + 2 t')] = <P_k, B_j[s'] Y[t']>, the products formed and dotted in one pass
+  if (((aj | bj | a2) & 15) == 0)
+    cta_closure16<true>(aj, bj, a2, Bj, aj, (long)aj * a2, s.Xb, p.pa, s.sbX, s.Pb, p.pa, s.sbX, s.red, s.M);
+  else
+    cta_closure16<false>(aj, bj, a2, Bj, aj, (long)aj * a2, s.Xb, p.pa, s.sbX, s.Pb, p.pa, s.sbX, s.red, s.M);
 }
 
 // C_kl from the closures, PDF over the grid, weight update, CDF sample with the walker's uniform

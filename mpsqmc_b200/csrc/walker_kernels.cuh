@@ -119,7 +119,7 @@ __host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, i
     boff += r;
   };
   const int d = kMaxD;
-  take(s ? s->red : dummy, 4 * kWarps);
+  take(s ? s->red : dummy, 16 * kWarps);
   take(s ? s->tau : dummy, maxB);
   take(s ? s->wv : dummy, maxB);
   take(s ? s->M : dummy, 16);

@@ -14,7 +14,7 @@ import pytest
 from conftest import WALK_CASES, couplings, load_golden
 from mpsqmc_b200 import Engine
 from mpsqmc_b200 import problem as pb
-from mpsqmc_b200.capi import OPT_SWEEP, OPT_WORKSPACE, SWEEP_GENERAL, WORKSPACE_GLOBAL
+from mpsqmc_b200.capi import OPT_SWEEP, OPT_WORKSPACE, SWEEP_NEAREST, WORKSPACE_GLOBAL
 from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu
@@ -46,19 +46,21 @@ def fidelity(dims_a, a, dims_b, b):
     return ab / np.sqrt(po.inner_product(A, A) * po.inner_product(B, B))
 
 
-MODES = {"auto": (None, None), "general": (SWEEP_GENERAL, None), "global-ws": (None, WORKSPACE_GLOBAL),
-         "general-global-ws": (SWEEP_GENERAL, WORKSPACE_GLOBAL)}
+MODES = {"auto": (None, None), "nearest": (SWEEP_NEAREST, None), "global-ws": (None, WORKSPACE_GLOBAL),
+         "nearest-global-ws": (SWEEP_NEAREST, WORKSPACE_GLOBAL)}
 
 
 @pytest.mark.parametrize("mode", list(MODES))
 @pytest.mark.parametrize("case", WALK_CASES)
 def test_walk_matches_reference(case, mode):
-    """Chains run the nearest-neighbour sweep by default and, forced, the general sweep; 2D
-    lattices always run the general sweep.  "global-ws" keeps the matrix work buffers in global
-    scratch (the placement large bond dimensions use) instead of shared memory."""
+    """Every case runs the general sweep (the default); chains also run the nearest-neighbour
+    sweep.  "global-ws" keeps the matrix work buffers in global scratch (the placement large bond
+    dimensions use) instead of shared memory."""
     z = load_golden(case)
     meta = z["meta"]
     sweep, ws = MODES[mode]
+    if sweep == SWEEP_NEAREST and "snake" in case:
+        pytest.skip("the nearest-neighbour sweep takes chains only")
     eng = engine_for(z, sweep=sweep, workspace=ws)
     assert eng.energy() == pytest.approx(meta["E0"], rel=RTOL)
     total_draws = 0
