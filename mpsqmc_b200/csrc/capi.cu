@@ -122,7 +122,8 @@ struct mpsqmc_ctx {
   int *d_cp_j = nullptr, *d_cp_q = nullptr, *d_site_c0 = nullptr, *d_ech_off = nullptr, *d_ech_slot = nullptr,
       *d_ech_cont = nullptr, *d_eopen = nullptr;
   double *d_ech_J = nullptr;
-  double *d_bondJ = nullptr, *d_tabU = nullptr, *d_tabS = nullptr, *d_tabVT = nullptr, *d_grid = nullptr;
+  double *d_bondJ = nullptr, *d_tabU = nullptr, *d_tabS = nullptr, *d_tabVT = nullptr, *d_grid = nullptr,
+         *d_tabSq = nullptr;
   double *d_scratch = nullptr, *d_trace = nullptr;
   int *d_err = nullptr;
   mq::MtState *d_mt = nullptr;
@@ -179,6 +180,7 @@ mq::Dev make_dev(mpsqmc_ctx *c) {
   p.tabU = c->d_tabU;
   p.tabS = c->d_tabS;
   p.tabVT = c->d_tabVT;
+  p.tabSq = c->d_tabSq;
   p.grid = c->d_grid;
   for (int k = 0; k < 4; ++k) {
     p.opSx[k] = c->opSx[k];
@@ -234,7 +236,7 @@ void free_all(mpsqmc_ctx *c) {
                   c->d_bondJ, c->d_tabU, c->d_tabS, c->d_tabVT, c->d_grid, c->d_scratch, c->d_trace,
                   c->d_err, c->d_mt, c->d_sd, c->d_cp_j, c->d_cp_q, c->d_site_c0, c->d_ech_off,
                   c->d_ech_slot, c->d_ech_cont, c->d_eopen, c->d_ech_J, c->d_ncop, c->d_wdims, c->d_wofs,
-                  c->d_ctr, c->d_stage, c->d_cscr, c->d_targets};
+                  c->d_ctr, c->d_stage, c->d_cscr, c->d_targets, c->d_tabSq};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
@@ -461,6 +463,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
         dalloc(&c->d_uni, (size_t)cap * c->nC) | dalloc(&c->d_ubr, cap) | dalloc(&c->d_bond_c, L - 1) |
         dalloc(&c->d_bond_j, L - 1) | dalloc(&c->d_bondJ, L - 1) | dalloc(&c->d_tabU, 16 * c->nJ) |
         dalloc(&c->d_tabS, 4 * c->nJ) | dalloc(&c->d_tabVT, 16 * c->nJ) | dalloc(&c->d_grid, 4 * c->G) |
+        dalloc(&c->d_tabSq, 4 * c->nJ) |
         dalloc(&c->d_scratch, (size_t)c->max_ctas * c->scr_stride) | dalloc(&c->d_err, 1) |
         dalloc(&c->d_mt, 1) | dalloc(&c->d_sd, 1) | dalloc(&c->d_cp_j, c->nC) | dalloc(&c->d_cp_q, c->nC) |
         dalloc(&c->d_site_c0, L + 1) | dalloc(&c->d_ech_off, L + 1) | dalloc(&c->d_ech_slot, ech_slot.size()) |
@@ -471,6 +474,8 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   if (cudaMallocHost((void **)&c->h_sd, sizeof(mq::StepDev)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_err, sizeof(int)) != cudaSuccess)
     return bail(fail(MPSQMC_E_CUDA, "pinned host buffers"));
+  std::vector<double> sqS(4 * c->nJ);
+  for (int q = 0; q < 4 * c->nJ; ++q) sqS[q] = std::sqrt(cfg->S[q]);
   auto up = [&](void *dst, const void *src, size_t bytes) {
     return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
   };
@@ -484,6 +489,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
             up(c->d_bondJ, bondJ.data(), sizeof(double) * (L - 1)) &&
             up(c->d_tabU, cfg->U, sizeof(double) * 16 * c->nJ) && up(c->d_tabS, cfg->S, sizeof(double) * 4 * c->nJ) &&
             up(c->d_tabVT, cfg->VT, sizeof(double) * 16 * c->nJ) && up(c->d_grid, cfg->grid, sizeof(double) * 4 * c->G) &&
+            up(c->d_tabSq, sqS.data(), sizeof(double) * 4 * c->nJ) &&
             up(c->d_cp_j, cp_j.data(), sizeof(int) * c->nC) && up(c->d_cp_q, cp_q.data(), sizeof(int) * c->nC) &&
             up(c->d_site_c0, site_c0.data(), sizeof(int) * (L + 1)) &&
             up(c->d_ech_off, ech_off.data(), sizeof(int) * (L + 1)) &&

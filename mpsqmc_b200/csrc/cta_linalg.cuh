@@ -321,12 +321,19 @@ __device__ __forceinline__ void cta_sum4(double v[4], double *red) {
   }
 }
 
-__device__ __forceinline__ double dlapy2(double x, double y) {
-  const double xa = fabs(x), ya = fabs(y);
-  const double w = fmax(xa, ya), z = fmin(xa, ya);
-  if (z == 0.0) return w;
-  const double r = z / w;
-  return w * sqrt(1.0 + r * r);
+// dlarfg's coefficients for a column with head alpha and squared tail norm xnorm2 > 0:
+// beta = -sign(alpha) ||(alpha, x)||, tau = (beta - alpha) / beta, scale of the tail 1/(alpha - beta).
+// FP64 square roots and divisions are long dependent sequences on this GPU, and this sits on the
+// QR's critical path (once per column): one sqrt of alpha^2 + xnorm2 (no overflow at the
+// magnitudes of normalised MPS tensors) and one division serve all three.
+__device__ __forceinline__ void reflector_coeffs(double alpha, double xnorm2, double &beta, double &tau,
+                                                 double &scale) {
+  const double mag = sqrt(fma(alpha, alpha, xnorm2));
+  beta = (alpha >= 0.0) ? -mag : mag;
+  const double dd = alpha - beta;  // nonzero: |beta| > 0 and of opposite sign to alpha
+  const double r = 1.0 / (beta * dd);
+  tau = -dd * dd * r;               // (beta - alpha) / beta
+  scale = beta * r;                 // 1 / (alpha - beta)
 }
 
 // Apply H = I - tau v v^T (v = (1, col[i+1..m)) stored below the diagonal of column i) to the
@@ -407,12 +414,7 @@ static __device__ __noinline__ void cta_qr_reg(int m, int n, double *__restrict_
       for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(full, part, o);
       alpha = __shfl_sync(full, alpha, i & 31);
       double ti = 0.0, beta = alpha, sc = 1.0;
-      if (m - i > 1 && part > 0.0) {
-        const double mag = dlapy2(alpha, sqrt(part));
-        beta = (alpha >= 0.0) ? -mag : mag;
-        ti = (beta - alpha) / beta;
-        sc = 1.0 / (alpha - beta);
-      }
+      if (m - i > 1 && part > 0.0) reflector_coeffs(alpha, part, beta, ti, sc);
 #pragma unroll
       for (int c = 0; c < MAXC; ++c)
         if (c == ci) {
@@ -570,10 +572,8 @@ static __device__ __noinline__ void cta_householder_qr(int m, int n, double *A, 
       const double alpha = col[i];
       double ti = 0.0;
       if (m - i > 1 && part > 0.0) {
-        const double mag = dlapy2(alpha, sqrt(part));
-        const double beta = (alpha >= 0.0) ? -mag : mag;
-        ti = (beta - alpha) / beta;
-        const double sc = 1.0 / (alpha - beta);
+        double beta, sc;
+        reflector_coeffs(alpha, part, beta, ti, sc);
         for (int r = i + 1 + lane; r < m; r += 32) col[r] *= sc;
         __syncwarp();
         if (lane == 0) col[i] = beta;

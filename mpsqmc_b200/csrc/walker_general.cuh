@@ -173,7 +173,7 @@ static __device__ void closures(const Dev &p, Smem &s, int j, const double *Rn) 
 // Returns 4 sum_kl C_kl x_k x_l of the sampled point (the new unnormalised overlap).
 static __device__ double sample_coupling(const Dev &p, Smem &s, int w, int c, int jq, double ov, double &wt) {
   const int tid = threadIdx.x;
-  const double *U = p.tabU + 16 * jq, *S = p.tabS + 4 * jq, *VT = p.tabVT + 16 * jq;
+  const double *U = p.tabU + 16 * jq, *Sq = p.tabSq + 4 * jq, *VT = p.tabVT + 16 * jq;
   if (tid < 16) {
     const int k = tid & 3, l = tid >> 2;
     double acc = 0.0;
@@ -182,7 +182,7 @@ static __device__ double sample_coupling(const Dev &p, Smem &s, int w, int c, in
       for (int pp = 0; pp < 4; ++pp) inner += U[pp + 4 * k] * s.M[pp + 4 * qq];
       acc += inner * VT[l + 4 * qq];
     }
-    s.Cm[k + 4 * l] = sqrt(S[k]) * sqrt(S[l]) * acc;
+    s.Cm[k + 4 * l] = Sq[k] * Sq[l] * acc;
   }
   __syncthreads();
   const double fac = 4.0 / (ov * p.G);
@@ -220,7 +220,7 @@ static __device__ double sample_coupling(const Dev &p, Smem &s, int w, int c, in
     for (int q = 0; q < 4; ++q) {
       double o1 = 0.0, o2 = 0.0;
       for (int k = 0; k < 4; ++k) {
-        const double pf = sqrt(S[k] * 4.0) * x[k];
+        const double pf = 2.0 * Sq[k] * x[k];  // sqrt(4 s_k) x_k
         o1 += pf * U[q + 4 * k];
         o2 += pf * VT[k + 4 * q];
       }

@@ -55,6 +55,7 @@ struct Dev {
   const int *bond_j;   // distinct-J index of the bond's coupling      [L-1]
   const double *bondJ; // coupling strength of bond (i, i+1) or 0     [L-1]
   const double *tabU, *tabS, *tabVT;  // [nJ][16], [nJ][4], [nJ][16]
+  const double *tabSq;                 // [nJ][4]: sqrt(S)
   const double *grid;  // [G][4]
   double opSx[4], opISy[4], opSz[4];  // [sigma + d*tau]
   double h;
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
       double num = ov;  // overlap numerator after the bond (no coupling: unchanged)
       if (c >= 0) {
         const int jq = p.bond_j[i];
-        const double *U = p.tabU + 16 * jq, *S = p.tabS + 4 * jq, *VT = p.tabVT + 16 * jq;
+        const double *U = p.tabU + 16 * jq, *Sq = p.tabSq + 4 * jq, *VT = p.tabVT + 16 * jq;
         // left branches P[s + d t] = B_i[s]^T Lenv C[t]
         for (int tau = 0; tau < d; ++tau)
           cta_gemm(al, br, bl, 1.0, s.Lenv, p.pa, false, s.Cen + tau * s.sbC, p.pb, false, 0.0,
@@ -409,7 +410,7 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
             for (int pp = 0; pp < 4; ++pp) inner += U[pp + 4 * k] * s.M[pp + 4 * qq];
             acc += inner * VT[l + 4 * qq];
           }
-          s.Cm[k + 4 * l] = sqrt(S[k]) * sqrt(S[l]) * acc;
+          s.Cm[k + 4 * l] = Sq[k] * Sq[l] * acc;
         }
         __syncthreads();
         // PDF over the grid (MPSQMC2.cpp:554-567)
@@ -450,7 +451,7 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_kernel(Dev p) {
           for (int q = 0; q < 4; ++q) {
             double o1 = 0.0, o2 = 0.0;
             for (int k = 0; k < 4; ++k) {
-              const double pf = sqrt(S[k] * 4.0) * x[k];
+              const double pf = 2.0 * Sq[k] * x[k];  // sqrt(4 s_k) x_k
               o1 += pf * U[q + 4 * k];
               o2 += pf * VT[k + 4 * q];
             }
