@@ -316,7 +316,8 @@ def main():
 
     if rank == 0:
         prof_traffic = None
-        tp = os.path.join(ROOT, "profiles", "walker_step_kernel_traffic.json")
+        kname = "walker_step_kernel" if args.sweep == "nearest" else "walker_step_general_kernel"
+        tp = os.path.join(ROOT, "profiles", f"{kname}_traffic.json")
         if os.path.exists(tp) and not lattice and N == 2048:
             prof_traffic = json.load(open(tp)).get("bytes_per_launch")
         line = {
