@@ -102,6 +102,20 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def aggregate_ranks(pg, t_ms, k_ms, walker_steps):
+    """Whole-job figures over the ranks: the slowest rank's times (max) and the walker-steps of all
+    ranks (sum).  pg is torch.distributed (any backend) or None for one rank."""
+    if pg is None:
+        return t_ms, k_ms, float(walker_steps)
+    import torch
+    tt = torch.tensor([t_ms, k_ms, float(walker_steps)], dtype=torch.float64)
+    mx = tt.clone()
+    pg.all_reduce(mx, op=pg.ReduceOp.MAX)
+    sm = tt.clone()
+    pg.all_reduce(sm, op=pg.ReduceOp.SUM)
+    return float(mx[0]), float(mx[1]), float(sm[2])
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     return json.load(open(p)) if os.path.exists(p) else {}
@@ -263,15 +277,7 @@ def main():
     ws_done = sum(s["n_walkers"] for s in stats)
     t_ms = tim["total_ms"]
     k_ms = tim["step_kernel_ms"]
-    if pg is not None:
-        tt = torch.tensor([t_ms, k_ms, float(ws_done)], dtype=torch.float64)
-        mx = tt.clone()
-        pg.all_reduce(mx, op=pg.ReduceOp.MAX)
-        sm = tt.clone()
-        pg.all_reduce(sm, op=pg.ReduceOp.SUM)
-        t_ms, k_ms, ws_all = float(mx[0]), float(mx[1]), float(sm[2])
-    else:
-        ws_all = float(ws_done)
+    t_ms, k_ms, ws_all = aggregate_ranks(pg, t_ms, k_ms, ws_done)
     value = ws_all / (t_ms * 1e-3)
 
     # roofline of the dominant kernel (the walker-step kernel): canonical FP64 work / kernel time,
@@ -302,7 +308,8 @@ def main():
         t1 = time.perf_counter()
         ws2 = sum(s["n_walkers"] for s in st2)
         nbytes = host_w.nbytes
-        e2e = {"value": ws2 * world / (t1 - t0), "unit": "walker-steps/s",
+        t_e2e, _, ws2_all = aggregate_ranks(pg, (t1 - t0) * 1e3, 0.0, ws2)
+        e2e = {"value": ws2_all / (t_e2e * 1e-3), "unit": "walker-steps/s",
                "h2d_bytes_per_step": int(nbytes / args.steps),
                "d2h_bytes_per_step": int(back[0].nbytes / args.steps + 72)}
         eng2.close()
