@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--sweep", default="auto", choices=["auto", "nearest", "general"],
                     help="walker-step kernel (auto: the general sweep)")
+    ap.add_argument("--vn", type=int, default=0, metavar="STEPS",
+                    help="after the timed steps, walk STEPS more and report the variance-normalised "
+                         "throughput (blocking error of the mixed energy; first 20%% discarded)")
     ap.add_argument("--workspace", default="auto", choices=["auto", "global"],
                     help="matrix work buffers: shared memory when they fit (auto) or global scratch")
     return ap.parse_args()
@@ -280,6 +283,19 @@ def main():
     t_ms, k_ms, ws_all = aggregate_ranks(pg, t_ms, k_ms, ws_done)
     value = ws_all / (t_ms * 1e-3)
 
+    vn = None
+    if args.vn > 0:
+        from mpsqmc_b200 import analysis
+        more = eng.walk(args.vn)
+        vn = analysis.variance_normalised(value / max(world, 1), [x["E_P"] for x in more],
+                                          [x["n_walkers"] for x in more])
+        vn["throughput_per_gpu"] = value / max(world, 1)
+        if not lattice:
+            e_ref = float(np.load(os.path.join(ROOT, "mpsqmc_b200", "data", "trial_L64D64.npz"))["energy"])
+            vn["E_ref"] = e_ref
+            vn["E_ref_source"] = "DMRG D=64 energy of the trial (mpsqmc_b200/data)"
+            vn["abs_err_per_site"] = abs(vn["E_mean"] - e_ref) / wl.L
+
     # roofline of the dominant kernel (the walker-step kernel): canonical FP64 work / kernel time,
     # averaged over the walkers' own bond dims
     cpl = list(zip(inputs["ci"], inputs["cj"]))
@@ -340,6 +356,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": tim["launches"],
+            **({"variance_normalised": vn} if vn is not None else {}),
             "clocks": clk.summary(),
         }
         print(json.dumps(line))
