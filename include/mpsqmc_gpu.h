@@ -181,6 +181,17 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
 #define MPSQMC_RESAMPLE_COMB 1    /*   comb: one uniform u, walker w gets the teeth k + u in
                                    *   [S_w, S_w + s_w) of the running sum of scaled weights s,
                                    *   each copy with weight 1 (about Ndesired walkers) */
+#define MPSQMC_OPT_PROJECTOR 5    /* what one mpsqmc_walk step does: */
+#define MPSQMC_PROJECTOR_TROTTER 0    /* MPSQMC2::Walk: Trotter two-site propagators with auxiliary
+                                       * fields (default) */
+#define MPSQMC_PROJECTOR_MPO_TERMS 1  /* MPSQMC::Walk (MPSQMC.cpp:236-369): 1 - dtau H sampled one MPO
+                                       * term at a time (identity or one of the terms J Sx Sx, -J iSy
+                                       * iSy, J Sz Sz per coupling, -h Sz per site), weights summed
+                                       * into an int as the reference does, and the reference's
+                                       * population control (every walker: int(w s + u) copies of
+                                       * weight 1); the trace then holds [N][3] = PDF norm, uniform,
+                                       * picked term (0 = identity).  The population-control options
+                                       * above do not apply. */
 int mpsqmc_set_option(mpsqmc_ctx *ctx, int option, long value);
 int mpsqmc_get_option(mpsqmc_ctx *ctx, int option, long *value);
 

@@ -22,6 +22,8 @@ WORKSPACE_AUTO, WORKSPACE_GLOBAL = 0, 1
 OPT_POPCONTROL_INTERVAL = 3
 OPT_RESAMPLING = 4
 RESAMPLE_THRESHOLD, RESAMPLE_COMB = 0, 1
+OPT_PROJECTOR = 5
+PROJECTOR_TROTTER, PROJECTOR_MPO_TERMS = 0, 1
 
 # Every symbol include/mpsqmc_gpu.h declares.
 EXPORTED = [

@@ -20,6 +20,7 @@
 #include "walker_kernels.cuh"
 #include "walker_general.cuh"
 #include "compress.cuh"
+#include "legacy.cuh"
 
 namespace {
 
@@ -115,6 +116,12 @@ struct mpsqmc_ctx {
   int *d_ctr = nullptr;                 // work counters of the persistent kernels
   double *d_stage = nullptr;            // mpsqmc_get_walkers: walkers gathered into logical order
   int stage_walkers = 0;
+  // MPO-term projector (MPSQMC::Walk)
+  int projector = MPSQMC_PROJECTOR_TROTTER;
+  int nterms = 0;
+  long loff = 0;
+  int *d_term_slot = nullptr, *d_term_site = nullptr, *d_term_op = nullptr, *d_changed = nullptr;
+  double *d_term_pref = nullptr;
   double *d_cscr = nullptr;             // mpsqmc_compress_walkers: per-CTA scratch
   long cstride = 0;
   int *d_targets = nullptr;
@@ -236,7 +243,8 @@ void free_all(mpsqmc_ctx *c) {
                   c->d_bondJ, c->d_tabU, c->d_tabS, c->d_tabVT, c->d_grid, c->d_scratch, c->d_trace,
                   c->d_err, c->d_mt, c->d_sd, c->d_cp_j, c->d_cp_q, c->d_site_c0, c->d_ech_off,
                   c->d_ech_slot, c->d_ech_cont, c->d_eopen, c->d_ech_J, c->d_ncop, c->d_wdims, c->d_wofs,
-                  c->d_ctr, c->d_stage, c->d_cscr, c->d_targets, c->d_tabSq};
+                  c->d_ctr, c->d_stage, c->d_cscr, c->d_targets, c->d_tabSq, c->d_term_slot,
+                  c->d_term_site, c->d_term_op, c->d_changed, c->d_term_pref};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
@@ -265,7 +273,7 @@ int layout_workspace(mpsqmc_ctx *c, bool force_global) {
     return fail(MPSQMC_E_UNSUPPORTED, "grid too large for the shared-memory budget of one CTA");
   const void *kernels[] = {(const void *)mq::walker_step_kernel, (const void *)mq::set_overlap_kernel,
                            (const void *)mq::energy_kernel, (const void *)mq::walker_step_general_kernel,
-                           (const void *)mq::energy_general_kernel};
+                           (const void *)mq::energy_general_kernel, (const void *)mq::legacy_step_kernel};
   for (const void *k : kernels)
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes));
   int occ = 1;
@@ -375,6 +383,30 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
     ech_cont.push_back(0);
   }
 
+  // Terms of the MPO-term projector, in the order HeisenbergMPO::findNonZeroContributions lists
+  // them (HeisenbergMPO.cpp:456-553): per coupling J Sx Sx, -J iSy iSy, J Sz Sz; then -h Sz on
+  // every site.  slot: where the sweep stores the term's overlap without prefactor.
+  std::vector<int> term_slot, term_site, term_op;
+  std::vector<double> term_pref;
+  for (int c = 0; c < cfg->nC; ++c)
+    for (int a = 0; a < 3; ++a) {
+      term_slot.push_back(3 * c + a);
+      term_site.push_back(cfg->ci[c]);
+      term_site.push_back(cfg->cj[c]);
+      term_op.push_back(a + 1);
+      term_op.push_back(a + 1);
+      term_pref.push_back(a == 1 ? -cfg->cJ[c] : cfg->cJ[c]);
+    }
+  if (cfg->h != 0.0)
+    for (int k = 0; k < L; ++k) {
+      term_slot.push_back(3 * cfg->nC + k);
+      term_site.push_back(k);
+      term_site.push_back(-1);
+      term_op.push_back(3);
+      term_op.push_back(0);
+      term_pref.push_back(-cfg->h);
+    }
+
   mpsqmc_ctx *c = new mpsqmc_ctx();
   c->device = cfg->device;
   if (cudaSetDevice(c->device) != cudaSuccess) {
@@ -391,6 +423,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   c->dtau = cfg->dtau;
   c->h = cfg->h;
   c->nn = nn;
+  c->nterms = (int)term_pref.size();
   c->aT.assign(cfg->trial_dims, cfg->trial_dims + L + 1);
   c->bW.assign(cfg->walker_dims, cfg->walker_dims + L + 1);
   c->toff.resize(L);
@@ -424,7 +457,8 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   }
   c->foff = ro;
   c->choff = ro + 2L * 4 * c->maxA * c->maxB;
-  c->scr_base = c->choff + (2L + 3L * nslots) * c->maxA * c->maxB;
+  c->loff = c->choff + (2L + 3L * nslots) * c->maxA * c->maxB;
+  c->scr_base = c->loff + ((2L * (3L * c->nC + L + 1) + 31) & ~31L);
   for (int s = 0; s < 2; ++s)
     for (int t = 0; t < 2; ++t) {
       c->opSx[s + 2 * t] = op_sx(d, s, t);
@@ -469,7 +503,9 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
         dalloc(&c->d_site_c0, L + 1) | dalloc(&c->d_ech_off, L + 1) | dalloc(&c->d_ech_slot, ech_slot.size()) |
         dalloc(&c->d_ech_cont, ech_cont.size()) | dalloc(&c->d_eopen, L) | dalloc(&c->d_ech_J, ech_J.size()) |
         dalloc(&c->d_ncop, cap) | dalloc(&c->d_wdims, (size_t)cap * (L + 1)) | dalloc(&c->d_wofs, (size_t)cap * L) |
-        dalloc(&c->d_ctr, mq::kNumCtr);
+        dalloc(&c->d_ctr, mq::kNumCtr) | dalloc(&c->d_term_slot, term_slot.size()) |
+        dalloc(&c->d_term_site, term_site.size()) | dalloc(&c->d_term_op, term_op.size()) |
+        dalloc(&c->d_term_pref, term_pref.size()) | dalloc(&c->d_changed, cap);
   if (rc) return bail(MPSQMC_E_CUDA);
   if (cudaMallocHost((void **)&c->h_sd, sizeof(mq::StepDev)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_err, sizeof(int)) != cudaSuccess)
@@ -496,7 +532,11 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
             up(c->d_ech_slot, ech_slot.data(), sizeof(int) * ech_slot.size()) &&
             up(c->d_ech_cont, ech_cont.data(), sizeof(int) * ech_cont.size()) &&
             up(c->d_eopen, eopen.data(), sizeof(int) * L) &&
-            up(c->d_ech_J, ech_J.data(), sizeof(double) * ech_J.size());
+            up(c->d_ech_J, ech_J.data(), sizeof(double) * ech_J.size()) &&
+            up(c->d_term_slot, term_slot.data(), sizeof(int) * term_slot.size()) &&
+            up(c->d_term_site, term_site.data(), sizeof(int) * term_site.size()) &&
+            up(c->d_term_op, term_op.data(), sizeof(int) * term_op.size()) &&
+            up(c->d_term_pref, term_pref.data(), sizeof(double) * term_pref.size());
   if (!ok) return bail(fail(MPSQMC_E_CUDA, "upload failed"));
   {  // every slot starts with the common walker dims
     std::vector<int> wd((size_t)cap * (L + 1));
@@ -743,7 +783,48 @@ int mpsqmc_energy(mpsqmc_ctx *c, double *E_P) {
 
 // Issue one timestep on c->stream (also used under stream capture): every grid has its fixed
 // maximal size and every kernel reads the current walker count from device memory.
+static int enqueue_legacy_step(mpsqmc_ctx *c, int *launches) {
+  mq::Dev p = make_dev(c);
+  const int grid = c->max_ctas;
+  mq::LegacyDev lp;
+  lp.nterms = c->nterms;
+  lp.term_slot = c->d_term_slot;
+  lp.term_pref = c->d_term_pref;
+  lp.term_site = c->d_term_site;
+  lp.term_op = c->d_term_op;
+  lp.dtau = c->dtau;
+  lp.loff = c->loff;
+  lp.changed = c->d_changed;
+  lp.tr = c->trace_on ? c->d_trace : nullptr;
+  CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(int) * mq::kNumCtr, c->stream));
+  // one uniform per walker for the term choice (MPSQMC.cpp:342), in walker order
+  mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, c->d_ncur, 0, 1, c->d_uni);
+  CK(cudaEventRecordWithFlags(c->ev[0], c->stream, cudaEventRecordExternal));
+  mq::legacy_step_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p, lp);
+  CK(cudaEventRecordWithFlags(c->ev[1], c->stream, cudaEventRecordExternal));
+  // LeftNormalize + overlap + sign of the walkers a term hit (MPSQMC.cpp:355-362)
+  mq::Dev ps = p;
+  ps.sel = c->d_changed;
+  mq::set_overlap_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(ps);
+  mq::energy_general_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+  mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 1, c->d_flag_pos, c->d_sw, 1,
+                                              mq::kResampleLegacy);
+  mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, &c->d_sd->n_flag, 0, 1, c->d_ubr);
+  mq::branch_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->d_flag_pos, c->d_sw, c->d_ubr, c->d_slot_new,
+                                               c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
+                                               c->capacity, c->d_ncop, 1, mq::kResampleLegacy);
+  mq::copy_walkers_kernel<<<4 * c->sm_count, 256, 0, c->stream>>>(p, c->d_sd, c->d_copy_src, c->d_copy_dst);
+  mq::finish_branch_kernel<<<1, 1024, 0, c->stream>>>(c->d_sd, c->d_ncur, c->d_slot_of, c->d_slot_new, c->d_err,
+                                                      c->capacity);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->h_sd, c->d_sd, sizeof(mq::StepDev), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  *launches = 10;
+  return 0;
+}
+
 static int enqueue_step(mpsqmc_ctx *c, int *launches) {
+  if (c->projector == MPSQMC_PROJECTOR_MPO_TERMS) return enqueue_legacy_step(c, launches);
   mq::Dev p = make_dev(c);
   const int grid = c->max_ctas;
   CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(int) * mq::kNumCtr, c->stream));
@@ -824,7 +905,8 @@ int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
     int rc = build_graph(c, &per_step);
     if (rc) return rc;
   }
-  if (c->use_graph) per_step = (c->h != 0.0) ? 11 : 7;
+  if (c->use_graph)
+    per_step = (c->projector == MPSQMC_PROJECTOR_MPO_TERMS) ? 10 : ((c->h != 0.0) ? 11 : 7);
   double kernel_ms = 0.0;
   int launches = 0;
   CK(cudaEventRecord(c->ev[2], c->stream));
@@ -846,7 +928,8 @@ int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
     kernel_ms += ms;
     if (err & mq::kErrNumeric) return fail(MPSQMC_E_NUMERIC, "non-finite weight, overlap or energy");
     if (err & mq::kErrCapacity) return fail(MPSQMC_E_CAPACITY, "population control exceeded the walker capacity");
-    const unsigned long long dr = (unsigned long long)N * c->nC + (unsigned long long)sd.n_flag;
+    const int per_walker = (c->projector == MPSQMC_PROJECTOR_MPO_TERMS) ? 1 : c->nC;
+    const unsigned long long dr = (unsigned long long)N * per_walker + (unsigned long long)sd.n_flag;
     c->draws += dr;
     c->last_n_before = N;
     c->last_n_after = sd.n_new;
@@ -947,6 +1030,11 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
       c->workspace = (int)value;
       break;
     }
+    case MPSQMC_OPT_PROJECTOR:
+      if (value != MPSQMC_PROJECTOR_TROTTER && value != MPSQMC_PROJECTOR_MPO_TERMS)
+        return fail(MPSQMC_E_ARG, "unknown projector");
+      c->projector = (int)value;
+      break;
     case MPSQMC_OPT_POPCONTROL_INTERVAL:
       if (value < 1 || value > (1L << 30)) return fail(MPSQMC_E_ARG, "population-control interval must be >= 1");
       c->pc_interval = (int)value;
@@ -980,6 +1068,9 @@ int mpsqmc_get_option(mpsqmc_ctx *c, int option, long *value) {
       return 0;
     case MPSQMC_OPT_RESAMPLING:
       *value = c->resample;
+      return 0;
+    case MPSQMC_OPT_PROJECTOR:
+      *value = c->projector;
       return 0;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");

@@ -41,6 +41,7 @@ struct Dev {
   const int *wdims; // per slot: the walker's own bond dims [capacity][L+1] (<= bW)
   const long *wofs; // per slot: the walker's site offsets [capacity][L]
   int *ctr;         // work counters of the persistent kernels (zeroed before each launch)
+  const int *sel;   // set_overlap_kernel: only walkers w with sel[w] != 0 (nullptr: all)
   const double *trial;
   long wstride;     // doubles per walker slot
   double *walkers;
@@ -564,6 +565,7 @@ __global__ void __launch_bounds__(kThreads, 1) set_overlap_kernel(Dev p) {
   const int L = p.L, d = kMaxD, tid = threadIdx.x;
   const int N = *p.n_cur;
   for (int w = next_walker(s, p.ctr + kCtrSetOverlap); w < N; w = next_walker(s, p.ctr + kCtrSetOverlap)) {
+    if (p.sel != nullptr && p.sel[w] == 0) continue;
     const int slot = p.slot_of[w];
     load_walker_dims(p, s, slot);
     double *W = p.walkers + (long)slot * p.wstride;
@@ -789,7 +791,7 @@ __device__ double block_sum_d(double v, double *buf) {  // blockDim.x == 1024
 // Population control modes (mpsqmc_set_option): threshold branching of the reference, or comb
 // (systematic) resampling to Ndesired equal-weight walkers; either every `interval` steps, with
 // the weights only rescaled by Ndesired / sum(w) on the steps in between.
-enum : int { kResampleThreshold = 0, kResampleComb = 1 };
+enum : int { kResampleThreshold = 0, kResampleComb = 1, kResampleLegacy = 2 };
 
 // Weight sum, E_T, E_P, energy history, fluctuation metric (MPSQMC2.cpp:468-487, 688-747),
 // then the branching flags of SeparatePopulationControl (613-648).
@@ -811,8 +813,10 @@ __global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Nde
     sw += wt;
     num += wt * p.energy[w];
   }
-  const double sumw = block_sum_d(sw, dbuf);
+  const double sumw_full = block_sum_d(sw, dbuf);
   const double numer = block_sum_d(num, dbuf);
+  // the MPO-term projector sums the weights into an int (MPSQMC.cpp:364-366)
+  const double sumw = (mode == kResampleLegacy) ? (double)(int)sumw_full : sumw_full;
   const double avgW = sumw / N;
   const double scaling = Ndesired / (N * avgW);
   double se = 0.0, se2 = 0.0;
@@ -837,7 +841,7 @@ __global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Nde
     if (w < N) {
       s = p.wt_out[w] * scaling;
       sw_out[w] = s;
-      f = (branch_now && mode == kResampleThreshold && (s < 0.25 || s > 1.5)) ? 1 : 0;
+      f = (branch_now && ((mode == kResampleThreshold && (s < 0.25 || s > 1.5)) || mode == kResampleLegacy)) ? 1 : 0;
     }
     int tot;
     const int ex = block_scan_excl<int>(f, ibuf, tot);
@@ -848,7 +852,7 @@ __global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Nde
     sd->sumw = sumw;
     sd->scaling = scaling;
     sd->ET = log(scaling) / dtau;
-    sd->EP = numer / sumw;
+    sd->EP = numer / sumw_full;
     sd->omega = update_history ? (sE2 - sE * sE / N) / N : 0.0;
     sd->n_flag = (branch_now && mode == kResampleComb) ? 1 : nflag_total;
     if (!(isfinite(sumw) && sumw > 0.0 && isfinite(numer))) atomicOr(p.err, kErrNumeric);
@@ -906,7 +910,7 @@ __global__ void __launch_bounds__(1024) branch_kernel(Dev p, StepDev *sd, const 
       s = sw_in[w];
       nc = ncop[w];
       neww = s;
-      if (comb) neww = 1.0;
+      if (comb || mode == kResampleLegacy) neww = 1.0;  // MPSQMC.cpp:413: every copy gets weight 1
       else if (flag_pos[w] >= 0) neww = (s < 0.25) ? 1.0 : s / nc;
     }
     int tot_new, tot_extra;

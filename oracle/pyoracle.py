@@ -331,6 +331,20 @@ def load_npy_dir(path: str) -> dict:
     return out
 
 
+def harness_legacy(L: int, D: int, Nw: int, dtau: float, steps: int, seed: int, field: float = 0.0,
+                   lattice: str | None = None) -> dict:
+    """The reference's MPO-term projector MPSQMC (oracle/_ref/ref_harness legacy): its own DMRG
+    trial, walkers = trial copies, and the per-step quantities of MPSQMC::Walk."""
+    with tempfile.TemporaryDirectory() as tmp:
+        extra = {"MPSQMC_REF_SEED": str(seed)}
+        if field:
+            extra["MPSQMC_REF_FIELD"] = repr(float(field))
+        if lattice:
+            extra["MPSQMC_REF_LATTICE"] = lattice
+        run_harness("legacy", L, D, Nw, dtau, steps, tmp, env_extra=extra)
+        return load_npy_dir(tmp)
+
+
 def harness_walk(trial_path: str, DW: int, Nw: int, dtau: float, steps: int, trace=True,
                  tensors=False, seed: int | None = None, field: float = 0.0, lattice: str | None = None) -> dict:
     """The reference's MPSQMC2 walk (oracle/_ref/ref_harness walk); lattice "snake:WxH" selects the

@@ -35,6 +35,7 @@
 // Walk step by step.  Access specifiers do not change the layout g++ gives these classes.
 #define private public
 #include "MPSQMC2.h"
+#include "MPSQMC.h"
 #undef private
 #include "HeisenbergMPO.h"
 #include "GridGenerator.h"
@@ -627,10 +628,111 @@ int mode_propagate(int argc, char **argv) {
 // reference's parallelism is OpenMP over walkers, so BLAS calls stay single-threaded.
 extern "C" void openblas_set_num_threads(int);
 
+// Legacy MPO-term projector (MPSQMC.cpp): MPSQMC(mpo, RN, D, Nw, dtau) builds its own DMRG trial
+// and walkers; the body of MPSQMC::Walk (MPSQMC.cpp:236-318) is replayed step by step so that
+// per-walker quantities can be saved:
+//   legacy <L> <D> <Nw> <dtau> <steps> <outdir>
+int mode_legacy(int argc, char **argv) {
+  if (argc < 8) return 2;
+  const int L = atoi(argv[2]), D = atoi(argv[3]), Nw = atoi(argv[4]);
+  const double dtau = atof(argv[5]);
+  const int steps = atoi(argv[6]);
+  const std::string out = argv[7];
+  std::streambuf *old = std::cout.rdbuf(&g_nullbuf);
+  HeisenbergMPO mpo(L, 2, false);
+  build_chain(mpo, L);
+  mpo.findNonZeroContributions();  // the terms MPSQMC samples (main.cpp:144)
+  Random RN;
+  MPSQMC q(&mpo, &RN, D, Nw, dtau);
+  const unsigned long long setup_draws = mpsqmc_compat::mt_draw_count();
+  std::cout.rdbuf(old);
+  save_mps(out + "/trial_ln", q.Psi0[0]);
+  {  // the MPO terms the projector samples (HeisenbergMPO.cpp:456-553): prefactor, sites, ops
+    std::vector<double> pref;
+    std::vector<int> sites, ops;
+    for (int t = 0; t < mpo.gRN_nTerms(); ++t) {
+      pref.push_back(mpo.gRN_prefactor(t));
+      int s0 = -1, s1 = -1, o0 = -1, o1 = -1;
+      for (int k = 0; k < L; ++k) {
+        Operator *op = mpo.gRN_operator(t, k);
+        if (op->AmIOpI()) continue;
+        const int code = (op == mpo.gRN_operator(t, k) && (*op)(0, 1) != 0.0) ? (((*op)(0, 1) == (*op)(1, 0)) ? 1 : 2) : 3;
+        if (s0 < 0) { s0 = k; o0 = code; } else { s1 = k; o1 = code; }
+      }
+      sites.push_back(s0); sites.push_back(s1); ops.push_back(o0); ops.push_back(o1);
+    }
+    save_d(out + "/terms_prefactor.npy", pref);
+    save_i2(out + "/terms_sites.npy", sites, pref.size(), 2);
+    save_i2(out + "/terms_ops.npy", ops, pref.size(), 2);  // 1 Sx, 2 iSy, 3 Sz
+  }
+  std::vector<double> stat_sum, stat_EP, stat_ET, stat_omega, stat_scaling;
+  std::vector<int> stat_n, stat_draws;
+  const double E0 = q.EnergyFunction();
+  for (int step = 1; step <= steps; ++step) {
+    const unsigned long long d0 = mpsqmc_compat::mt_draw_count();
+    std::cout.rdbuf(&g_nullbuf);
+    const double sum = q.PropagateSeparately();
+    std::cout.rdbuf(old);
+    const int N = q.myNCurrentWalkers;
+    std::vector<double> coeff(q.walkerCoeff, q.walkerCoeff + N), ov(q.walkerOverlap, q.walkerOverlap + N), en(N);
+    for (int w = 0; w < N; ++w) en[w] = q.HPsi0[0]->InnerProduct(q.theWalkers[w]) / q.walkerOverlap[w];
+    char pre[64];
+    snprintf(pre, sizeof pre, "%s/step%03d_", out.c_str(), step);
+    save_d(std::string(pre) + "weight.npy", coeff);
+    save_d(std::string(pre) + "overlap.npy", ov);
+    save_d(std::string(pre) + "energy.npy", en);
+    const double avgCoeff = sum / q.totalNCurrentWalkers;
+    const double omega = q.updateEnergyHistory(step);
+    const double EP = q.EnergyFunction();
+    const double scaling = q.totalNDesiredWalkers / (q.totalNCurrentWalkers * avgCoeff);
+    const double ET = std::log(scaling) / dtau;
+    const unsigned long long d1 = mpsqmc_compat::mt_draw_count();
+    std::cout.rdbuf(&g_nullbuf);
+    q.SeparatePopulationControl(scaling);
+    std::cout.rdbuf(old);
+    q.totalNCurrentWalkers = q.myNCurrentWalkers;
+    const unsigned long long d2 = mpsqmc_compat::mt_draw_count();
+    const int Nn = q.myNCurrentWalkers;
+    std::vector<double> ov2(q.walkerOverlap, q.walkerOverlap + Nn), eh2(q.walkerEnergyHistorySum,
+                                                                     q.walkerEnergyHistorySum + Nn);
+    save_d(std::string(pre) + "newoverlap.npy", ov2);
+    save_d(std::string(pre) + "newehist.npy", eh2);
+    if (step == steps) {
+      for (int w = 0; w < Nn; ++w) {
+        char nm[96];
+        snprintf(nm, sizeof nm, "%swalker%04d", pre, w);
+        save_mps(nm, q.theWalkers[w]);
+      }
+    }
+    stat_sum.push_back(sum);
+    stat_EP.push_back(EP);
+    stat_ET.push_back(ET);
+    stat_omega.push_back(omega);
+    stat_scaling.push_back(scaling);
+    stat_n.push_back(N);
+    stat_draws.push_back((int)(d1 - d0));
+    stat_draws.push_back((int)(d2 - d1));
+  }
+  save_d(out + "/stat_sum.npy", stat_sum);
+  save_d(out + "/stat_EP.npy", stat_EP);
+  save_d(out + "/stat_ET.npy", stat_ET);
+  save_d(out + "/stat_omega.npy", stat_omega);
+  save_d(out + "/stat_scaling.npy", stat_scaling);
+  save_i(out + "/stat_n.npy", stat_n);
+  save_i2(out + "/stat_draws.npy", stat_draws, stat_draws.size() / 2, 2);
+  std::ostringstream js;
+  js << "{\"L\": " << L << ", \"D\": " << D << ", \"Nw\": " << Nw << ", \"dtau\": " << fmt17(dtau)
+     << ", \"steps\": " << steps << ", \"seed\": " << mpsqmc_compat::mt_last_seed()
+     << ", \"setup_draws\": " << setup_draws << ", \"E0\": " << fmt17(E0)
+     << ", \"nTerms\": " << mpo.gRN_nTerms() << ", \"h\": " << fmt17(field_from_env()) << "}";
+  write_json(out + "/meta.json", js.str());
+  return 0;
+}
+
 int main(int argc, char **argv) {
   openblas_set_num_threads(1);
   if (argc < 2) {
-    fprintf(stderr, "usage: ref_harness <dmrg|trotter|grid|mpsops|walk|time|propagate> ...\n");
+    fprintf(stderr, "usage: ref_harness <dmrg|trotter|grid|mpsops|walk|time|propagate|legacy> ...\n");
     return 2;
   }
   std::cout.precision(17);
@@ -643,6 +745,7 @@ int main(int argc, char **argv) {
   else if (m == "walk") rc = mode_walk(argc, argv);
   else if (m == "time") rc = mode_time(argc, argv);
   else if (m == "propagate") rc = mode_propagate(argc, argv);
+  else if (m == "legacy") rc = mode_legacy(argc, argv);
   if (rc == 2) fprintf(stderr, "bad arguments for mode %s\n", m.c_str());
   return rc;
 }

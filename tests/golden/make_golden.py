@@ -118,6 +118,26 @@ def gen_walk(name, trial: po.MPS, DW, Nw, dtau, steps, tensors=True, field=0.0, 
     save(name, **keep)
 
 
+def gen_legacy(name, L, D, Nw, dtau, steps, field=0.0, lattice=None):
+    D_ = po.harness_legacy(L, D, Nw, dtau, steps, seed=SEED, field=field, lattice=lattice)
+    meta = D_.pop("meta")
+    if lattice:
+        meta["lattice"] = lattice
+    last = f"step{steps:03d}_"
+    n = len(D_[last + "newoverlap"])
+    D_[last + "tensors"] = np.stack([D_.pop(f"{last}walker{w:04d}_data") for w in range(n)])
+    for w in range(n):
+        D_.pop(f"{last}walker{w:04d}_dims", None)
+    D_["meta"] = np.array(json.dumps(meta))
+    save(name, **D_)
+
+
+def gen_legacy_all():
+    gen_legacy("legacy_L10D8", 10, 8, 16, 0.05, 4)
+    gen_legacy("legacy_L10D8_field", 10, 8, 16, 0.05, 3, field=0.4)
+    gen_legacy("legacy_snake3x3_D8", 9, 8, 12, 0.1, 3, lattice="snake:3x3")
+
+
 def main():
     if not po.harness_available():
         po.build(ref=True)
@@ -134,6 +154,7 @@ def main():
     gen_walk("walk_debug_DW2", dbg, 2, 32, 0.01, 3)
     gen_walk("walk_L10D8_DW4_field", T(10, 8), 4, 16, 0.05, 3, field=0.7)
     gen_2d()
+    gen_legacy_all()
 
 
 def gen_2d():
@@ -153,5 +174,7 @@ if __name__ == "__main__":
             gen_walk("walk_L10D8_DW4_field", T(10, 8), 4, 16, 0.05, 3, field=0.7)
         if "2d" in only:
             gen_2d()
+        if "legacy" in only:
+            gen_legacy_all()
     else:
         main()
