@@ -128,3 +128,20 @@ def test_dropin_walk_runs_main_call_sequence(tmp_path):
     assert np.all(np.abs(EP - ed.ground_energy(10)) < 5e-3)   # projected energies stay at the ground state
     assert r.stdout.count("        Step = ") == steps
     assert "The min. encountered weight on rank 0 is" in r.stdout
+
+
+@pytest.mark.gpu
+def test_dropin_legacy_projector(tmp_path):
+    """MPSQMC (the MPO-term projector class) over the engine: DMRG trial on the host, walk on the
+    GPU, the reference's console lines and energies.txt; energies stay at the ground state."""
+    exe = compile_cpp(os.path.join(ROOT, "tests", "cpp", "dropin_legacy.cpp"), str(tmp_path / "dropin_legacy"))
+    steps = 5
+    r = subprocess.run([exe, "10", "8", "32", "0.05", str(steps), "0.0"], cwd=tmp_path, capture_output=True,
+                       text=True, env={**os.environ, "MPSQMC_SEED": "11"}, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "GPU engine unavailable" not in r.stderr and "MPSQMC::Walk" not in r.stderr
+    lines = (tmp_path / "energies.txt").read_text().splitlines()
+    assert lines[0].startswith("#Step") and len(lines) == steps + 1
+    EP = np.array([float(x.split()[1]) for x in lines[1:]])
+    assert np.all(np.abs(EP - ed.ground_energy(10)) < 5e-3)
+    assert r.stdout.count("        Step = ") == steps
