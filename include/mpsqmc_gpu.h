@@ -195,6 +195,14 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
 int mpsqmc_set_option(mpsqmc_ctx *ctx, int option, long value);
 int mpsqmc_get_option(mpsqmc_ctx *ctx, int option, long *value);
 
+/* Autotuner (no counterpart in the reference): times `steps` steps of every applicable
+ * (MPSQMC_OPT_SWEEP, MPSQMC_OPT_WORKSPACE) choice on the first walkers of the current population
+ * (two waves of one CTA per SM), restores the population, random stream and step count after
+ * each trial, and keeps the fastest.  The choice is remembered per problem shape (L, trial and
+ * walker bond dims, couplings, projector) for later contexts of this process, which then skip the
+ * measurement.  best_* (may be NULL) receive the chosen option values. */
+int mpsqmc_autotune(mpsqmc_ctx *ctx, int steps, int *best_sweep, int *best_workspace);
+
 /* ---------------------------------------------------------------------------------------------
  * Local energies without any device allocation.  No counterpart in the reference.
  *

@@ -32,7 +32,7 @@ EXPORTED = [
     "mpsqmc_energy", "mpsqmc_walk", "mpsqmc_last_step_walkers", "mpsqmc_set_trace",
     "mpsqmc_get_trace", "mpsqmc_last_timing", "mpsqmc_local_energy_noalloc", "mpsqmc_set_step",
     "mpsqmc_set_option", "mpsqmc_get_option", "mpsqmc_set_walkers_dims", "mpsqmc_get_walker_dims",
-    "mpsqmc_compress_walkers",
+    "mpsqmc_compress_walkers", "mpsqmc_autotune",
 ]
 
 
@@ -115,6 +115,7 @@ def load(build_if_missing: bool = True):
         "mpsqmc_set_walkers_dims": (C.c_int, [P, C.c_int, ip, dp, dp, dp, dp, C.c_int]),
         "mpsqmc_get_walker_dims": (C.c_int, [P, ip, ip]),
         "mpsqmc_compress_walkers": (C.c_int, [P, ip, C.c_int]),
+        "mpsqmc_autotune": (C.c_int, [P, C.c_int, ip, ip]),
         "mpsqmc_get_option": (C.c_int, [P, C.c_int, C.POINTER(C.c_long)]),
         "mpsqmc_local_energy_noalloc": (C.c_int, [C.POINTER(EnergyLayout), P, P, C.c_long, P, C.c_int, P,
                                                   C.c_int, P]),
@@ -199,6 +200,13 @@ class Engine:
         eh = None if ehist is None else np.ascontiguousarray(ehist, dtype=np.float64)
         check(self.lib.mpsqmc_set_walkers_dims(self._ctx, N, _ip(dm), _dp(packed), _dp(wt), _dp(ov), _dp(eh),
                                                int(normalize)))
+
+    def autotune(self, steps: int = 2):
+        """Time the kernel choices on a subset of the population and keep the fastest; returns
+        (sweep, workspace)."""
+        a, b = C.c_int(0), C.c_int(0)
+        check(self.lib.mpsqmc_autotune(self._ctx, steps, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def compress_walkers(self, target_D, normalize=True):
         """MPSstate::CompressState on the device: walker w to bond dimension target_D[w] (scalar: all)."""

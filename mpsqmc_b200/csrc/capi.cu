@@ -8,6 +8,8 @@
 
 #include <algorithm>
 #include <cstddef>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -956,6 +958,138 @@ int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
   c->last_kernel_ms = kernel_ms;
   c->last_total_ms = tot;
   c->last_launches = launches;
+  return 0;
+}
+
+// Autotuning: choices measured once per problem shape (L, trial and walker bond dims, coupling
+// structure, projector) and remembered for every later context of the same shape in this process.
+namespace {
+std::mutex g_tune_mutex;
+std::map<std::string, std::pair<int, int>> g_tuned;  // shape -> (sweep, workspace)
+
+std::string tune_key(const mpsqmc_ctx *c) {
+  std::ostringstream k;
+  k << c->L << '|' << c->nC << '|' << c->nn << '|' << c->projector << '|' << (c->h != 0.0) << '|';
+  for (int v : c->aT) k << v << ',';
+  k << '|';
+  for (int v : c->bW) k << v << ',';
+  return k.str();
+}
+}  // namespace
+
+int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspace) {
+  if (!c || steps < 1) return fail(MPSQMC_E_ARG, "bad arguments");
+  if (c->n_cur < 1) return fail(MPSQMC_E_ARG, "no walkers");
+  CK(cudaSetDevice(c->device));
+  const std::string key = tune_key(c);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      int rc = mpsqmc_set_option(c, MPSQMC_OPT_SWEEP, it->second.first);
+      if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_WORKSPACE, it->second.second);
+      if (best_sweep) *best_sweep = it->second.first;
+      if (best_workspace) *best_workspace = it->second.second;
+      return rc;
+    }
+  }
+  // candidates: every sweep that takes these couplings, both work-buffer placements (one when the
+  // buffers do not fit on chip)
+  std::vector<std::pair<int, int>> cands;
+  const bool fits = sizeof(double) * (size_t)c->all_doubles <= c->smem_optin;
+  for (int sw : {MPSQMC_SWEEP_GENERAL, MPSQMC_SWEEP_NEAREST}) {
+    if (sw == MPSQMC_SWEEP_NEAREST && (!c->nn || c->projector != MPSQMC_PROJECTOR_TROTTER)) continue;
+    cands.push_back({sw, MPSQMC_WORKSPACE_AUTO});
+    if (fits) cands.push_back({sw, MPSQMC_WORKSPACE_GLOBAL});
+  }
+  // measure on the first k walkers (two waves of one CTA per SM), with the population state saved
+  // and restored around every trial
+  const int N = c->n_cur, k = std::min(N, 2 * c->sm_count), cap = c->capacity, L = c->L;
+  std::vector<int> slots(N), h_free(cap), wd((size_t)cap * (L + 1));
+  std::vector<long> wf((size_t)cap * L);
+  std::vector<double> wt(cap), ov(cap), eh(cap);
+  mq::MtState mt;
+  mq::StepDev sd;
+  CK(cudaMemcpy(slots.data(), c->d_slot_of, sizeof(int) * N, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h_free.data(), c->d_free, sizeof(int) * cap, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(wd.data(), c->d_wdims, sizeof(int) * wd.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(wf.data(), c->d_wofs, sizeof(long) * wf.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(wt.data(), c->d_weight, sizeof(double) * cap, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ov.data(), c->d_overlap, sizeof(double) * cap, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(eh.data(), c->d_ehist, sizeof(double) * cap, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&mt, c->d_mt, sizeof mt, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&sd, c->d_sd, sizeof sd, cudaMemcpyDeviceToHost));
+  double *snap = nullptr;
+  if (dalloc(&snap, (size_t)k * c->wstride)) return MPSQMC_E_CUDA;
+  for (int w = 0; w < k; ++w)
+    CK(cudaMemcpyAsync(snap + (size_t)w * c->wstride, c->d_walkers + (size_t)slots[w] * c->wstride,
+                       sizeof(double) * c->wstride, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const int keep_sweep = c->sweep, keep_ws = c->global_work ? MPSQMC_WORKSPACE_GLOBAL : MPSQMC_WORKSPACE_AUTO;
+  const int keep_nd = c->Ndesired, keep_step = c->step_count;
+  const unsigned long long keep_draws = c->draws;
+  const bool keep_trace = c->trace_on;
+  auto restore = [&](int n_walkers) -> int {
+    for (int w = 0; w < k; ++w)
+      CK(cudaMemcpyAsync(c->d_walkers + (size_t)slots[w] * c->wstride, snap + (size_t)w * c->wstride,
+                         sizeof(double) * c->wstride, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_slot_of, slots.data(), sizeof(int) * N, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_free, h_free.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_wdims, wd.data(), sizeof(int) * wd.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_wofs, wf.data(), sizeof(long) * wf.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_weight, wt.data(), sizeof(double) * cap, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_overlap, ov.data(), sizeof(double) * cap, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_ehist, eh.data(), sizeof(double) * cap, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_mt, &mt, sizeof mt, cudaMemcpyHostToDevice, c->stream));
+    mq::StepDev s2 = sd;
+    s2.n_cur = n_walkers;
+    CK(cudaMemcpyAsync(c->d_sd, &s2, sizeof s2, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_ncur, &n_walkers, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->n_cur = n_walkers;
+    c->step_count = keep_step;
+    c->draws = keep_draws;
+    return 0;
+  };
+  c->trace_on = false;
+  c->Ndesired = k;  // population control sized for the measured subset
+  double best = 1e300;
+  std::pair<int, int> choice = {keep_sweep, keep_ws};
+  int rc = 0;
+  for (const auto &cd : cands) {
+    rc = mpsqmc_set_option(c, MPSQMC_OPT_SWEEP, cd.first);
+    if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_WORKSPACE, cd.second);
+    if (!rc) rc = restore(k);
+    if (!rc) rc = mpsqmc_walk(c, 1, nullptr);  // warm-up (graph capture)
+    if (!rc) rc = restore(k);
+    if (!rc) rc = mpsqmc_walk(c, steps, nullptr);
+    if (rc) break;
+    const double per = c->last_kernel_ms / ((double)k * steps);
+    if (per < best) {
+      best = per;
+      choice = cd;
+    }
+  }
+  c->Ndesired = keep_nd;
+  c->trace_on = keep_trace;
+  const int rr = restore(N);
+  cudaFree(snap);
+  if (rc) return rc;
+  if (rr) return rr;
+  if (c->graph_exec) {  // captured with the subset's population size
+    cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+  }
+  rc = mpsqmc_set_option(c, MPSQMC_OPT_SWEEP, choice.first);
+  if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_WORKSPACE, choice.second);
+  if (rc) return rc;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    g_tuned[key] = choice;
+  }
+  if (best_sweep) *best_sweep = choice.first;
+  if (best_workspace) *best_workspace = choice.second;
   return 0;
 }
 

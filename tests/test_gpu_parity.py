@@ -156,3 +156,29 @@ def test_nearest_neighbour_sweep_refuses_long_couplings():
         eng.set_option(OPT_SWEEP, SWEEP_NEAREST)
     assert ei.value.code == E_UNSUPPORTED
     assert eng.get_option(OPT_SWEEP) == 0
+
+
+def test_autotune_restores_population_and_keeps_trajectory():
+    """mpsqmc_autotune measures the kernel choices on a copy of the population's state: after it,
+    walkers, weights, overlaps, random stream and step count are as before, and the walk follows
+    the reference trajectory."""
+    from mpsqmc_b200.capi import OPT_SWEEP, OPT_WORKSPACE
+    z = load_golden("walk_L10D8_DW2_branch")
+    meta = z["meta"]
+    eng = engine_for(z)
+    before = eng.get_walkers()
+    d0 = eng.rng_draws()
+    sweep, ws = eng.autotune(steps=2)
+    assert eng.get_option(OPT_SWEEP) == sweep and eng.get_option(OPT_WORKSPACE) == ws
+    after = eng.get_walkers()
+    for a, b in zip(before, after):
+        np.testing.assert_array_equal(a, b)
+    assert eng.rng_draws() == d0
+    for s in range(1, meta["steps"] + 1):
+        st = eng.walk(1)[0]
+        assert st["step"] == s
+        assert st["E_P"] == pytest.approx(z["stat_EP"][s - 1], rel=RTOL)
+        np.testing.assert_array_equal(eng.last_step_walkers()["parent"], z[f"step{s:03d}_parent"])
+    # the choice is remembered for the same shape
+    eng2 = engine_for(z)
+    assert eng2.autotune(steps=2) == (sweep, ws)
