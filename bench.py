@@ -48,7 +48,53 @@ def parse():
                          "throughput (blocking error of the mixed energy; first 20%% discarded)")
     ap.add_argument("--workspace", default="auto", choices=["auto", "global"],
                     help="matrix work buffers: shared memory when they fit (auto) or global scratch")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3", "tf32"],
+                    help="walker-step contractions: FP64 tensor cores, or FP32 buffers on TF32 tensor cores "
+                         "(three passes / one pass); weights, overlaps, energies stay FP64")
+    ap.add_argument("--proposal", default="grid", choices=["grid", "learned"],
+                    help="auxiliary-field proposal: the exact grid PDF, or the learned network (trained online "
+                         "on the grid walk for --train-steps steps first; exact-ratio reweighting)")
+    ap.add_argument("--train-steps", type=int, default=30)
+    ap.add_argument("--canon", type=int, default=None, metavar="K",
+                    help="QR-free sweep, left-normalise every K steps (0: Householder QR per site; "
+                         "default: the engine's, 8)")
+    ap.add_argument("--vn-compare", type=int, default=0, metavar="STEPS",
+                    help="VN of this configuration and of the plain FP64 grid walk (same workload, start "
+                         "and random stream), STEPS steps each after the timed ones; reports their ratio")
     return ap.parse_args()
+
+
+PRECISIONS = {"fp64": 0, "tf32": 1, "tf32x3": 2}
+
+
+def configure(eng, args, sweep, plain=False):
+    """Kernel and method options of a bench engine; plain: the FP64 grid walk (the VN yardstick)."""
+    from mpsqmc_b200.capi import (OPT_CANONICAL_INTERVAL, OPT_PRECISION, OPT_SWEEP, OPT_WORKSPACE,
+                                  WORKSPACE_GLOBAL)
+    eng.set_option(OPT_SWEEP, sweep)
+    if args.workspace == "global":
+        eng.set_option(OPT_WORKSPACE, WORKSPACE_GLOBAL)
+    if args.canon is not None:
+        eng.set_option(OPT_CANONICAL_INTERVAL, args.canon)
+    if not plain:
+        eng.set_option(OPT_PRECISION, PRECISIONS[args.precision])
+
+
+def train_proposal(eng, args):
+    """Online training of the learned proposal on the grid walk (untimed set-up); then the walk
+    samples from it.  Returns what the training did."""
+    from mpsqmc_b200.capi import OPT_PROPOSAL, OPT_PROPOSAL_TRAINING, PROPOSAL_LEARNED
+    if args.proposal != "learned":
+        return None
+    eng.set_option(OPT_PROPOSAL_TRAINING, 1)
+    t0 = time.perf_counter()
+    st = eng.walk(args.train_steps)
+    dt = time.perf_counter() - t0
+    ps = eng.proposal_stats()
+    eng.set_option(OPT_PROPOSAL_TRAINING, 0)
+    eng.set_option(OPT_PROPOSAL, PROPOSAL_LEARNED)
+    return {"steps": args.train_steps, "pairs": int(sum(s["n_walkers"] for s in st)), "adam_steps": ps["updates"],
+            "final_kl": ps["loss"], "seconds": dt}
 
 
 def dist_setup(n):
@@ -144,6 +190,30 @@ def fp64_peak_tflops():
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def tf32_peak_tflops():
+    """cuBLAS FP32 GEMM 8192^3 with TF32 tensor cores allowed, best of 5 (CUDA events): the
+    denominator of the mixed-precision sweep."""
+    import torch
+    keep = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    c = a @ b
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    torch.backends.cuda.matmul.allow_tf32 = keep
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
 def reference_cpu(wl, sample_walkers=None, steps=1, threads=None):
     """The reference's own classes (oracle/_ref/ref_harness, built from the reference sources) timed on
     this host: propagation of `sample_walkers` walkers for `steps` steps, energy excluded (the
@@ -207,7 +277,8 @@ def main():
                            f"D_T shape, walkers = trial compressed on the device",
                "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.Ds, "dtau": wl.dtau,
                "parallelism": f"replicas x{world}", "sweep": args.sweep,
-               "workspace": args.workspace}
+               "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
+               "canonical_interval": args.canon if args.canon is not None else 8}
     else:
         wl = workloads.chain64(Nw=args.walkers or 2048)
         cfg = {"workload": f"{wl.name}: L={wl.L} Heisenberg chain, D_T={wl.DT}, D_W={wl.DW}, {wl.Nw} walkers/GPU, "
@@ -215,7 +286,8 @@ def main():
                "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.DW, "dtau": wl.dtau,
                "l2": f"population ({wl.Nw * wl.walker.data.size * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
                "parallelism": f"replicas x{world}", "sweep": args.sweep,
-               "workspace": args.workspace}
+               "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
+               "canonical_interval": args.canon if args.canon is not None else 8}
 
     if args.impl == "reference":
         if rank != 0:
@@ -248,7 +320,6 @@ def main():
     torch.cuda.set_device(local)
     from mpsqmc_b200 import Engine
 
-    from mpsqmc_b200.capi import OPT_SWEEP
     sweep = {"auto": 0, "nearest": 1, "general": 2}[args.sweep]
     if lattice:
         eng, inputs = lattice_engine(wl, local)
@@ -262,11 +333,9 @@ def main():
         eng = Engine(device=local, **inputs)
         N = walkers.shape[0]
         eng.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
-    eng.set_option(OPT_SWEEP, sweep)
-    if args.workspace == "global":
-        from mpsqmc_b200.capi import OPT_WORKSPACE, WORKSPACE_GLOBAL
-        eng.set_option(OPT_WORKSPACE, WORKSPACE_GLOBAL)
+    configure(eng, args, sweep)
     eng.set_rng(wl.seed + 7919 * rank, 0)
+    training = train_proposal(eng, args)
     eng.walk(args.warmup)
     torch.cuda.synchronize()
     if pg is not None:
@@ -284,17 +353,43 @@ def main():
     value = ws_all / (t_ms * 1e-3)
 
     vn = None
-    if args.vn > 0:
+    vn_steps = max(args.vn, args.vn_compare)
+    if vn_steps > 0:
         from mpsqmc_b200 import analysis
-        more = eng.walk(args.vn)
-        vn = analysis.variance_normalised(value / max(world, 1), [x["E_P"] for x in more],
-                                          [x["n_walkers"] for x in more])
-        vn["throughput_per_gpu"] = value / max(world, 1)
+        e_ref = None
         if not lattice:
             e_ref = float(np.load(os.path.join(ROOT, "mpsqmc_b200", "data", "trial_L64D64.npz"))["energy"])
-            vn["E_ref"] = e_ref
-            vn["E_ref_source"] = "DMRG D=64 energy of the trial (mpsqmc_b200/data)"
-            vn["abs_err_per_site"] = abs(vn["E_mean"] - e_ref) / wl.L
+
+        def vn_of(e, throughput):
+            more = e.walk(vn_steps)
+            r = analysis.variance_normalised(throughput, [x["E_P"] for x in more], [x["n_walkers"] for x in more])
+            r["throughput_per_gpu"] = throughput
+            if e_ref is not None:
+                r["E_ref"] = e_ref
+                r["E_ref_source"] = "DMRG D=64 energy of the trial (mpsqmc_b200/data)"
+                r["abs_err_per_site"] = abs(r["E_mean"] - e_ref) / wl.L
+            return r
+
+        vn = vn_of(eng, value / max(world, 1))
+        vn["arm"] = f"{args.precision}/{args.proposal}"
+        if args.vn_compare > 0:
+            # the yardstick: plain FP64 grid walk from the same start and random stream
+            if lattice:
+                ep, _ = lattice_engine(wl, local)
+            else:
+                ep = Engine(device=local, **inputs)
+                ep.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
+            configure(ep, args, sweep, plain=True)
+            ep.set_rng(wl.seed + 7919 * rank, 0)
+            ep.walk(args.warmup + (args.train_steps if training else 0))
+            sp = ep.walk(args.steps)
+            tp = ep.last_timing()
+            thr = sum(x["n_walkers"] for x in sp) / (tp["total_ms"] * 1e-3)
+            plain_vn = vn_of(ep, thr)
+            ep.close()
+            vn = {"this": vn, "plain_fp64_grid": plain_vn,
+                  "vn_ratio_vs_plain_fp64": vn["vn"] / plain_vn["vn"] if plain_vn["vn"] else None,
+                  "throughput_ratio_vs_plain_fp64": vn["throughput_per_gpu"] / thr}
 
     # roofline of the dominant kernel (the walker-step kernel): canonical FP64 work / kernel time,
     # averaged over the walkers' own bond dims
@@ -304,14 +399,19 @@ def main():
     flops_ws = float(sum(c * workloads.algorithmic_flops_per_walker_step(inputs["trial_dims"], r, cpl)
                          for r, c in zip(rows, counts)) / counts.sum())
     achieved = flops_ws * ws_done / (k_ms * 1e-3) / 1e12
-    peak = fp64_peak_tflops() if rank == 0 else None
+    mixed = args.precision != "fp64"
+    peak = (tf32_peak_tflops() if mixed else fp64_peak_tflops()) if rank == 0 else None
 
     # end to end through the public API: host population -> device, K steps (stats read back each
     # step), population -> host; host wall clock.
     e2e = None
     if not args.no_e2e:
         eng2 = Engine(device=local, **inputs)
-        eng2.set_option(OPT_SWEEP, sweep)
+        configure(eng2, args, sweep)
+        if training:  # the trained network, as the timed engine walks with it
+            from mpsqmc_b200.capi import OPT_PROPOSAL, PROPOSAL_LEARNED
+            eng2.proposal_params(eng.proposal_params())
+            eng2.set_option(OPT_PROPOSAL, PROPOSAL_LEARNED)
         # the population in pinned host memory (both directions), as a serving caller would keep it
         host_w = torch.empty(walkers.shape, dtype=torch.float64, pin_memory=True).numpy()
         host_w[:] = walkers
@@ -339,24 +439,28 @@ def main():
 
     if rank == 0:
         prof_traffic = None
-        kname = "walker_step_kernel" if args.sweep == "nearest" else "walker_step_general_kernel"
+        kname = "walker_step_kernel" if args.sweep == "nearest" else (
+            "walker_step_mixed_kernel" if mixed else "walker_step_general_kernel")
         tp = os.path.join(ROOT, "profiles", f"{kname}_traffic.json")
         if os.path.exists(tp) and not lattice and N == 2048:
             prof_traffic = json.load(open(tp)).get("bytes_per_launch")
         line = {
             "metric": METRIC, "value": value, "unit": "walker-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "vs_baseline": None, "dtype": "f64" if not mixed else f"{args.precision}+f64", "data": "synthetic",
+            "config": cfg,
             "energy": {"E_P_last": stats[-1]["E_P"], "E_T_last": stats[-1]["E_T"], "walkers_last": stats[-1]["n_after"]},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": prof_traffic,
-                         "kernel": "walker_step_kernel" if args.sweep == "nearest" else "walker_step_general_kernel",
-                         "flops_per_walker_step": flops_ws,
-                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor path)"},
+                         "kernel": kname, "flops_per_walker_step": flops_ws,
+                         "peak_source": ("cuBLAS TF32 GEMM 8192^3 measured in this run (TF32 tensor path; the "
+                                         "canonical flops count each product once)") if mixed else
+                                        "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor path)"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": tim["launches"],
             **({"variance_normalised": vn} if vn is not None else {}),
+            **({"proposal_training": training} if training else {}),
             "clocks": clk.summary(),
         }
         print(json.dumps(line))

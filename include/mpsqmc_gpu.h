@@ -192,8 +192,59 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
                                        * weight 1); the trace then holds [N][3] = PDF norm, uniform,
                                        * picked term (0 = identity).  The population-control options
                                        * above do not apply. */
+#define MPSQMC_OPT_CANONICAL_INTERVAL 6 /* K >= 1 (default 8): the general sweep stores each site
+                                         * as it leaves the centre, without the per-site
+                                         * Householder QR (the norm comes from a left norm
+                                         * environment), and restores the left-canonical form of
+                                         * Walker::setOverlap on every K-th step; 0: one QR per
+                                         * site, the state the reference's per-coupling setOverlap
+                                         * leaves.  Same walk (every quantity it uses is gauge
+                                         * invariant).  mpsqmc_get_walkers and
+                                         * mpsqmc_compress_walkers left-normalise first when the
+                                         * last step did not.  Applies to the Trotter projector's
+                                         * general sweep; with h != 0 the walkers are
+                                         * left-normalised every step anyway. */
+#define MPSQMC_OPT_PRECISION 7       /* arithmetic of the walker-step contractions (the set_precision
+                                      * of the C ABI the north star lists): */
+#define MPSQMC_PRECISION_FP64 0      /*   FP64 tensor cores (DMMA), the reference's arithmetic (default) */
+#define MPSQMC_PRECISION_TF32 1      /*   FP32 work buffers, one TF32 tensor-core pass per product */
+#define MPSQMC_PRECISION_TF32X3 2    /*   FP32 work buffers, three TF32 passes (head/tail split):
+                                      *   about FP32 accuracy.  Both mixed modes keep the walkers,
+                                      *   closures, PDF, sampling, weights, overlaps, norms, energies
+                                      *   and population control in FP64, run the QR-free sweep
+                                      *   (left-normalising in FP64 every MPSQMC_OPT_CANONICAL_INTERVAL
+                                      *   steps, 4 when that option is 0) and apply to the general
+                                      *   sweep of the Trotter projector; the per-coupling trace is
+                                      *   FP64-only (MPSQMC_E_UNSUPPORTED). */
+#define MPSQMC_OPT_PROPOSAL 8        /* how a coupling's grid point is drawn (the set_proposal of the
+                                      * north star's C ABI): */
+#define MPSQMC_PROPOSAL_GRID 0       /*   the exact grid PDF, as MPSQMC2.cpp:551-588 (default) */
+#define MPSQMC_PROPOSAL_LEARNED 1    /*   the learned proposal q: the point is drawn from q restricted
+                                      *   to the PDF's support and the weight takes P(x) / q(x)
+                                      *   (exact-ratio reweighting; unbiased).  The grid PDF is the
+                                      *   zero-variance choice for one coupling, so q can at best
+                                      *   match it; Trotter projector, grids of up to 256 points */
+#define MPSQMC_OPT_PROPOSAL_TRAINING 9 /* 1: every grid step also stores (features, exact PDF) of one
+                                        * coupling per walker and takes one Adam step (step size
+                                        * 1e-3) of the network on them (mean KL(P || q)) */
 int mpsqmc_set_option(mpsqmc_ctx *ctx, int option, long value);
 int mpsqmc_get_option(mpsqmc_ctx *ctx, int option, long *value);
+
+/* Learned proposal (no counterpart in the reference).  The network maps 32 features of a
+ * coupling (4 C_kl / ov and 4 M / ov: the overlap-ratio coefficients and the 16 closures of the
+ * environment branches) through two hidden layers of 128 (ReLU) to logits over the G grid points.
+ * Parameters: one FP32 vector of n = 32*128 + 128 + 128*128 + 128 + 128*G + G, W input-major
+ * (W1[i*128 + o], then b1, W2, b2, W3[i*G + o], b3); the sweep reads a BF16 copy.
+ *   mpsqmc_proposal_params: copies the parameters out (out != NULL) and/or in (in != NULL; resets
+ *     the Adam state); *n_params receives n.  Parameters are created on first use (He-uniform,
+ *     fixed seed).
+ *   mpsqmc_proposal_loss_grad: mean KL(p || softmax(z)) over a batch of B <= capacity pairs
+ *     (features [B][32], targets [B][G], each target a normalised PDF) and its gradient [n].
+ *   mpsqmc_proposal_stats: the loss of the last training step and the number of Adam steps. */
+int mpsqmc_proposal_params(mpsqmc_ctx *ctx, float *out, const float *in, long *n_params);
+int mpsqmc_proposal_loss_grad(mpsqmc_ctx *ctx, int B, const float *features, const float *targets,
+                              double *loss, float *grad);
+int mpsqmc_proposal_stats(mpsqmc_ctx *ctx, double *last_loss, int *updates);
 
 /* Autotuner (no counterpart in the reference): times `steps` steps of every applicable
  * (MPSQMC_OPT_SWEEP, MPSQMC_OPT_WORKSPACE) choice on the first walkers of the current population

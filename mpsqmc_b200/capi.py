@@ -24,6 +24,12 @@ OPT_RESAMPLING = 4
 RESAMPLE_THRESHOLD, RESAMPLE_COMB = 0, 1
 OPT_PROJECTOR = 5
 PROJECTOR_TROTTER, PROJECTOR_MPO_TERMS = 0, 1
+OPT_CANONICAL_INTERVAL = 6
+OPT_PRECISION = 7
+PRECISION_FP64, PRECISION_TF32, PRECISION_TF32X3 = 0, 1, 2
+OPT_PROPOSAL = 8
+PROPOSAL_GRID, PROPOSAL_LEARNED = 0, 1
+OPT_PROPOSAL_TRAINING = 9
 
 # Every symbol include/mpsqmc_gpu.h declares.
 EXPORTED = [
@@ -32,7 +38,8 @@ EXPORTED = [
     "mpsqmc_energy", "mpsqmc_walk", "mpsqmc_last_step_walkers", "mpsqmc_set_trace",
     "mpsqmc_get_trace", "mpsqmc_last_timing", "mpsqmc_local_energy_noalloc", "mpsqmc_set_step",
     "mpsqmc_set_option", "mpsqmc_get_option", "mpsqmc_set_walkers_dims", "mpsqmc_get_walker_dims",
-    "mpsqmc_compress_walkers", "mpsqmc_autotune",
+    "mpsqmc_compress_walkers", "mpsqmc_autotune", "mpsqmc_proposal_params", "mpsqmc_proposal_loss_grad",
+    "mpsqmc_proposal_stats",
 ]
 
 
@@ -94,6 +101,7 @@ def load(build_if_missing: bool = True):
     P = C.c_void_p
     dp = C.POINTER(C.c_double)
     ip = C.POINTER(C.c_int)
+    fp = C.POINTER(C.c_float)
     sig = {
         "mpsqmc_create": (C.c_int, [C.POINTER(Config), C.POINTER(P)]),
         "mpsqmc_destroy": (C.c_int, [P]),
@@ -119,6 +127,9 @@ def load(build_if_missing: bool = True):
         "mpsqmc_get_option": (C.c_int, [P, C.c_int, C.POINTER(C.c_long)]),
         "mpsqmc_local_energy_noalloc": (C.c_int, [C.POINTER(EnergyLayout), P, P, C.c_long, P, C.c_int, P,
                                                   C.c_int, P]),
+        "mpsqmc_proposal_params": (C.c_int, [P, fp, fp, C.POINTER(C.c_long)]),
+        "mpsqmc_proposal_loss_grad": (C.c_int, [P, C.c_int, fp, fp, dp, fp]),
+        "mpsqmc_proposal_stats": (C.c_int, [P, dp, ip]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -130,6 +141,10 @@ def load(build_if_missing: bool = True):
 
 def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
 
 
 def _ip(a):
@@ -293,6 +308,31 @@ class Engine:
         k, t, n = C.c_double(0), C.c_double(0), C.c_int(0)
         check(self.lib.mpsqmc_last_timing(self._ctx, C.byref(k), C.byref(t), C.byref(n)))
         return dict(step_kernel_ms=k.value, total_ms=t.value, launches=n.value)
+
+    # learned proposal
+    def proposal_params(self, new=None):
+        """The network's FP32 parameter vector; with `new`, replaces it (and resets Adam)."""
+        n = C.c_long(0)
+        check(self.lib.mpsqmc_proposal_params(self._ctx, None, None, C.byref(n)))
+        out = np.zeros(n.value, dtype=np.float32)
+        src = None if new is None else np.ascontiguousarray(new, dtype=np.float32)
+        check(self.lib.mpsqmc_proposal_params(self._ctx, _fp(out), _fp(src), None))
+        return out
+
+    def proposal_loss_grad(self, features, targets):
+        X = np.ascontiguousarray(features, dtype=np.float32)
+        Pt = np.ascontiguousarray(targets, dtype=np.float32)
+        n = C.c_long(0)
+        check(self.lib.mpsqmc_proposal_params(self._ctx, None, None, C.byref(n)))
+        grad = np.zeros(n.value, dtype=np.float32)
+        loss = C.c_double(0)
+        check(self.lib.mpsqmc_proposal_loss_grad(self._ctx, X.shape[0], _fp(X), _fp(Pt), C.byref(loss), _fp(grad)))
+        return loss.value, grad
+
+    def proposal_stats(self):
+        loss, upd = C.c_double(0), C.c_int(0)
+        check(self.lib.mpsqmc_proposal_stats(self._ctx, C.byref(loss), C.byref(upd)))
+        return dict(loss=loss.value, updates=upd.value)
 
 
 def local_energy_noalloc(*, L, trial_dims, walker_dims, ci, cj, cJ, h, trial_ptr, walkers_ptr, walker_stride,

@@ -23,6 +23,7 @@
 #include "walker_general.cuh"
 #include "compress.cuh"
 #include "legacy.cuh"
+#include "proposal.cuh"
 
 namespace {
 
@@ -97,6 +98,22 @@ struct mpsqmc_ctx {
   int maxA = 1, maxB = 1, pa = 4, pb = 4, pq = 4;
   size_t smem_bytes = 0;
   int sm_count = 1, max_ctas = 1;
+  // mixed-precision sweep (FP32 work buffers, TF32 tensor cores): its own shared memory and grid
+  int precision = MPSQMC_PRECISION_FP64;
+  size_t smem_bytes_mixed = 0;
+  int max_ctas_mixed = 1;
+  float *d_trial32 = nullptr;
+  // learned proposal: FP32 master parameters, Adam moments, gradient, BF16 copy, training pairs
+  // and activations (allocated on first use)
+  int proposal = MPSQMC_PROPOSAL_GRID;
+  bool prop_train = false;
+  long nparams = 0;
+  float *d_pw = nullptr, *d_pm = nullptr, *d_pv = nullptr, *d_pg = nullptr;
+  __nv_bfloat16 *d_pwb = nullptr;
+  int *d_pt = nullptr, *d_pb = nullptr;
+  double *d_ploss = nullptr;
+  float *d_pfeat = nullptr, *d_ptarget = nullptr, *d_ph1 = nullptr, *d_ph2 = nullptr, *d_pz = nullptr,
+        *d_pdz = nullptr, *d_pdh2 = nullptr, *d_pdh1 = nullptr;
   // device memory
   int *d_aT = nullptr, *d_bW = nullptr;
   long *d_toff = nullptr, *d_woff = nullptr, *d_roff = nullptr, *d_nroff = nullptr;
@@ -112,6 +129,9 @@ struct mpsqmc_ctx {
   int workspace = MPSQMC_WORKSPACE_AUTO;
   int pc_interval = 1;                  // population control every pc_interval steps
   int resample = MPSQMC_RESAMPLE_THRESHOLD;
+  int canon_interval = 8;               // QR-free general sweep, LeftNormalize every K steps (0: off)
+  bool gauge_dirty = false;             // the last step left the walkers un-normalised (QR-free)
+  long nloff = 0;                       // its left norm environment inside a CTA's scratch
   int *d_ncop = nullptr;                // copies per walker in the branching step
   int *d_wdims = nullptr;               // per slot: the walker's bond dims [capacity][L+1]
   long *d_wofs = nullptr;               // per slot: its site offsets [capacity][L]
@@ -147,12 +167,18 @@ struct mpsqmc_ctx {
   // one timestep captured as a CUDA graph (re-captured when the trace setting changes)
   bool use_graph = true;
   cudaGraphExec_t graph_exec = nullptr;
+  cudaGraphExec_t graph_exec_canon = nullptr;  // QR-free sweep: the step that also left-normalises
+  int graph_launches[2] = {0, 0};
   bool graph_trace = false;
   mq::StepDev *h_sd = nullptr;  // pinned copies read back after every step
   int *h_err = nullptr;
 };
 
 namespace {
+
+bool general_sweep(const mpsqmc_ctx *c);
+bool qr_free(const mpsqmc_ctx *c);
+bool mixed(const mpsqmc_ctx *c);
 
 mq::Dev make_dev(mpsqmc_ctx *c) {
   mq::Dev p;
@@ -172,6 +198,7 @@ mq::Dev make_dev(mpsqmc_ctx *c) {
   p.toff = c->d_toff;
   p.woff = c->d_woff;
   p.trial = c->d_trial;
+  p.trial32 = c->d_trial32;
   p.wstride = c->wstride;
   p.walkers = c->d_walkers;
   p.slot_of = c->d_slot_of;
@@ -218,12 +245,48 @@ mq::Dev make_dev(mpsqmc_ctx *c) {
   p.wdims = c->d_wdims;
   p.wofs = c->d_wofs;
   p.ctr = c->d_ctr;
+  p.nloff = qr_free(c) ? c->nloff : -1;
+  const bool trotter = c->projector == MPSQMC_PROJECTOR_TROTTER;
+  p.prop_mode = (c->proposal == MPSQMC_PROPOSAL_LEARNED && trotter && c->d_pwb) ? 1 : 0;
+  p.prop_collect = (c->prop_train && c->proposal == MPSQMC_PROPOSAL_GRID && trotter && c->d_pwb) ? 1 : 0;
+  p.prop_w = c->d_pwb;
+  p.prop_feat = c->d_pfeat;
+  p.prop_target = c->d_ptarget;
   return p;
 }
 
 // The general sweep (walker_general.cuh) runs unless the nearest-neighbour sweep is requested
 // (it needs every coupling to be (i, i+1)); it is the faster of the two on chains as well.
 bool general_sweep(const mpsqmc_ctx *c) { return c->sweep != MPSQMC_SWEEP_NEAREST; }
+
+// The mixed-precision sweep (MPSQMC_OPT_PRECISION, general sweep of the Trotter projector).
+bool mixed(const mpsqmc_ctx *c) {
+  return c->precision != MPSQMC_PRECISION_FP64 && general_sweep(c) && c->projector == MPSQMC_PROJECTOR_TROTTER;
+}
+
+// The QR-free variant of the general sweep (MPSQMC_OPT_CANONICAL_INTERVAL > 0, Trotter projector;
+// always for the mixed-precision sweep).
+bool qr_free(const mpsqmc_ctx *c) {
+  return (c->canon_interval > 0 || mixed(c)) && general_sweep(c) && c->projector == MPSQMC_PROJECTOR_TROTTER;
+}
+
+// Steps between two left-normalisations of the QR-free sweep.
+constexpr int kMixedCanonInterval = 4;  // default of the mixed-precision sweep
+int canon_every(const mpsqmc_ctx *c) { return c->canon_interval > 0 ? c->canon_interval : kMixedCanonInterval; }
+
+// Doubles of per-CTA scratch for the largest grid of any walker kernel (the mixed sweep reads a
+// CTA's scratch as floats with the same stride).
+size_t scratch_doubles(const mpsqmc_ctx *c) {
+  return std::max((size_t)c->max_ctas * c->scr_stride, ((size_t)c->max_ctas_mixed * c->scr_stride + 1) / 2);
+}
+
+void drop_graphs(mpsqmc_ctx *c) {
+  for (cudaGraphExec_t *g : {&c->graph_exec, &c->graph_exec_canon})
+    if (*g) {
+      cudaGraphExecDestroy(*g);
+      *g = nullptr;
+    }
+}
 
 int grid_for(const mpsqmc_ctx *c, int n) { return std::max(1, std::min(n, c->max_ctas)); }
 
@@ -238,7 +301,8 @@ int check_err(mpsqmc_ctx *c) {
 }
 
 void free_all(mpsqmc_ctx *c) {
-  void *ptrs[] = {c->d_aT, c->d_bW, c->d_toff, c->d_woff, c->d_roff, c->d_nroff, c->d_trial, c->d_walkers,
+  void *ptrs[] = {c->d_pw, c->d_pm, c->d_pv, c->d_pg, c->d_pwb, c->d_pt, c->d_pb, c->d_ploss, c->d_pfeat,
+                  c->d_ptarget, c->d_ph1, c->d_ph2, c->d_pz, c->d_pdz, c->d_pdh2, c->d_pdh1, c->d_trial32, c->d_aT, c->d_bW, c->d_toff, c->d_woff, c->d_roff, c->d_nroff, c->d_trial, c->d_walkers,
                   c->d_slot_of, c->d_slot_new, c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
                   c->d_flag_pos, c->d_ncur, c->d_weight, c->d_overlap, c->d_ehist, c->d_energy,
                   c->d_ovout, c->d_wtout, c->d_sw, c->d_uni, c->d_ubr, c->d_bond_c, c->d_bond_j,
@@ -249,7 +313,7 @@ void free_all(mpsqmc_ctx *c) {
                   c->d_term_site, c->d_term_op, c->d_changed, c->d_term_pref};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  drop_graphs(c);
   if (c->h_sd) cudaFreeHost(c->h_sd);
   if (c->h_err) cudaFreeHost(c->h_err);
   for (auto &e : c->ev)
@@ -281,6 +345,19 @@ int layout_workspace(mpsqmc_ctx *c, bool force_global) {
   int occ = 1;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mq::walker_step_kernel, mq::kThreads, c->smem_bytes));
   c->max_ctas = std::max(1, occ) * c->sm_count;
+  // mixed-precision sweep: FP32 matrix buffers next to the small FP64 ones, on chip unless the
+  // FP64 buffers were placed in global scratch
+  long big_floats = 0;
+  const long mixed_all = mq::smem_bytes_f32(c->L, c->maxA, c->maxB, c->G, c->pa, c->pb, nullptr, nullptr, nullptr,
+                                            &big_floats);
+  c->smem_bytes_mixed = global ? (size_t)(mixed_all - (long)sizeof(float) * big_floats) : (size_t)mixed_all;
+  const void *mk[] = {(const void *)mq::walker_step_mixed_kernel<1>, (const void *)mq::walker_step_mixed_kernel<3>};
+  for (const void *k : mk)
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes_mixed));
+  int occm = 1;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occm, mq::walker_step_mixed_kernel<3>, mq::kThreads,
+                                                   c->smem_bytes_mixed));
+  c->max_ctas_mixed = std::max(1, std::min(occm, 2)) * c->sm_count;
   return 0;
 }
 
@@ -460,7 +537,8 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   c->foff = ro;
   c->choff = ro + 2L * 4 * c->maxA * c->maxB;
   c->loff = c->choff + (2L + 3L * nslots) * c->maxA * c->maxB;
-  c->scr_base = c->loff + ((2L * (3L * c->nC + L + 1) + 31) & ~31L);
+  c->nloff = c->loff + ((2L * (3L * c->nC + L + 1) + 31) & ~31L);
+  c->scr_base = c->nloff + (((long)c->pb * c->maxB + 31) & ~31L);
   for (int s = 0; s < 2; ++s)
     for (int t = 0; t < 2; ++t) {
       c->opSx[s + 2 * t] = op_sx(d, s, t);
@@ -500,7 +578,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
         dalloc(&c->d_bond_j, L - 1) | dalloc(&c->d_bondJ, L - 1) | dalloc(&c->d_tabU, 16 * c->nJ) |
         dalloc(&c->d_tabS, 4 * c->nJ) | dalloc(&c->d_tabVT, 16 * c->nJ) | dalloc(&c->d_grid, 4 * c->G) |
         dalloc(&c->d_tabSq, 4 * c->nJ) |
-        dalloc(&c->d_scratch, (size_t)c->max_ctas * c->scr_stride) | dalloc(&c->d_err, 1) |
+        dalloc(&c->d_scratch, scratch_doubles(c)) | dalloc(&c->d_err, 1) | dalloc(&c->d_trial32, to) |
         dalloc(&c->d_mt, 1) | dalloc(&c->d_sd, 1) | dalloc(&c->d_cp_j, c->nC) | dalloc(&c->d_cp_q, c->nC) |
         dalloc(&c->d_site_c0, L + 1) | dalloc(&c->d_ech_off, L + 1) | dalloc(&c->d_ech_slot, ech_slot.size()) |
         dalloc(&c->d_ech_cont, ech_cont.size()) | dalloc(&c->d_eopen, L) | dalloc(&c->d_ech_J, ech_J.size()) |
@@ -512,6 +590,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   if (cudaMallocHost((void **)&c->h_sd, sizeof(mq::StepDev)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_err, sizeof(int)) != cudaSuccess)
     return bail(fail(MPSQMC_E_CUDA, "pinned host buffers"));
+  std::vector<float> trial32(cfg->trial, cfg->trial + to);
   std::vector<double> sqS(4 * c->nJ);
   for (int q = 0; q < 4 * c->nJ; ++q) sqS[q] = std::sqrt(cfg->S[q]);
   auto up = [&](void *dst, const void *src, size_t bytes) {
@@ -521,7 +600,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
             up(c->d_toff, c->toff.data(), sizeof(long) * L) && up(c->d_woff, c->woff.data(), sizeof(long) * L) &&
             up(c->d_roff, c->roff.data(), sizeof(long) * (L + 1)) &&
             up(c->d_nroff, c->nroff.data(), sizeof(long) * (L + 1)) &&
-            up(c->d_trial, cfg->trial, sizeof(double) * to) &&
+            up(c->d_trial, cfg->trial, sizeof(double) * to) && up(c->d_trial32, trial32.data(), sizeof(float) * to) &&
             up(c->d_bond_c, bond_c.data(), sizeof(int) * (L - 1)) &&
             up(c->d_bond_j, bond_j.data(), sizeof(int) * (L - 1)) &&
             up(c->d_bondJ, bondJ.data(), sizeof(double) * (L - 1)) &&
@@ -659,6 +738,7 @@ static int set_walkers_impl(mpsqmc_ctx *c, int N, const int *dims, const double 
   CK(cudaMemcpyAsync(c->d_ncur, &N, sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
   c->n_cur = N;
+  c->gauge_dirty = false;
   if (normalize) {
     mq::Dev p = make_dev(c);
     CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(int) * mq::kNumCtr, c->stream));
@@ -666,6 +746,21 @@ static int set_walkers_impl(mpsqmc_ctx *c, int N, const int *dims, const double 
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(c->stream));
+  return check_err(c);
+}
+
+// Walkers left by a QR-free step are not left-canonical: set_overlap_kernel restores
+// Walker::setOverlap's state (same quantum state, overlap recomputed) before they are read out
+// or compressed.
+static int restore_canonical(mpsqmc_ctx *c) {
+  if (!c->gauge_dirty || c->n_cur < 1) return 0;
+  CK(cudaSetDevice(c->device));
+  mq::Dev p = make_dev(c);
+  CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(int) * mq::kNumCtr, c->stream));
+  mq::set_overlap_kernel<<<grid_for(c, c->n_cur), mq::kThreads, c->smem_bytes, c->stream>>>(p);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  c->gauge_dirty = false;
   return check_err(c);
 }
 
@@ -684,6 +779,10 @@ int mpsqmc_compress_walkers(mpsqmc_ctx *c, const int *target_D, int normalize) {
   if (!c || !target_D) return fail(MPSQMC_E_ARG, "null argument");
   const int n = c->n_cur;
   if (n < 1) return fail(MPSQMC_E_ARG, "no walkers");
+  {
+    const int rc = restore_canonical(c);
+    if (rc) return rc;
+  }
   CK(cudaSetDevice(c->device));
   if (!c->d_cscr) {
     const long q2 = 2L * c->maxB;
@@ -726,6 +825,10 @@ int mpsqmc_get_walker_dims(mpsqmc_ctx *c, int *N, int *dims) {
 int mpsqmc_get_walkers(mpsqmc_ctx *c, int *N, double *walkers, double *weights, double *overlaps,
                        double *ehist) {
   if (!c) return fail(MPSQMC_E_ARG, "null context");
+  if (walkers || overlaps) {
+    const int rc = restore_canonical(c);
+    if (rc) return rc;
+  }
   CK(cudaSetDevice(c->device));
   const int n = c->n_cur;
   if (N) *N = n;
@@ -783,6 +886,90 @@ int mpsqmc_energy(mpsqmc_ctx *c, double *E_P) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Learned proposal (proposal.cuh)
+// ---------------------------------------------------------------------------------------------
+constexpr float kPropLr = 1e-3f;  // Adam step size of the online training
+
+// Parameters and buffers on first use: He-uniform weights (seeded mt19937), zero biases and moments.
+static int prop_alloc(mpsqmc_ctx *c) {
+  if (c->d_pw) return 0;
+  if (c->G > mq::kMlpMaxOut) return fail(MPSQMC_E_UNSUPPORTED, "the learned proposal takes grids of up to 256 points");
+  CK(cudaSetDevice(c->device));
+  const long n = mq::mlp_params(c->G);
+  const size_t cap = c->capacity, G = c->G, H = mq::kMlpHid;
+  if (dalloc(&c->d_pw, n) || dalloc(&c->d_pm, n) || dalloc(&c->d_pv, n) || dalloc(&c->d_pg, n) ||
+      dalloc(&c->d_pwb, n) || dalloc(&c->d_pt, 1) || dalloc(&c->d_pb, 1) || dalloc(&c->d_ploss, 1) ||
+      dalloc(&c->d_pfeat, cap * mq::kMlpIn) || dalloc(&c->d_ptarget, cap * G) || dalloc(&c->d_ph1, cap * H) ||
+      dalloc(&c->d_ph2, cap * H) || dalloc(&c->d_pz, cap * G) || dalloc(&c->d_pdz, cap * G) ||
+      dalloc(&c->d_pdh2, cap * H) || dalloc(&c->d_pdh1, cap * H))
+    return MPSQMC_E_CUDA;
+  c->nparams = n;
+  std::vector<float> w(n, 0.f);
+  std::mt19937 gen(20131015u);
+  const long offs[3] = {0, mq::mlp_off_w2(), mq::mlp_off_w3()};
+  const int fan_in[3] = {mq::kMlpIn, mq::kMlpHid, mq::kMlpHid}, fan_out[3] = {mq::kMlpHid, mq::kMlpHid, c->G};
+  for (int l = 0; l < 3; ++l) {
+    std::uniform_real_distribution<float> u(-std::sqrt(6.f / fan_in[l]), std::sqrt(6.f / fan_in[l]));
+    for (long e = 0; e < (long)fan_in[l] * fan_out[l]; ++e) w[offs[l] + e] = u(gen);
+  }
+  CK(cudaMemcpy(c->d_pw, w.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemset(c->d_pm, 0, sizeof(float) * n));
+  CK(cudaMemset(c->d_pv, 0, sizeof(float) * n));
+  CK(cudaMemset(c->d_pt, 0, sizeof(int)));
+  CK(cudaMemset(c->d_ploss, 0, sizeof(double)));
+  mq::mlp_to_bf16_kernel<<<64, 256, 0, c->stream>>>(n, c->d_pw, c->d_pwb);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+// Forward and backward pass over the pairs in d_pfeat / d_ptarget (batch size *Bdev): mean
+// KL(p || q) into d_ploss, its gradient into d_pg; with update, one Adam step on the parameters
+// (and their BF16 copy).  Adds the number of launches to *n.
+static int enqueue_training(mpsqmc_ctx *c, const int *Bdev, bool update, int *n) {
+  const int cap = c->capacity, G = c->G, H = mq::kMlpHid, I = mq::kMlpIn;
+  float *W1 = c->d_pw, *b1 = c->d_pw + mq::mlp_off_b1(), *W2 = c->d_pw + mq::mlp_off_w2(),
+        *b2 = c->d_pw + mq::mlp_off_b2(), *W3 = c->d_pw + mq::mlp_off_w3(), *b3 = c->d_pw + mq::mlp_off_b3(G);
+  float *gW1 = c->d_pg, *gb1 = c->d_pg + mq::mlp_off_b1(), *gW2 = c->d_pg + mq::mlp_off_w2(),
+        *gb2 = c->d_pg + mq::mlp_off_b2(), *gW3 = c->d_pg + mq::mlp_off_w3(), *gb3 = c->d_pg + mq::mlp_off_b3(G);
+  int k = 0;
+  // M == 0 with md: M is the batch size; K == 0 with kd: K is the batch size
+  auto gemm = [&](int M, int N, int K, const int *md, const int *kd, const float *A, int lda, int ta, const float *B,
+                  int ldb, int tb, float *C, int ldc, const float *bias, int relu) {
+    const dim3 grid((N + 63) / 64, ((md ? cap : M) + 63) / 64);
+    mq::mlp_gemm_kernel<<<grid, 256, 0, c->stream>>>(M, N, K, md, kd, A, lda, ta, B, ldb, tb, C, ldc, bias, relu);
+    ++k;
+  };
+  const int rows_blocks = std::min(1024, (cap * H + 255) / 256);
+  CK(cudaMemsetAsync(c->d_ploss, 0, sizeof(double), c->stream));
+  gemm(0, H, I, Bdev, nullptr, c->d_pfeat, I, 0, W1, H, 0, c->d_ph1, H, b1, 1);
+  gemm(0, H, H, Bdev, nullptr, c->d_ph1, H, 0, W2, H, 0, c->d_ph2, H, b2, 1);
+  gemm(0, G, H, Bdev, nullptr, c->d_ph2, H, 0, W3, G, 0, c->d_pz, G, b3, 0);
+  mq::mlp_softmax_grad_kernel<<<(cap + 7) / 8, 256, 0, c->stream>>>(Bdev, G, c->d_pz, c->d_ptarget, c->d_pdz,
+                                                                     c->d_ploss);
+  gemm(H, G, 0, nullptr, Bdev, c->d_ph2, H, 1, c->d_pdz, G, 0, gW3, G, nullptr, 0);
+  mq::mlp_colsum_kernel<<<(G + 255) / 256, 256, 0, c->stream>>>(Bdev, G, c->d_pdz, gb3);
+  gemm(0, H, G, Bdev, nullptr, c->d_pdz, G, 0, W3, G, 1, c->d_pdh2, H, nullptr, 0);
+  mq::mlp_relu_back_kernel<<<rows_blocks, 256, 0, c->stream>>>(Bdev, H, c->d_ph2, c->d_pdh2);
+  gemm(H, H, 0, nullptr, Bdev, c->d_ph1, H, 1, c->d_pdh2, H, 0, gW2, H, nullptr, 0);
+  mq::mlp_colsum_kernel<<<1, 256, 0, c->stream>>>(Bdev, H, c->d_pdh2, gb2);
+  gemm(0, H, H, Bdev, nullptr, c->d_pdh2, H, 0, W2, H, 1, c->d_pdh1, H, nullptr, 0);
+  mq::mlp_relu_back_kernel<<<rows_blocks, 256, 0, c->stream>>>(Bdev, H, c->d_ph1, c->d_pdh1);
+  gemm(I, H, 0, nullptr, Bdev, c->d_pfeat, I, 1, c->d_pdh1, H, 0, gW1, H, nullptr, 0);
+  mq::mlp_colsum_kernel<<<1, 256, 0, c->stream>>>(Bdev, H, c->d_pdh1, gb1);
+  k += 6;
+  if (update) {
+    mq::mlp_adam_kernel<<<128, 256, 0, c->stream>>>(c->nparams, kPropLr, c->d_pt, c->d_pg, c->d_pw, c->d_pm, c->d_pv,
+                                                    c->d_pwb);
+    mq::mlp_count_kernel<<<1, 1, 0, c->stream>>>(c->d_pt);
+    k += 2;
+  }
+  CK(cudaGetLastError());
+  *n += k;
+  return 0;
+}
+
 // Issue one timestep on c->stream (also used under stream capture): every grid has its fixed
 // maximal size and every kernel reads the current walker count from device memory.
 static int enqueue_legacy_step(mpsqmc_ctx *c, int *launches) {
@@ -825,7 +1012,9 @@ static int enqueue_legacy_step(mpsqmc_ctx *c, int *launches) {
   return 0;
 }
 
-static int enqueue_step(mpsqmc_ctx *c, int *launches) {
+// canon: the QR-free sweep's step that also restores the left-canonical form (LeftNormalize,
+// overlap and sign of Walker::setOverlap) after the couplings.
+static int enqueue_step(mpsqmc_ctx *c, int *launches, bool canon) {
   if (c->projector == MPSQMC_PROJECTOR_MPO_TERMS) return enqueue_legacy_step(c, launches);
   mq::Dev p = make_dev(c);
   const int grid = c->max_ctas;
@@ -841,7 +1030,12 @@ static int enqueue_step(mpsqmc_ctx *c, int *launches) {
   // step kernel inside the graph
   CK(cudaEventRecordWithFlags(c->ev[0], c->stream, cudaEventRecordExternal));
   const bool gen = general_sweep(c);
-  if (gen)
+  if (mixed(c)) {
+    if (c->precision == MPSQMC_PRECISION_TF32)
+      mq::walker_step_mixed_kernel<1><<<c->max_ctas_mixed, mq::kThreads, c->smem_bytes_mixed, c->stream>>>(p);
+    else
+      mq::walker_step_mixed_kernel<3><<<c->max_ctas_mixed, mq::kThreads, c->smem_bytes_mixed, c->stream>>>(p);
+  } else if (gen)
     mq::walker_step_general_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
   else
     mq::walker_step_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
@@ -856,6 +1050,13 @@ static int enqueue_step(mpsqmc_ctx *c, int *launches) {
     else
       mq::energy_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
     n += 3;
+  } else if (canon && qr_free(c)) {
+    mq::set_overlap_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+    n += 1;
+  }
+  if (p.prop_collect) {  // online training of the proposal on this step's pairs
+    const int rc = enqueue_training(c, c->d_ncur, true, &n);
+    if (rc) return rc;
   }
   mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 1, c->d_flag_pos, c->d_sw,
                                               c->pc_interval, c->resample);
@@ -873,21 +1074,22 @@ static int enqueue_step(mpsqmc_ctx *c, int *launches) {
   return 0;
 }
 
-static int build_graph(mpsqmc_ctx *c, int *launches) {
-  if (c->graph_exec) {
-    cudaGraphExecDestroy(c->graph_exec);
-    c->graph_exec = nullptr;
+static int build_graph(mpsqmc_ctx *c, bool canon) {
+  cudaGraphExec_t &ge = canon ? c->graph_exec_canon : c->graph_exec;
+  if (ge) {
+    cudaGraphExecDestroy(ge);
+    ge = nullptr;
   }
   cudaGraph_t g = nullptr;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = enqueue_step(c, launches);
+  int rc = enqueue_step(c, &c->graph_launches[canon ? 1 : 0], canon);
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   if (rc) {
     if (g) cudaGraphDestroy(g);
     return rc;
   }
   if (e != cudaSuccess) return fail(MPSQMC_E_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
-  e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+  e = cudaGraphInstantiate(&ge, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(MPSQMC_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   c->graph_trace = c->trace_on;
@@ -902,23 +1104,26 @@ int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
   if (c->trace_on && !c->d_trace) {
     if (dalloc(&c->d_trace, (size_t)c->capacity * c->nC * mq::kTraceStride)) return MPSQMC_E_CUDA;
   }
+  if (c->trace_on && mixed(c))
+    return fail(MPSQMC_E_UNSUPPORTED, "the per-coupling trace is recorded by the FP64 sweep only");
+  if (c->use_graph && c->graph_trace != c->trace_on) drop_graphs(c);
   int per_step = 0;
-  if (c->use_graph && (!c->graph_exec || c->graph_trace != c->trace_on)) {
-    int rc = build_graph(c, &per_step);
-    if (rc) return rc;
-  }
-  if (c->use_graph)
-    per_step = (c->projector == MPSQMC_PROJECTOR_MPO_TERMS) ? 10 : ((c->h != 0.0) ? 11 : 7);
   double kernel_ms = 0.0;
   int launches = 0;
   CK(cudaEventRecord(c->ev[2], c->stream));
   for (int s = 0; s < nsteps; ++s) {
     const int N = c->n_cur;
     const int step = ++c->step_count;
+    const bool canon = qr_free(c) && step % canon_every(c) == 0;
     if (c->use_graph) {
-      CK(cudaGraphLaunch(c->graph_exec, c->stream));
+      if (!(canon ? c->graph_exec_canon : c->graph_exec)) {
+        int rc = build_graph(c, canon);
+        if (rc) return rc;
+      }
+      CK(cudaGraphLaunch(canon ? c->graph_exec_canon : c->graph_exec, c->stream));
+      per_step = c->graph_launches[canon ? 1 : 0];
     } else {
-      int rc = enqueue_step(c, &per_step);
+      int rc = enqueue_step(c, &per_step, canon);
       if (rc) return rc;
     }
     launches += per_step;
@@ -936,6 +1141,7 @@ int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
     c->last_n_before = N;
     c->last_n_after = sd.n_new;
     c->n_cur = sd.n_new;
+    c->gauge_dirty = qr_free(c) && !canon && c->h == 0.0;
     if (stats) {
       mpsqmc_step_stats &o = stats[s];
       o.step = step;
@@ -1029,6 +1235,7 @@ int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspa
   const int keep_nd = c->Ndesired, keep_step = c->step_count;
   const unsigned long long keep_draws = c->draws;
   const bool keep_trace = c->trace_on;
+  const bool keep_dirty = c->gauge_dirty;
   auto restore = [&](int n_walkers) -> int {
     for (int w = 0; w < k; ++w)
       CK(cudaMemcpyAsync(c->d_walkers + (size_t)slots[w] * c->wstride, snap + (size_t)w * c->wstride,
@@ -1074,13 +1281,11 @@ int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspa
   c->Ndesired = keep_nd;
   c->trace_on = keep_trace;
   const int rr = restore(N);
+  c->gauge_dirty = keep_dirty;
   cudaFree(snap);
   if (rc) return rc;
   if (rr) return rr;
-  if (c->graph_exec) {  // captured with the subset's population size
-    cudaGraphExecDestroy(c->graph_exec);
-    c->graph_exec = nullptr;
-  }
+  drop_graphs(c);  // captured with the subset's population size
   rc = mpsqmc_set_option(c, MPSQMC_OPT_SWEEP, choice.first);
   if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_WORKSPACE, choice.second);
   if (rc) return rc;
@@ -1160,7 +1365,7 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
       if (rc) return rc;
       cudaFree(c->d_scratch);
       c->d_scratch = nullptr;
-      if (dalloc(&c->d_scratch, (size_t)c->max_ctas * c->scr_stride)) return MPSQMC_E_CUDA;
+      if (dalloc(&c->d_scratch, scratch_doubles(c))) return MPSQMC_E_CUDA;
       c->workspace = (int)value;
       break;
     }
@@ -1178,13 +1383,35 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
         return fail(MPSQMC_E_ARG, "unknown resampling");
       c->resample = (int)value;
       break;
+    case MPSQMC_OPT_CANONICAL_INTERVAL:
+      if (value < 0 || value > (1L << 30)) return fail(MPSQMC_E_ARG, "canonical interval must be >= 0");
+      c->canon_interval = (int)value;
+      break;
+    case MPSQMC_OPT_PRECISION:
+      if (value != MPSQMC_PRECISION_FP64 && value != MPSQMC_PRECISION_TF32 && value != MPSQMC_PRECISION_TF32X3)
+        return fail(MPSQMC_E_ARG, "unknown precision");
+      c->precision = (int)value;
+      break;
+    case MPSQMC_OPT_PROPOSAL:
+      if (value != MPSQMC_PROPOSAL_GRID && value != MPSQMC_PROPOSAL_LEARNED) return fail(MPSQMC_E_ARG, "unknown proposal");
+      if (value == MPSQMC_PROPOSAL_LEARNED) {
+        const int rc = prop_alloc(c);
+        if (rc) return rc;
+      }
+      c->proposal = (int)value;
+      break;
+    case MPSQMC_OPT_PROPOSAL_TRAINING:
+      if (value != 0 && value != 1) return fail(MPSQMC_E_ARG, "proposal training is 0 or 1");
+      if (value) {
+        const int rc = prop_alloc(c);
+        if (rc) return rc;
+      }
+      c->prop_train = value != 0;
+      break;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");
   }
-  if (c->graph_exec) {  // the captured step no longer matches
-    cudaGraphExecDestroy(c->graph_exec);
-    c->graph_exec = nullptr;
-  }
+  drop_graphs(c);  // the captured steps no longer match
   return 0;
 }
 
@@ -1206,9 +1433,72 @@ int mpsqmc_get_option(mpsqmc_ctx *c, int option, long *value) {
     case MPSQMC_OPT_PROJECTOR:
       *value = c->projector;
       return 0;
+    case MPSQMC_OPT_CANONICAL_INTERVAL:
+      *value = c->canon_interval;
+      return 0;
+    case MPSQMC_OPT_PRECISION:
+      *value = c->precision;
+      return 0;
+    case MPSQMC_OPT_PROPOSAL:
+      *value = c->proposal;
+      return 0;
+    case MPSQMC_OPT_PROPOSAL_TRAINING:
+      *value = c->prop_train ? 1 : 0;
+      return 0;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");
   }
+}
+
+int mpsqmc_proposal_params(mpsqmc_ctx *c, float *out, const float *in, long *n_params) {
+  if (!c) return fail(MPSQMC_E_ARG, "null context");
+  int rc = prop_alloc(c);
+  if (rc) return rc;
+  if (n_params) *n_params = c->nparams;
+  CK(cudaSetDevice(c->device));
+  if (out) CK(cudaMemcpy(out, c->d_pw, sizeof(float) * c->nparams, cudaMemcpyDeviceToHost));
+  if (in) {
+    CK(cudaMemcpy(c->d_pw, in, sizeof(float) * c->nparams, cudaMemcpyHostToDevice));
+    CK(cudaMemset(c->d_pm, 0, sizeof(float) * c->nparams));
+    CK(cudaMemset(c->d_pv, 0, sizeof(float) * c->nparams));
+    CK(cudaMemset(c->d_pt, 0, sizeof(int)));
+    mq::mlp_to_bf16_kernel<<<64, 256, 0, c->stream>>>(c->nparams, c->d_pw, c->d_pwb);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return 0;
+}
+
+int mpsqmc_proposal_loss_grad(mpsqmc_ctx *c, int B, const float *features, const float *targets, double *loss,
+                              float *grad) {
+  if (!c || !features || !targets) return fail(MPSQMC_E_ARG, "null argument");
+  if (B < 1 || B > c->capacity) return fail(MPSQMC_E_ARG, "batch size outside [1, capacity]");
+  int rc = prop_alloc(c);
+  if (rc) return rc;
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(c->d_pfeat, features, sizeof(float) * (size_t)B * mq::kMlpIn, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_ptarget, targets, sizeof(float) * (size_t)B * c->G, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_pb, &B, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  int n = 0;
+  rc = enqueue_training(c, c->d_pb, false, &n);
+  if (rc) return rc;
+  if (loss) CK(cudaMemcpyAsync(loss, c->d_ploss, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (grad) CK(cudaMemcpyAsync(grad, c->d_pg, sizeof(float) * c->nparams, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int mpsqmc_proposal_stats(mpsqmc_ctx *c, double *last_loss, int *updates) {
+  if (!c) return fail(MPSQMC_E_ARG, "null context");
+  if (!c->d_pw) {
+    if (last_loss) *last_loss = 0.0;
+    if (updates) *updates = 0;
+    return 0;
+  }
+  CK(cudaSetDevice(c->device));
+  if (last_loss) CK(cudaMemcpy(last_loss, c->d_ploss, sizeof(double), cudaMemcpyDeviceToHost));
+  if (updates) CK(cudaMemcpy(updates, c->d_pt, sizeof(int), cudaMemcpyDeviceToHost));
+  return 0;
 }
 
 }  // extern "C"

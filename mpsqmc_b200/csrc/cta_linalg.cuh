@@ -289,6 +289,236 @@ static __device__ __noinline__ void cta_closure16(int M, int N, int K, const dou
   __syncthreads();
 }
 
+// ---------------------------------------------------------------------------------------------
+// FP32 storage, TF32 tensor cores (the mixed-precision sweep)
+//
+// mma.sync.m16n8k8 .tf32 with FP32 accumulation.  Fragment layouts (PTX ISA, m16n8k8 .tf32),
+// g = lane >> 2, t = lane & 3:
+//   A (16x8, row):  a0 A[g][t], a1 A[g+8][t], a2 A[g][t+4], a3 A[g+8][t+4]
+//   B (8x8, col):   b0 B[t][g], b1 B[t+4][g]
+//   C/D (16x8):     c0 C[g][2t], c1 C[g][2t+1], c2 C[g+8][2t], c3 C[g+8][2t+1]
+// NP = 1: operands rounded to TF32 (10-bit mantissa) once.  NP = 3: each operand split into a
+// TF32 head and a TF32 tail, three products (tail*head + head*tail + head*head), which carries
+// the FP32 operands' precision through the tensor cores.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t tf32_bits(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// One k-step of 8 for a 16x16 output block: A fragment a[4] (FP32 values), B fragments of the
+// two 8-column halves b[2][2]; acc[j] is the 16x8 half j.
+template <int NP>
+__device__ __forceinline__ void mma_block16(float (&acc)[2][4], const float (&a)[4], const float (&b)[2][2]) {
+  uint32_t ah[4], bh[2][2];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) ah[q] = tf32_bits(a[q]);
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) bh[j][q] = tf32_bits(b[j][q]);
+  if (NP == 3) {
+    uint32_t at[4], bt[2][2];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) at[q] = tf32_bits(a[q] - __uint_as_float(ah[q]));
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) bt[j][q] = tf32_bits(b[j][q] - __uint_as_float(bh[j][q]));
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      mma_tf32(acc[j], at[0], at[1], at[2], at[3], bh[j][0], bh[j][1]);
+      mma_tf32(acc[j], ah[0], ah[1], ah[2], ah[3], bt[j][0], bt[j][1]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j) mma_tf32(acc[j], ah[0], ah[1], ah[2], ah[3], bh[j][0], bh[j][1]);
+}
+
+// C (M x N, ldc) = alpha * op(A) * op(B) + beta * C in FP32 with TF32 tensor cores; the same
+// operand conventions, block ownership (16x16 output blocks per warp, so two calls with the same
+// M, N may accumulate without a barrier) and bounds rules as the FP64 cta_gemm.
+template <int NP>
+static __device__ __noinline__ void cta_gemm_tf32(int M, int N, int K, float alpha, const float *A, int lda,
+                                                  bool ta, const float *B, int ldb, bool tb, float beta,
+                                                  float *C, int ldc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int bm = (M + 15) >> 4, bn = (N + 15) >> 4;
+  const bool full = ((M | N | K) & 15) == 0;
+  const long sam = ta ? lda : 1, sak = ta ? 1 : lda;  // A(m, k) = A[m*sam + k*sak]
+  const long sbk = tb ? ldb : 1, sbn = tb ? 1 : ldb;  // B(k, n) = B[k*sbk + n*sbn]
+  for (int blk = warp; blk < bm * bn; blk += kWarps) {
+    const int m0 = (blk % bm) << 4, n0 = (blk / bm) << 4;
+    const int ma = m0 + g, mb = m0 + 8 + g;
+    float acc[2][4];
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[j][q] = 0.f;
+    if (full) {
+      const float *pa = A + ma * sam + t * sak, *pb = B + t * sbk + (n0 + g) * sbn;
+      const long a8 = 8 * sam, k4a = 4 * sak, k4b = 4 * sbk, n8 = 8 * sbn;
+#pragma unroll 2
+      for (int k0 = 0; k0 < K; k0 += 8) {
+        const float *qa = pa + k0 * sak, *qb = pb + k0 * sbk;
+        const float a[4] = {qa[0], qa[a8], qa[k4a], qa[a8 + k4a]};
+        const float b[2][2] = {{qb[0], qb[k4b]}, {qb[n8], qb[n8 + k4b]}};
+        mma_block16<NP>(acc, a, b);
+      }
+    } else {
+      for (int k0 = 0; k0 < K; k0 += 8) {
+        const int ka = k0 + t, kb = k0 + t + 4;
+        float a[4] = {0.f, 0.f, 0.f, 0.f}, b[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+        if (ka < K) {
+          if (ma < M) a[0] = A[ma * sam + ka * sak];
+          if (mb < M) a[1] = A[mb * sam + ka * sak];
+        }
+        if (kb < K) {
+          if (ma < M) a[2] = A[ma * sam + kb * sak];
+          if (mb < M) a[3] = A[mb * sam + kb * sak];
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int n = n0 + 8 * j + g;
+          if (n < N) {
+            if (ka < K) b[j][0] = B[ka * sbk + n * sbn];
+            if (kb < K) b[j][1] = B[kb * sbk + n * sbn];
+          }
+        }
+        mma_block16<NP>(acc, a, b);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int m = (q < 2) ? ma : mb, n = n0 + 8 * j + 2 * t + (q & 1);
+        if (full || (m < M && n < N)) {
+          float *c = C + m + (long)ldc * n;
+          const float v = alpha * acc[j][q];
+          *c = (beta == 0.f) ? v : v + beta * (*c);
+        }
+      }
+  }
+}
+
+// Sixteen closures (the FP32/TF32 counterpart of cta_closure16):
+//   out[k + 4 (s + 2 t)] = sum_{m < M, n < N} (A_s B_t)[m, n] P_k[m, n],   s, t in {0, 1}, k < 4,
+// A_s = A + s*sa (M x K, ld lda, not transposed), B_t = B + t*sb (K x N, ld ldb), P_k = P + k*sp.
+// Partial sums leave the warps in FP64.  red: >= 16*kWarps doubles.  Ends with a barrier.
+template <int NP>
+static __device__ __noinline__ void cta_closure16_tf32(int M, int N, int K, const float *A, int lda, long sa,
+                                                       const float *B, int ldb, long sb, const float *P, int ldp,
+                                                       long sp, double *red, double *out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int bm = (M + 15) >> 4, bn = (N + 15) >> 4;
+  double v[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = 0.0;
+  for (int blk = warp; blk < bm * bn; blk += kWarps) {
+    const int m0 = (blk % bm) << 4, n0 = (blk / bm) << 4;
+    const int ma = m0 + g, mb = m0 + 8 + g;
+#pragma unroll 1
+    for (int s = 0; s < 2; ++s) {
+      const float *As = A + s * sa;
+      float acc[2][2][4];  // [t][n half][fragment]
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[u][j][q] = 0.f;
+      for (int k0 = 0; k0 < K; k0 += 8) {
+        const int ka = k0 + t, kb = k0 + t + 4;
+        float a[4] = {0.f, 0.f, 0.f, 0.f};
+        if (ka < K) {
+          if (ma < M) a[0] = As[ma + (long)lda * ka];
+          if (mb < M) a[1] = As[mb + (long)lda * ka];
+        }
+        if (kb < K) {
+          if (ma < M) a[2] = As[ma + (long)lda * kb];
+          if (mb < M) a[3] = As[mb + (long)lda * kb];
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          float b[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const int n = n0 + 8 * j + g;
+            if (n < N) {
+              if (ka < K) b[j][0] = B[u * sb + ka + (long)ldb * n];
+              if (kb < K) b[j][1] = B[u * sb + kb + (long)ldb * n];
+            }
+          }
+          mma_block16<NP>(acc[u], a, b);
+        }
+      }
+      // epilogue: dot the product blocks with the four P blocks
+      float w[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) w[q] = 0.f;
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int m = (q < 2) ? ma : mb, n = n0 + 8 * j + 2 * t + (q & 1);
+          if (m < M && n < N) {
+            const float *pp = P + m + (long)ldp * n;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const float pk = pp[k * sp];
+              w[k] += acc[0][j][q] * pk;
+              w[k + 4] += acc[1][j][q] * pk;
+            }
+          }
+        }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        v[k + 4 * s] += w[k];
+        v[k + 8 + 4 * s] += w[k + 4];
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 16; ++q)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < 16; ++q) red[q * kWarps + warp] = v[q];
+  __syncthreads();
+  if (threadIdx.x < 16) {
+    double sum = 0.0;
+    for (int w = 0; w < kWarps; ++w) sum += red[threadIdx.x * kWarps + w];
+    out[threadIdx.x] = sum;
+  }
+  __syncthreads();
+}
+
+// Overloads that let the sweep be written once for FP64 (DMMA) and FP32 (TF32) work buffers.
+template <int NP>
+__device__ __forceinline__ void gemm_t(int M, int N, int K, double alpha, const double *A, int lda, bool ta,
+                                       const double *B, int ldb, bool tb, double beta, double *C, int ldc) {
+  cta_gemm(M, N, K, alpha, A, lda, ta, B, ldb, tb, beta, C, ldc);
+}
+template <int NP>
+__device__ __forceinline__ void gemm_t(int M, int N, int K, float alpha, const float *A, int lda, bool ta,
+                                       const float *B, int ldb, bool tb, float beta, float *C, int ldc) {
+  cta_gemm_tf32<NP>(M, N, K, alpha, A, lda, ta, B, ldb, tb, beta, C, ldc);
+}
+
 // Sum of v over the CTA; result returned to every thread.  red: >= kWarps doubles of smem.
 __device__ __forceinline__ double cta_sum(double v, double *red) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

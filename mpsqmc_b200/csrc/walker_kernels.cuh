@@ -22,6 +22,8 @@
 // (C_kl, PDF, weights, overlaps, energies) is gauge invariant.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "cta_linalg.cuh"
 
 namespace mq {
@@ -43,6 +45,7 @@ struct Dev {
   int *ctr;         // work counters of the persistent kernels (zeroed before each launch)
   const int *sel;   // set_overlap_kernel: only walkers w with sel[w] != 0 (nullptr: all)
   const double *trial;
+  const float *trial32;  // FP32 copy of the trial (mixed-precision sweep), or nullptr
   long wstride;     // doubles per walker slot
   double *walkers;
   const int *slot_of;  // logical walker -> slot
@@ -78,6 +81,14 @@ struct Dev {
   const int *eopen;        // [L]: slot of the channel that site k opens, or -1
   long choff;              // energy channels inside a CTA's scratch: 2 "done" + 3 per slot
   long gwoff;              // matrix work buffers inside a CTA's scratch, or -1 (shared memory)
+  // QR-free general sweep: sites are stored as they leave the centre (rescaled to unit Frobenius
+  // norm) and a left norm environment (maxB x maxB, ld pb) inside the scratch gives the norm
+  long nloff;              // its offset inside a CTA's scratch, or -1 (Householder QR per site)
+  // learned proposal (proposal.cuh)
+  int prop_mode;                 // 0: the exact grid PDF; 1: the network's proposal, exact-ratio weights
+  int prop_collect;              // 1: store (features, PDF) of coupling w % nC of every walker w
+  const __nv_bfloat16 *prop_w;   // network parameters (BF16 copy)
+  float *prop_feat, *prop_target;  // [capacity][32], [capacity][G]
 };
 
 enum : int { kErrNumeric = 1, kErrCapacity = 2 };
@@ -88,13 +99,20 @@ __host__ __device__ inline int padld(int x) {
   return p;
 }
 
-struct Smem {
-  double *Lenv, *Cen, *Nxt, *Xb, *Pb, *Qt, *QRb, *Rf, *red, *tau, *wv, *M, *Cm, *O1, *O2, *pdf, *sc;
+// Work buffers of one CTA.  T: precision of the matrix buffers (double, or float in the
+// mixed-precision sweep); the small buffers (reductions, closures, PDF) are always FP64.
+template <typename T>
+struct SmemT {
+  T *Lenv, *Cen, *Nxt, *Xb, *Pb, *Qt, *QRb, *Rf;
+  double *red, *tau, *wv, *M, *Cm, *O1, *O2, *pdf, *sc;
+  float *mlp;   // learned proposal: features (32), hidden (256), partial sums (256), logits (256)
+  double *qprop;  // learned proposal: q~ over the grid (G)
   int *bW;      // bond dims of the walker being processed [L+1]
   long *woff;   // its site offsets [L]
   int *wsel;    // the walker index handed out by the work counter
   int sbC, sbX;  // sigma-block strides of Cen/Nxt and of Xb/Pb
 };
+using Smem = SmemT<double>;
 
 // Work buffers of one CTA.  The small ones always live in shared memory.  The matrix buffers
 // (environments, site tensors, branches, QR panel) follow them in shared memory when they fit;
@@ -131,16 +149,19 @@ __host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, i
   take(s ? s->pdf : dummy, G);
   take(s ? s->sc : dummy, 16);
   {
-    double *b, *o, *q;
+    double *b, *o, *q, *m;
     take(b, (L + 2) / 2);
     take(o, L);
     take(q, 1);
+    take(m, 400);
     if (s) {
       s->bW = reinterpret_cast<int *>(b);
       s->woff = reinterpret_cast<long *>(o);
       s->wsel = reinterpret_cast<int *>(q);
+      s->mlp = reinterpret_cast<float *>(m);
     }
   }
+  take(s ? s->qprop : dummy, G);
   take_big(s ? s->Lenv : dummy, (long)pa * maxB);
   take_big(s ? s->Cen : dummy, (long)pb * maxB * d);
   take_big(s ? s->Nxt : dummy, (long)pb * maxB * d);
@@ -157,15 +178,87 @@ __host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, i
   return off;
 }
 
+// The same buffers for the mixed-precision sweep: FP64 small buffers as above, FP32 matrix
+// buffers, no QR panel (that sweep is QR-free).  Sizes in bytes; *big_floats (if given)
+// receives the size of the matrix buffers in floats.
+__host__ __device__ inline long smem_bytes_f32(int L, int maxA, int maxB, int G, int pa, int pb,
+                                               SmemT<float> *s, double *base, float *big = nullptr,
+                                               long *big_floats = nullptr) {
+  long off = 0, boff = 0;  // doubles of the small buffers; floats of the matrix buffers
+  double *dummy;
+  float *fdummy;
+  auto take = [&](double *&p, long n) {
+    if (s) p = base + off;
+    off += (n + 3) & ~3L;
+  };
+  const int d = kMaxD;
+  take(s ? s->red : dummy, 16 * kWarps);
+  take(s ? s->tau : dummy, maxB);
+  take(s ? s->wv : dummy, maxB);
+  take(s ? s->M : dummy, 16);
+  take(s ? s->Cm : dummy, 16);
+  take(s ? s->O1 : dummy, 4);
+  take(s ? s->O2 : dummy, 4);
+  take(s ? s->pdf : dummy, G);
+  take(s ? s->sc : dummy, 16);
+  {
+    double *b, *o, *q, *m;
+    take(b, (L + 2) / 2);
+    take(o, L);
+    take(q, 1);
+    take(m, 400);
+    if (s) {
+      s->bW = reinterpret_cast<int *>(b);
+      s->woff = reinterpret_cast<long *>(o);
+      s->wsel = reinterpret_cast<int *>(q);
+      s->mlp = reinterpret_cast<float *>(m);
+    }
+  }
+  take(s ? s->qprop : dummy, G);
+  float *fbase = reinterpret_cast<float *>(base + off);
+  long soff = 0;  // floats placed in shared memory after the small buffers
+  auto take_big = [&](float *&p, long n) {
+    const long r = (n + 7) & ~7L;
+    if (big) {
+      if (s) p = big + boff;
+    } else {
+      if (s) p = fbase + soff;
+      soff += r;
+    }
+    boff += r;
+  };
+  take_big(s ? s->Lenv : fdummy, (long)pa * maxB);
+  take_big(s ? s->Cen : fdummy, (long)pb * maxB * d);
+  take_big(s ? s->Nxt : fdummy, (long)pb * maxB * d);
+  take_big(s ? s->Xb : fdummy, (long)pa * maxB * d);
+  take_big(s ? s->Pb : fdummy, (long)pa * maxB * kN2);
+  take_big(s ? s->Qt : fdummy, (long)pa * maxB);
+  if (s) {
+    s->QRb = nullptr;
+    s->Rf = nullptr;
+    s->sbC = pb * maxB;
+    s->sbX = pa * maxB;
+  }
+  if (big_floats) *big_floats = boff;
+  return (long)sizeof(double) * off + (long)sizeof(float) * soff;
+}
+
 // Carve the work buffers of the calling CTA (shared memory, plus its global scratch when the
 // matrix buffers do not fit on chip).
 __device__ __forceinline__ void carve(const Dev &p, Smem &s, double *smem_raw) {
   double *big = (p.gwoff >= 0) ? p.scratch + (long)blockIdx.x * p.scr_stride + p.gwoff : nullptr;
   smem_doubles(p.L, p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw, big);
 }
+// Mixed precision: the CTA's scratch is read as floats with the same element offsets.
+__device__ __forceinline__ void carve(const Dev &p, SmemT<float> &s, double *smem_raw) {
+  float *big = (p.gwoff >= 0) ? reinterpret_cast<float *>(p.scratch) + (long)blockIdx.x * p.scr_stride + p.gwoff
+                              : nullptr;
+  smem_bytes_f32(p.L, p.maxA, p.maxB, p.G, p.pa, p.pb, &s, smem_raw, big);
+}
 
 // Bond dims and site offsets of the walker in `slot` into shared memory.  Ends with a barrier.
-__device__ __forceinline__ void load_walker_dims(const Dev &p, Smem &s, int slot) {
+template <typename T>
+__device__ __forceinline__ void load_walker_dims(const Dev &p, SmemT<T> &s, int slot) {
   for (int k = threadIdx.x; k <= p.L; k += kThreads) s.bW[k] = p.wdims[(long)slot * (p.L + 1) + k];
   for (int k = threadIdx.x; k < p.L; k += kThreads) s.woff[k] = p.wofs[(long)slot * p.L + k];
   __syncthreads();
@@ -174,7 +267,8 @@ __device__ __forceinline__ void load_walker_dims(const Dev &p, Smem &s, int slot
 // Dynamic scheduling of the persistent grid: the next logical walker from the kernel's work
 // counter (walkers of uneven bond dimension cost unevenly).  Starts with a barrier, so the
 // previous walker's shared data is no longer in use.
-__device__ __forceinline__ int next_walker(Smem &s, int *ctr) {
+template <typename T>
+__device__ __forceinline__ int next_walker(SmemT<T> &s, int *ctr) {
   __syncthreads();
   if (threadIdx.x == 0) *s.wsel = atomicAdd(ctr, 1);
   __syncthreads();
@@ -183,21 +277,22 @@ __device__ __forceinline__ int next_walker(Smem &s, int *ctr) {
 
 enum : int { kCtrStep = 0, kCtrSetOverlap = 1, kCtrEnergy = 2, kCtrCompress = 3, kNumCtr = 8 };
 
-// dst[sigma*sb + r + ld*c] = src[r + dl*(c + dr*sigma)]   (site storage -> padded smem)
-__device__ __forceinline__ void load_site(double *dst, int ld, int sb, const double *src, int dl,
-                                          int dr) {
+// dst[sigma*sb + r + ld*c] = src[r + dl*(c + dr*sigma)]   (site storage -> padded smem; an
+// FP32 destination rounds the FP64 walker)
+template <typename T>
+__device__ __forceinline__ void load_site(T *dst, int ld, int sb, const double *src, int dl, int dr) {
   const int n = dl * dr * kMaxD;
   for (int q = threadIdx.x; q < n; q += kThreads) {
     const int r = q % dl, rest = q / dl, c = rest % dr, s = rest / dr;
-    dst[s * sb + r + ld * c] = src[q];
+    dst[s * sb + r + ld * c] = T(src[q]);
   }
 }
-__device__ __forceinline__ void store_site(double *dst, const double *src, int ld, int sb, int dl,
-                                           int dr) {
+template <typename T>
+__device__ __forceinline__ void store_site(double *dst, const T *src, int ld, int sb, int dl, int dr) {
   const int n = dl * dr * kMaxD;
   for (int q = threadIdx.x; q < n; q += kThreads) {
     const int r = q % dl, rest = q / dl, c = rest % dr, s = rest / dr;
-    dst[q] = src[s * sb + r + ld * c];
+    dst[q] = double(src[s * sb + r + ld * c]);
   }
 }
 

@@ -14,7 +14,7 @@ import pytest
 from conftest import WALK_CASES, couplings, load_golden
 from mpsqmc_b200 import Engine
 from mpsqmc_b200 import problem as pb
-from mpsqmc_b200.capi import OPT_SWEEP, OPT_WORKSPACE, SWEEP_NEAREST, WORKSPACE_GLOBAL
+from mpsqmc_b200.capi import OPT_CANONICAL_INTERVAL, OPT_SWEEP, OPT_WORKSPACE, SWEEP_NEAREST, WORKSPACE_GLOBAL
 from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu
@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-10
 
 
-def engine_for(z, capacity=None, sweep=None, workspace=None):
+def engine_for(z, capacity=None, sweep=None, workspace=None, canon=None):
     meta = z["meta"]
     L, N = meta["L"], meta["Nw"]
     ci, cj, cJ = couplings(z)
@@ -37,6 +37,9 @@ def engine_for(z, capacity=None, sweep=None, workspace=None):
     if workspace is not None:
         eng.set_option(OPT_WORKSPACE, workspace)
         assert eng.get_option(OPT_WORKSPACE) == workspace
+    if canon is not None:
+        eng.set_option(OPT_CANONICAL_INTERVAL, canon)
+        assert eng.get_option(OPT_CANONICAL_INTERVAL) == canon
     return eng
 
 
@@ -46,8 +49,9 @@ def fidelity(dims_a, a, dims_b, b):
     return ab / np.sqrt(po.inner_product(A, A) * po.inner_product(B, B))
 
 
-MODES = {"auto": (None, None), "nearest": (SWEEP_NEAREST, None), "global-ws": (None, WORKSPACE_GLOBAL),
-         "nearest-global-ws": (SWEEP_NEAREST, WORKSPACE_GLOBAL)}
+MODES = {"auto": (None, None, None), "qr-per-site": (None, None, 0), "nearest": (SWEEP_NEAREST, None, None),
+         "global-ws": (None, WORKSPACE_GLOBAL, None), "nearest-global-ws": (SWEEP_NEAREST, WORKSPACE_GLOBAL, None),
+         "qr-free-2": (None, None, 2), "qr-free-global-ws": (None, WORKSPACE_GLOBAL, 3)}
 
 
 @pytest.mark.parametrize("mode", list(MODES))
@@ -55,13 +59,16 @@ MODES = {"auto": (None, None), "nearest": (SWEEP_NEAREST, None), "global-ws": (N
 def test_walk_matches_reference(case, mode):
     """Every case runs the general sweep (the default); chains also run the nearest-neighbour
     sweep.  "global-ws" keeps the matrix work buffers in global scratch (the placement large bond
-    dimensions use) instead of shared memory."""
+    dimensions use) instead of shared memory.  The default general sweep skips the per-site QR and
+    left-normalises every 8 steps; "qr-per-site" runs the Householder QR at every site, "qr-free-2"
+    ("qr-free-global-ws") left-normalise every 2 (3) steps, so that steps of both kinds are
+    compared."""
     z = load_golden(case)
     meta = z["meta"]
-    sweep, ws = MODES[mode]
+    sweep, ws, canon = MODES[mode]
     if sweep == SWEEP_NEAREST and "snake" in case:
         pytest.skip("the nearest-neighbour sweep takes chains only")
-    eng = engine_for(z, sweep=sweep, workspace=ws)
+    eng = engine_for(z, sweep=sweep, workspace=ws, canon=canon)
     assert eng.energy() == pytest.approx(meta["E0"], rel=RTOL)
     total_draws = 0
     for s in range(1, meta["steps"] + 1):
@@ -182,3 +189,24 @@ def test_autotune_restores_population_and_keeps_trajectory():
     # the choice is remembered for the same shape
     eng2 = engine_for(z)
     assert eng2.autotune(steps=2) == (sweep, ws)
+
+
+def test_qr_free_walkers_read_back_left_canonical():
+    """After QR-free steps (default interval 8, so the walkers were not left-normalised by the
+    walk), mpsqmc_get_walkers returns Walker::setOverlap's state: every site but the last
+    left-orthonormal, norm 1, overlaps <Psi_T|phi> > 0 of those tensors."""
+    z = load_golden("walk_snake4x4_D16_DW8_branch")
+    eng = engine_for(z)
+    eng.walk(3)
+    w, wt, ov, eh = eng.get_walkers()
+    dims = z["walker0_init_dims"]
+    trial = po.MPS(z["trial_ln_dims"], z["trial_ln_data"])
+    for k in range(w.shape[0]):
+        m = po.MPS(np.asarray(dims, np.int32), w[k])
+        for s in range(m.L - 1):
+            A = m.site(s)  # [sigma, Dr, Dl]: the transposed sigma blocks
+            G = sum(A[q] @ A[q].T for q in range(A.shape[0]))
+            np.testing.assert_allclose(G, np.eye(G.shape[0]), atol=1e-12)
+        assert po.inner_product(m, m) == pytest.approx(1.0, abs=1e-12)
+        assert po.inner_product(trial, m) == pytest.approx(ov[k], rel=1e-10)
+        assert ov[k] > 0
