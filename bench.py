@@ -57,10 +57,14 @@ def parse():
     ap.add_argument("--train-steps", type=int, default=30)
     ap.add_argument("--canon", type=int, default=None, metavar="K",
                     help="QR-free sweep, left-normalise every K steps (0: Householder QR per site; "
-                         "default: the engine's, 8)")
-    ap.add_argument("--vn-compare", type=int, default=0, metavar="STEPS",
-                    help="VN of this configuration and of the plain FP64 grid walk (same workload, start "
-                         "and random stream), STEPS steps each after the timed ones; reports their ratio")
+                         "default: the engine's, 16)")
+    ap.add_argument("--vn-compare", type=int, default=None, metavar="STEPS",
+                    help="variance-normalised throughput (the BASELINE metric) of the plain FP64 grid walk "
+                         "and of the --vn-arms variants, STEPS steps each after their timed steps, from the "
+                         "same start and random stream; ratios against the plain walk (default: 300 on the "
+                         "default chain64 run, else off)")
+    ap.add_argument("--vn-arms", default="tf32x3/grid,tf32x3/learned",
+                    help="precision/proposal variants compared with the plain FP64 grid walk")
     return ap.parse_args()
 
 
@@ -278,7 +282,7 @@ def main():
                "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.Ds, "dtau": wl.dtau,
                "parallelism": f"replicas x{world}", "sweep": args.sweep,
                "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
-               "canonical_interval": args.canon if args.canon is not None else 8}
+               "canonical_interval": args.canon if args.canon is not None else 16}
     else:
         wl = workloads.chain64(Nw=args.walkers or 2048)
         cfg = {"workload": f"{wl.name}: L={wl.L} Heisenberg chain, D_T={wl.DT}, D_W={wl.DW}, {wl.Nw} walkers/GPU, "
@@ -287,7 +291,7 @@ def main():
                "l2": f"population ({wl.Nw * wl.walker.data.size * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
                "parallelism": f"replicas x{world}", "sweep": args.sweep,
                "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
-               "canonical_interval": args.canon if args.canon is not None else 8}
+               "canonical_interval": args.canon if args.canon is not None else 16}
 
     if args.impl == "reference":
         if rank != 0:
@@ -353,7 +357,11 @@ def main():
     value = ws_all / (t_ms * 1e-3)
 
     vn = None
-    vn_steps = max(args.vn, args.vn_compare)
+    vn_compare = args.vn_compare
+    if vn_compare is None:
+        vn_compare = 300 if (not lattice and args.precision == "fp64" and args.proposal == "grid"
+                             and args.walkers is None and args.steps >= 5) else 0
+    vn_steps = max(args.vn, vn_compare)
     if vn_steps > 0:
         from mpsqmc_b200 import analysis
         e_ref = None
@@ -370,26 +378,42 @@ def main():
                 r["abs_err_per_site"] = abs(r["E_mean"] - e_ref) / wl.L
             return r
 
-        vn = vn_of(eng, value / max(world, 1))
-        vn["arm"] = f"{args.precision}/{args.proposal}"
-        if args.vn_compare > 0:
-            # the yardstick: plain FP64 grid walk from the same start and random stream
+        def arm(precision, proposal):
+            """A variant from the same start and random stream: set-up (training for the learned
+            proposal), warm-up, timed steps for its throughput, then the VN steps."""
+            a = argparse.Namespace(**vars(args))
+            a.precision, a.proposal = precision, proposal
             if lattice:
-                ep, _ = lattice_engine(wl, local)
+                e, _ = lattice_engine(wl, local)
             else:
-                ep = Engine(device=local, **inputs)
-                ep.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
-            configure(ep, args, sweep, plain=True)
-            ep.set_rng(wl.seed + 7919 * rank, 0)
-            ep.walk(args.warmup + (args.train_steps if training else 0))
-            sp = ep.walk(args.steps)
-            tp = ep.last_timing()
-            thr = sum(x["n_walkers"] for x in sp) / (tp["total_ms"] * 1e-3)
-            plain_vn = vn_of(ep, thr)
-            ep.close()
-            vn = {"this": vn, "plain_fp64_grid": plain_vn,
-                  "vn_ratio_vs_plain_fp64": vn["vn"] / plain_vn["vn"] if plain_vn["vn"] else None,
-                  "throughput_ratio_vs_plain_fp64": vn["throughput_per_gpu"] / thr}
+                e = Engine(device=local, **inputs)
+                e.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
+            configure(e, a, sweep, plain=(precision == "fp64"))
+            e.set_rng(wl.seed + 7919 * rank, 0)
+            tr = train_proposal(e, a)
+            e.walk(args.warmup)
+            st = e.walk(args.steps)
+            t = e.last_timing()
+            thr = sum(x["n_walkers"] for x in st) / (t["total_ms"] * 1e-3)
+            r = vn_of(e, thr)
+            if tr:
+                r["proposal_training"] = tr
+            e.close()
+            return r
+
+        this = vn_of(eng, value / max(world, 1))
+        this["arm"] = f"{args.precision}/{args.proposal}"
+        vn = this
+        if vn_compare > 0:
+            plain = this if (args.precision, args.proposal) == ("fp64", "grid") else arm("fp64", "grid")
+            vn = {"plain_fp64_grid": plain, "vn_ratio_vs_plain_fp64": {}, "throughput_ratio_vs_plain_fp64": {}}
+            arms = [this["arm"]] if this is not plain else []
+            arms += [x for x in args.vn_arms.split(",") if x and x not in arms and x != "fp64/grid"]
+            for name in arms:
+                r = this if name == this["arm"] else arm(*name.split("/"))
+                vn[name] = r
+                vn["vn_ratio_vs_plain_fp64"][name] = r["vn"] / plain["vn"] if plain["vn"] else None
+                vn["throughput_ratio_vs_plain_fp64"][name] = r["throughput_per_gpu"] / plain["throughput_per_gpu"]
 
     # roofline of the dominant kernel (the walker-step kernel): canonical FP64 work / kernel time,
     # averaged over the walkers' own bond dims

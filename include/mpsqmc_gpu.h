@@ -192,7 +192,7 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
                                        * weight 1); the trace then holds [N][3] = PDF norm, uniform,
                                        * picked term (0 = identity).  The population-control options
                                        * above do not apply. */
-#define MPSQMC_OPT_CANONICAL_INTERVAL 6 /* K >= 1 (default 8): the general sweep stores each site
+#define MPSQMC_OPT_CANONICAL_INTERVAL 6 /* K >= 1 (default 16): the general sweep stores each site
                                          * as it leaves the centre, without the per-site
                                          * Householder QR (the norm comes from a left norm
                                          * environment), and restores the left-canonical form of

@@ -93,6 +93,7 @@ struct mpsqmc_ctx {
   long wsize = 0, wstride = 0, scr_stride = 0, foff = 0, gwoff = -1;
   long scr_base = 0;                    // scratch doubles per CTA before the matrix work buffers
   long all_doubles = 0, big_doubles = 0;  // work buffers: all of them / the matrix ones
+  long mlp_doubles = 0;                 // the learned proposal's small buffers (on chip while it is in use)
   size_t smem_optin = 0;
   bool global_work = false;             // matrix work buffers in global scratch
   int maxA = 1, maxB = 1, pa = 4, pb = 4, pq = 4;
@@ -129,7 +130,7 @@ struct mpsqmc_ctx {
   int workspace = MPSQMC_WORKSPACE_AUTO;
   int pc_interval = 1;                  // population control every pc_interval steps
   int resample = MPSQMC_RESAMPLE_THRESHOLD;
-  int canon_interval = 8;               // QR-free general sweep, LeftNormalize every K steps (0: off)
+  int canon_interval = 16;              // QR-free general sweep, LeftNormalize every K steps (0: off)
   bool gauge_dirty = false;             // the last step left the walkers un-normalised (QR-free)
   long nloff = 0;                       // its left norm environment inside a CTA's scratch
   int *d_ncop = nullptr;                // copies per walker in the branching step
@@ -280,6 +281,23 @@ size_t scratch_doubles(const mpsqmc_ctx *c) {
   return std::max((size_t)c->max_ctas * c->scr_stride, ((size_t)c->max_ctas_mixed * c->scr_stride + 1) / 2);
 }
 
+int layout_workspace(mpsqmc_ctx *c, bool force_global);
+
+// Recompute the work-buffer layout (after an option that changes it) and grow the scratch if needed.
+int relayout(mpsqmc_ctx *c, bool force_global) {
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  const size_t before = c->d_scratch ? scratch_doubles(c) : 0;
+  const int rc = layout_workspace(c, force_global);
+  if (rc) return rc;
+  if (scratch_doubles(c) > before) {
+    cudaFree(c->d_scratch);
+    c->d_scratch = nullptr;
+    if (dalloc(&c->d_scratch, scratch_doubles(c))) return MPSQMC_E_CUDA;
+  }
+  return 0;
+}
+
 void drop_graphs(mpsqmc_ctx *c) {
   for (cudaGraphExec_t *g : {&c->graph_exec, &c->graph_exec_canon})
     if (*g) {
@@ -324,15 +342,24 @@ void free_all(mpsqmc_ctx *c) {
 // Where the matrix work buffers of a CTA live: shared memory when they fit (and are not forced
 // out), else the CTA's global scratch.  Sets the scratch stride, the dynamic shared memory of
 // every walker kernel and the persistent grid size.
+// The learned proposal's buffers are on chip while the proposal samples or trains (the same
+// condition make_dev gives the kernels).
+bool mlp_on(const mpsqmc_ctx *c) {
+  return c->d_pwb != nullptr && c->projector == MPSQMC_PROJECTOR_TROTTER &&
+         (c->proposal == MPSQMC_PROPOSAL_LEARNED || c->prop_train);
+}
+
 int layout_workspace(mpsqmc_ctx *c, bool force_global) {
-  const bool global = force_global || sizeof(double) * (size_t)c->all_doubles > c->smem_optin;
+  const bool mlp = mlp_on(c);
+  const long all = c->all_doubles + (mlp ? c->mlp_doubles : 0);
+  const bool global = force_global || sizeof(double) * (size_t)all > c->smem_optin;
   c->scr_stride = (c->scr_base + 31) & ~31L;
   c->gwoff = -1;
-  c->smem_bytes = sizeof(double) * (size_t)c->all_doubles;
+  c->smem_bytes = sizeof(double) * (size_t)all;
   if (global) {
     c->gwoff = c->scr_stride;
     c->scr_stride = (c->gwoff + c->big_doubles + 31) & ~31L;
-    c->smem_bytes = sizeof(double) * (size_t)(c->all_doubles - c->big_doubles);
+    c->smem_bytes = sizeof(double) * (size_t)(all - c->big_doubles);
   }
   c->global_work = global;
   if (c->smem_bytes > c->smem_optin)
@@ -349,7 +376,7 @@ int layout_workspace(mpsqmc_ctx *c, bool force_global) {
   // FP64 buffers were placed in global scratch
   long big_floats = 0;
   const long mixed_all = mq::smem_bytes_f32(c->L, c->maxA, c->maxB, c->G, c->pa, c->pb, nullptr, nullptr, nullptr,
-                                            &big_floats);
+                                            &big_floats, mlp);
   c->smem_bytes_mixed = global ? (size_t)(mixed_all - (long)sizeof(float) * big_floats) : (size_t)mixed_all;
   const void *mk[] = {(const void *)mq::walker_step_mixed_kernel<1>, (const void *)mq::walker_step_mixed_kernel<3>};
   for (const void *k : mk)
@@ -523,6 +550,8 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   c->pq = mq::padld(d * c->maxB);
   c->all_doubles =
       mq::smem_doubles(L, c->maxA, c->maxB, c->G, c->pa, c->pb, c->pq, nullptr, nullptr, nullptr, &c->big_doubles);
+  c->mlp_doubles = mq::smem_doubles(L, c->maxA, c->maxB, c->G, c->pa, c->pb, c->pq, nullptr, nullptr, nullptr,
+                                    nullptr, true) - c->all_doubles;
   c->roff.resize(L + 1);
   long ro = 0;
   for (int k = 0; k <= L; ++k) {
@@ -1359,13 +1388,8 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
     case MPSQMC_OPT_WORKSPACE: {
       if (value != MPSQMC_WORKSPACE_AUTO && value != MPSQMC_WORKSPACE_GLOBAL)
         return fail(MPSQMC_E_ARG, "unknown workspace placement");
-      CK(cudaSetDevice(c->device));
-      CK(cudaStreamSynchronize(c->stream));
-      const int rc = layout_workspace(c, value == MPSQMC_WORKSPACE_GLOBAL);
+      const int rc = relayout(c, value == MPSQMC_WORKSPACE_GLOBAL);
       if (rc) return rc;
-      cudaFree(c->d_scratch);
-      c->d_scratch = nullptr;
-      if (dalloc(&c->d_scratch, scratch_doubles(c))) return MPSQMC_E_CUDA;
       c->workspace = (int)value;
       break;
     }
@@ -1399,6 +1423,10 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
         if (rc) return rc;
       }
       c->proposal = (int)value;
+      {
+        const int rc = relayout(c, c->workspace == MPSQMC_WORKSPACE_GLOBAL);
+        if (rc) return rc;
+      }
       break;
     case MPSQMC_OPT_PROPOSAL_TRAINING:
       if (value != 0 && value != 1) return fail(MPSQMC_E_ARG, "proposal training is 0 or 1");
@@ -1407,6 +1435,10 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
         if (rc) return rc;
       }
       c->prop_train = value != 0;
+      {
+        const int rc = relayout(c, c->workspace == MPSQMC_WORKSPACE_GLOBAL);
+        if (rc) return rc;
+      }
       break;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");

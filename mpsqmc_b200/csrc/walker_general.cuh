@@ -90,20 +90,24 @@ static __device__ void transfer_in_place(const Dev &p, SmemT<T> &s, const T *B, 
 // (slot q, operator a at Fch + (3q + a) * maxA * maxB, leading dimension maxA).
 // Order: branches P; done' from Fd, the channels that close on k and the field; channels that
 // stay open; then Lenv' and the channel site k opens (its slot may be one that closed on k).
+// have_P: the branches P of Tm are already in Pb (the caller derived them), skip their products.
 template <typename T, int NP = 0>
 static __device__ void env_update_general(const Dev &p, SmemT<T> &s, int k, const T *B, int al, int ar, int bl,
-                                          int br, const T *Tm, int cs, int ss, const T *Fd, T *Fdn, T *Fch) {
+                                          int br, const T *Tm, int cs, int ss, const T *Fd, T *Fdn, T *Fch,
+                                          bool have_P = false) {
   const int d = kMaxD, lda = p.maxA;
   const long fm = (long)p.maxA * p.maxB;
   // P[s + d t] = B[s]^T Lenv Tm[t]    (ar x br)
-  for (int tau = 0; tau < d; ++tau)
-    gemm_t<NP>(al, br, bl, T(1), s.Lenv, p.pa, false, Tm + tau * ss, cs, false, T(0), s.Xb + tau * s.sbX, p.pa);
-  __syncthreads();
-  for (int sg = 0; sg < d; ++sg)
+  if (!have_P) {
     for (int tau = 0; tau < d; ++tau)
-      gemm_t<NP>(ar, br, al, T(1), B + (long)sg * al * ar, al, true, s.Xb + tau * s.sbX, p.pa, false, T(0),
-                 s.Pb + (sg + d * tau) * s.sbX, p.pa);
-  __syncthreads();
+      gemm_t<NP>(al, br, bl, T(1), s.Lenv, p.pa, false, Tm + tau * ss, cs, false, T(0), s.Xb + tau * s.sbX, p.pa);
+    __syncthreads();
+    for (int sg = 0; sg < d; ++sg)
+      for (int tau = 0; tau < d; ++tau)
+        gemm_t<NP>(ar, br, al, T(1), B + (long)sg * al * ar, al, true, s.Xb + tau * s.sbX, p.pa, false, T(0),
+                   s.Pb + (sg + d * tau) * s.sbX, p.pa);
+    __syncthreads();
+  }
   // done' = -h sum Sz P + sum_s B[s]^T (sum_t G_st Tm[t]),
   // G_st = delta_st Fd + sum_{i closing on k} J_ik (Sx F_i,x - iSy F_i,iy + Sz F_i,z)(s,t)
   for (int q = threadIdx.x; q < ar * br; q += kThreads) {
@@ -340,6 +344,16 @@ __device__ __forceinline__ void apply_site_op(T *X, int ld, int sb, int dl, int 
   }
 }
 
+// The same on a site as stored in HBM (X[r + dl (c + dr sigma)], FP64), in place.  No barrier.
+__device__ __forceinline__ void apply_site_op_stored(double *X, int dl, int dr, const double *O) {
+  const int blk = dl * dr;
+  for (int q = threadIdx.x; q < blk; q += kThreads) {
+    const double x0 = X[q], x1 = X[blk + q];
+    X[q] = O[0] * x0 + O[2] * x1;
+    X[blk + q] = O[1] * x0 + O[3] * x1;
+  }
+}
+
 // ||phi||^2 of the walker with the centre C on site i (sites > i as stored in global memory):
 // N = sum_s A_k[s] N A_k[s]^T from site L-1 down to i+1 (in the norm-environment scratch), then
 // sum_s tr(C[s]^T Nl C[s] N) with the left norm environment Nl of sites < i (ld pb), or the
@@ -390,6 +404,7 @@ static __device__ double norm_from_centre(const Dev &p, SmemT<T> &s, const doubl
 // The walker step (all walkers of the population, one CTA per walker at a time).
 template <typename T, int NP>
 __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
+  constexpr bool kMixed = !std::is_same<T, double>::value;
   SmemT<T> s;
   carve(p, s, smem_raw);
   const int L = p.L, d = kMaxD, tid = threadIdx.x;
@@ -434,6 +449,9 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
     for (int i = 0; i < L; ++i) {
       const int al = p.aT[i], ar = p.aT[i + 1], bl = s.bW[i], br = s.bW[i + 1];
       const T *Bi = trial + p.toff[i];
+      // Pb still holds the last coupling's left branches at cut i+1 (its partner was i+1, so they
+      // were not carried further, and the trace did not use Pb as scratch)
+      bool branches_kept = false;
       for (int c = p.site_c0[i]; c < p.site_c0[i + 1]; ++c) {
         const int j = p.cp_j[c];
         while (rv > j + 1) {
@@ -466,11 +484,20 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
         closures<T, NP>(p, s, j, scr + p.roff[j + 1]);
         const double num = sample_coupling(p, s, w, c, p.cp_q[c], ov, wt);
         apply_site_op(s.Cen, p.pb, s.sbC, bl, br, s.O1);
-        apply_site_op(s.Nxt, p.pb, s.sbC, bj, bj1, s.O2);
-        __syncthreads();
-        store_site(W + s.woff[j], s.Nxt, p.pb, s.sbC, bj, bj1);
+        if constexpr (kMixed) {
+          // the walker itself stays FP64: the operators act on its copy in HBM as well, the FP32
+          // centre only feeds the contractions
+          apply_site_op_stored(W + s.woff[i], bl, br, s.O1);
+          apply_site_op_stored(W + s.woff[j], bj, bj1, s.O2);
+          __syncthreads();
+        } else {
+          apply_site_op(s.Nxt, p.pb, s.sbC, bj, bj1, s.O2);
+          __syncthreads();
+          store_site(W + s.woff[j], s.Nxt, p.pb, s.sbC, bj, bj1);
+        }
         if (rv < j + 1) rv = j + 1;
         ov = num;
+        branches_kept = (j == i + 1) && (p.trace == nullptr);
         if (p.trace != nullptr) {
           // the reference normalises after every coupling: report C of the normalised walker
           // and the normalised overlap (the walk itself does not need the norm)
@@ -494,21 +521,38 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
         // an isometry (sqrt(br)) so that the tensor scales cannot drift over the steps (the
         // overlap takes the same factor), and the left norm environment takes it in:
         // Nl' = sum_s C[s]^T Nl C[s]
+        double *Wi = W + s.woff[i];
         double part = 0.0;
         for (int q = tid; q < bl * br * d; q += kThreads) {
           const int r = q % bl, rest = q / bl, cc = rest % br, sg = rest / br;
-          const double x = s.Cen[sg * s.sbC + r + p.pb * cc];
+          const double x = kMixed ? Wi[q] : (double)s.Cen[sg * s.sbC + r + p.pb * cc];
           part += x * x;
         }
         const double inv = sqrt((double)br / cta_sum(part, s.red));
         for (int q = tid; q < bl * br * d; q += kThreads) {
           const int r = q % bl, rest = q / bl, cc = rest % br, sg = rest / br;
           s.Cen[sg * s.sbC + r + p.pb * cc] *= T(inv);
+          if (kMixed) Wi[q] *= inv;
         }
         ov *= inv;
         nrm_prev *= inv;
+        if (branches_kept) {
+          // the left branches of the final site, without their products: P is linear in the
+          // centre's sigma blocks, so P'[s, t] = inv sum_t' O1(t, t') P[s, t'] (O1 of the last coupling)
+          const T o0 = T(inv * s.O1[0]), o1 = T(inv * s.O1[1]), o2 = T(inv * s.O1[2]), o3 = T(inv * s.O1[3]);
+          for (int q = tid; q < ar * br; q += kThreads) {
+            const int off = q % ar + p.pa * (q / ar);
+#pragma unroll
+            for (int sg = 0; sg < d; ++sg) {
+              T *P0 = s.Pb + sg * s.sbX + off, *P1 = s.Pb + (sg + d) * s.sbX + off;
+              const T x0 = *P0, x1 = *P1;
+              *P0 = o0 * x0 + o2 * x1;
+              *P1 = o1 * x0 + o3 * x1;
+            }
+          }
+        }
         __syncthreads();
-        store_site(W + s.woff[i], s.Cen, p.pb, s.sbC, bl, br);
+        if (!kMixed) store_site(Wi, s.Cen, p.pb, s.sbC, bl, br);
         for (int sg = 0; sg < d; ++sg)
           gemm_t<NP>(bl, br, bl, T(1), Nl, p.pb, false, s.Cen + sg * s.sbC, p.pb, false, T(0), s.Xb + sg * s.sbX,
                      p.pa);
@@ -518,7 +562,7 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
                      sg == 0 ? T(0) : T(1), Nl, p.pb);
         __syncthreads();
         env_update_general<T, NP>(p, s, i, Bi, al, ar, bl, br, s.Cen, p.pb, s.sbC, Fdone[cur], Fdone[1 - cur],
-                                  Fch);
+                                  Fch, branches_kept);
         cur = 1 - cur;
         load_site(s.Cen, p.pb, s.sbC, W + s.woff[i + 1], br, s.bW[i + 2]);
         __syncthreads();
@@ -552,15 +596,17 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
       } else {
         // last site: energy and overlap of the unnormalised walker, then normalise the centre
         env_update_general<T, NP>(p, s, i, Bi, al, 1, bl, 1, s.Cen, p.pb, s.sbC, Fdone[cur], Fdone[1 - cur], Fch);
+        double *Wi = W + s.woff[i];
         double part = 0.0;
         for (int q = tid; q < bl * d; q += kThreads) {  // site L-1: bl x 1 per sigma
           const T *cs = s.Cen + (q / bl) * s.sbC;
-          const double x = cs[q % bl];
+          const double *ws = Wi + (q / bl) * bl;  // the FP64 walker (mixed sweep)
+          const double x = kMixed ? ws[q % bl] : (double)cs[q % bl];
           if (Nl == nullptr) {
             part += x * x;
           } else {  // x (Nl c)_r
             double y = 0.0;
-            for (int k = 0; k < bl; ++k) y += (double)Nl[(q % bl) + p.pb * k] * (double)cs[k];
+            for (int k = 0; k < bl; ++k) y += (double)Nl[(q % bl) + p.pb * k] * (kMixed ? ws[k] : (double)cs[k]);
             part += x * y;
           }
         }
@@ -568,9 +614,13 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
         const double ovr = s.Lenv[0];
         const double en = Fdone[1 - cur][0];
         const double scale = (ovr < 0.0) ? -1.0 / nrm : 1.0 / nrm;
-        for (int q = tid; q < bl * d; q += kThreads) s.Cen[(q / bl) * s.sbC + (q % bl)] *= T(scale);
-        __syncthreads();
-        store_site(W + s.woff[i], s.Cen, p.pb, s.sbC, bl, 1);
+        if (kMixed) {
+          for (int q = tid; q < bl * d; q += kThreads) Wi[q] *= scale;
+        } else {
+          for (int q = tid; q < bl * d; q += kThreads) s.Cen[(q / bl) * s.sbC + (q % bl)] *= T(scale);
+          __syncthreads();
+          store_site(Wi, s.Cen, p.pb, s.sbC, bl, 1);
+        }
         if (tid == 0) {
           const double ovf = fabs(ovr) / nrm;
           const double ew = en / ovr;

@@ -118,10 +118,10 @@ using Smem = SmemT<double>;
 // (environments, site tensors, branches, QR panel) follow them in shared memory when they fit;
 // for large bond dimensions they live in the CTA's global scratch instead (big != nullptr), where
 // the GEMMs read them through L1/L2.  Returns the doubles placed in shared memory; *big_doubles
-// (if given) receives the size of the matrix buffers.
+// (if given) receives the size of the matrix buffers.  mlp: the learned proposal's buffers.
 __host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, int pa, int pb, int pq,
                                               Smem *s, double *base, double *big = nullptr,
-                                              long *big_doubles = nullptr) {
+                                              long *big_doubles = nullptr, bool mlp = false) {
   long off = 0, boff = 0;
   double *dummy;
   auto take = [&](double *&p, long n) {
@@ -153,7 +153,7 @@ __host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, i
     take(b, (L + 2) / 2);
     take(o, L);
     take(q, 1);
-    take(m, 400);
+    take(m, mlp ? 400 : 0);
     if (s) {
       s->bW = reinterpret_cast<int *>(b);
       s->woff = reinterpret_cast<long *>(o);
@@ -161,7 +161,7 @@ __host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, i
       s->mlp = reinterpret_cast<float *>(m);
     }
   }
-  take(s ? s->qprop : dummy, G);
+  take(s ? s->qprop : dummy, mlp ? G : 0);
   take_big(s ? s->Lenv : dummy, (long)pa * maxB);
   take_big(s ? s->Cen : dummy, (long)pb * maxB * d);
   take_big(s ? s->Nxt : dummy, (long)pb * maxB * d);
@@ -183,7 +183,7 @@ __host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, i
 // receives the size of the matrix buffers in floats.
 __host__ __device__ inline long smem_bytes_f32(int L, int maxA, int maxB, int G, int pa, int pb,
                                                SmemT<float> *s, double *base, float *big = nullptr,
-                                               long *big_floats = nullptr) {
+                                               long *big_floats = nullptr, bool mlp = false) {
   long off = 0, boff = 0;  // doubles of the small buffers; floats of the matrix buffers
   double *dummy;
   float *fdummy;
@@ -206,7 +206,7 @@ __host__ __device__ inline long smem_bytes_f32(int L, int maxA, int maxB, int G,
     take(b, (L + 2) / 2);
     take(o, L);
     take(q, 1);
-    take(m, 400);
+    take(m, mlp ? 400 : 0);
     if (s) {
       s->bW = reinterpret_cast<int *>(b);
       s->woff = reinterpret_cast<long *>(o);
@@ -214,7 +214,7 @@ __host__ __device__ inline long smem_bytes_f32(int L, int maxA, int maxB, int G,
       s->mlp = reinterpret_cast<float *>(m);
     }
   }
-  take(s ? s->qprop : dummy, G);
+  take(s ? s->qprop : dummy, mlp ? G : 0);
   float *fbase = reinterpret_cast<float *>(base + off);
   long soff = 0;  // floats placed in shared memory after the small buffers
   auto take_big = [&](float *&p, long n) {
@@ -247,13 +247,15 @@ __host__ __device__ inline long smem_bytes_f32(int L, int maxA, int maxB, int G,
 // matrix buffers do not fit on chip).
 __device__ __forceinline__ void carve(const Dev &p, Smem &s, double *smem_raw) {
   double *big = (p.gwoff >= 0) ? p.scratch + (long)blockIdx.x * p.scr_stride + p.gwoff : nullptr;
-  smem_doubles(p.L, p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw, big);
+  smem_doubles(p.L, p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw, big, nullptr,
+               p.prop_mode != 0 || p.prop_collect != 0);
 }
 // Mixed precision: the CTA's scratch is read as floats with the same element offsets.
 __device__ __forceinline__ void carve(const Dev &p, SmemT<float> &s, double *smem_raw) {
   float *big = (p.gwoff >= 0) ? reinterpret_cast<float *>(p.scratch) + (long)blockIdx.x * p.scr_stride + p.gwoff
                               : nullptr;
-  smem_bytes_f32(p.L, p.maxA, p.maxB, p.G, p.pa, p.pb, &s, smem_raw, big);
+  smem_bytes_f32(p.L, p.maxA, p.maxB, p.G, p.pa, p.pb, &s, smem_raw, big, nullptr,
+                 p.prop_mode != 0 || p.prop_collect != 0);
 }
 
 // Bond dims and site offsets of the walker in `slot` into shared memory.  Ends with a barrier.

@@ -8,7 +8,8 @@ energies and population control stay FP64.  Its error is stated per mode and che
   - TF32 (one pass, 10-bit mantissa operands): E_P of the first step within 2e-3 relative, and the
     median per-walker weight error below 5e-3 (a sampled grid index may flip for a walker whose
     uniform falls within the PDF error of a CDF boundary).
-Over a longer walk the mixed modes' mean projected energy agrees with the FP64 walk's.
+Over longer walks TF32X3 stays on the FP64 trajectory and both modes' mean projected energies agree
+with the FP64 walk's.
 """
 import numpy as np
 import pytest
@@ -84,19 +85,47 @@ def test_precision_option_and_trace():
     eng.walk(1)
 
 
-@pytest.mark.parametrize("precision", [PRECISION_TF32X3, PRECISION_TF32])
-def test_mixed_walk_energy_agrees_with_fp64(precision):
-    """Twenty steps of the 4x4 snake with branching from the same start and random stream: the
-    mean projected energy of the mixed walk agrees with the FP64 walk's to the mode's accuracy
-    (trajectories may part once a sampled index flips, so the comparison is of means)."""
+def test_tf32x3_walk_follows_fp64_trajectory():
+    """Twenty steps of the 4x4 snake (dtau 0.3, heavy branching) from the same start and random
+    stream: with about FP32 accuracy no sampled index flips, so the per-step E_P of the TF32X3
+    walk stays on the FP64 walk's trajectory."""
     z = load_golden("walk_snake4x4_D16_DW8_branch")
     runs = {}
-    for prec in (PRECISION_FP64, precision):
+    for prec in (PRECISION_FP64, PRECISION_TF32X3):
         eng = engine_for(z, prec)
         st = eng.walk(20)
         runs[prec] = np.array([s["E_P"] for s in st])
         w, wt, ov, eh = eng.get_walkers()
         assert np.all(np.isfinite(w)) and np.all(ov > 0)
         eng.close()
-    tol = 1e-5 if precision == PRECISION_TF32X3 else 2e-3
-    assert np.mean(runs[precision]) == pytest.approx(np.mean(runs[PRECISION_FP64]), rel=tol)
+    np.testing.assert_allclose(runs[PRECISION_TF32X3], runs[PRECISION_FP64], rtol=1e-5)
+
+
+@pytest.mark.parametrize("precision", [PRECISION_TF32X3, PRECISION_TF32])
+def test_mixed_walk_energy_agrees_with_fp64(precision):
+    """Thirty steps of 256 walkers of the L=16 chain (D_T = D_W = 16, dtau 0.01) from the same
+    start and random stream: the mean projected energy of the mixed walk agrees with the FP64
+    walk's to the mode's accuracy (a TF32 walk may part from the FP64 trajectory once a sampled
+    index flips, so the comparison is of means)."""
+    z = load_golden("walk_L16D16_DW16")
+    meta = z["meta"]
+    ci, cj, cJ = couplings(z)
+    N = 256
+    rng = np.random.default_rng(7)
+    w0 = z["walker0_init_data"]
+    walkers = w0[None, :] + 1e-3 * rng.standard_normal((N, w0.size))
+    means = {}
+    for prec in (PRECISION_FP64, precision):
+        eng = Engine(L=meta["L"], ci=ci, cj=cj, cJ=cJ, h=0.0, dtau=meta["dtau"], trial_dims=z["trial_ln_dims"],
+                     trial=z["trial_ln_data"], Jvals=[1.0], U=z["U"], S=z["S"], VT=z["VT"], grid=z["grid"],
+                     Ndesired=N, capacity=3 * N, walker_dims=z["walker0_init_dims"])
+        eng.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
+        eng.set_rng(meta["seed"], 0)
+        eng.set_option(OPT_PRECISION, prec)
+        st = eng.walk(30)
+        means[prec] = float(np.mean([s["E_P"] for s in st]))
+        w, wt, ov, eh = eng.get_walkers()
+        assert np.all(np.isfinite(w)) and np.all(ov > 0)
+        eng.close()
+    tol = 1e-6 if precision == PRECISION_TF32X3 else 1e-3
+    assert means[precision] == pytest.approx(means[PRECISION_FP64], rel=tol)

@@ -60,7 +60,7 @@ def test_walk_matches_reference(case, mode):
     """Every case runs the general sweep (the default); chains also run the nearest-neighbour
     sweep.  "global-ws" keeps the matrix work buffers in global scratch (the placement large bond
     dimensions use) instead of shared memory.  The default general sweep skips the per-site QR and
-    left-normalises every 8 steps; "qr-per-site" runs the Householder QR at every site, "qr-free-2"
+    left-normalises every 16 steps; "qr-per-site" runs the Householder QR at every site, "qr-free-2"
     ("qr-free-global-ws") left-normalise every 2 (3) steps, so that steps of both kinds are
     compared."""
     z = load_golden(case)
@@ -192,7 +192,7 @@ def test_autotune_restores_population_and_keeps_trajectory():
 
 
 def test_qr_free_walkers_read_back_left_canonical():
-    """After QR-free steps (default interval 8, so the walkers were not left-normalised by the
+    """After QR-free steps (default interval 16, so the walkers were not left-normalised by the
     walk), mpsqmc_get_walkers returns Walker::setOverlap's state: every site but the last
     left-orthonormal, norm 1, overlaps <Psi_T|phi> > 0 of those tensors."""
     z = load_golden("walk_snake4x4_D16_DW8_branch")
