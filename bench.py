@@ -63,6 +63,9 @@ def parse():
                          "and of the --vn-arms variants, STEPS steps each after their timed steps, from the "
                          "same start and random stream; ratios against the plain walk (default: 300 on the "
                          "default chain64 run, else off)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="N>1: one walk split over the ranks (global population control and walker "
+                         "balancing, mpsqmc_b200.population) instead of N independent replicas")
     ap.add_argument("--vn-arms", default="tf32x3/grid,tf32x3/learned",
                     help="precision/proposal variants compared with the plain FP64 grid walk")
     return ap.parse_args()
@@ -280,7 +283,7 @@ def main():
                            f"dtau={wl.dtau}, Marsaglia(4) grid, FP64; seeded random left-normalised trial of the "
                            f"D_T shape, walkers = trial compressed on the device",
                "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.Ds, "dtau": wl.dtau,
-               "parallelism": f"replicas x{world}", "sweep": args.sweep,
+               "parallelism": f"{'split walk' if args.sharded else 'replicas'} x{world}", "sweep": args.sweep,
                "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
                "canonical_interval": args.canon if args.canon is not None else 16}
     else:
@@ -289,7 +292,7 @@ def main():
                            f"dtau={wl.dtau}, Marsaglia(4) grid, FP64",
                "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.DW, "dtau": wl.dtau,
                "l2": f"population ({wl.Nw * wl.walker.data.size * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
-               "parallelism": f"replicas x{world}", "sweep": args.sweep,
+               "parallelism": f"{'split walk' if args.sharded else 'replicas'} x{world}", "sweep": args.sweep,
                "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
                "canonical_interval": args.canon if args.canon is not None else 16}
 
@@ -344,10 +347,23 @@ def main():
     torch.cuda.synchronize()
     if pg is not None:
         pg.barrier()
+    rw = None
+    if args.sharded and pg is not None:
+        from mpsqmc_b200.population import RankWalk
+        rw = RankWalk(eng, pg, [N] * world, device="cpu")
     with ClockSampler(local) as clk:
-        stats = eng.walk(args.steps)
-        torch.cuda.synchronize()
-        tim = eng.last_timing()
+        if rw is None:
+            stats = eng.walk(args.steps)
+            torch.cuda.synchronize()
+            tim = eng.last_timing()
+        else:
+            # split walk: every step ends in a host exchange, so the device time is the host time
+            # between synchronised ends (max over ranks below)
+            t0 = time.perf_counter()
+            stats = [rw.step() for _ in range(args.steps)]
+            torch.cuda.synchronize()
+            wall = (time.perf_counter() - t0) * 1e3
+            tim = {"total_ms": wall, "step_kernel_ms": wall, "launches": eng.last_timing()["launches"] * args.steps}
     if pg is not None:
         pg.barrier()
     ws_done = sum(s["n_walkers"] for s in stats)
@@ -358,6 +374,8 @@ def main():
 
     vn = None
     vn_compare = args.vn_compare
+    if rw is not None:
+        vn_compare = 0
     if vn_compare is None:
         vn_compare = 300 if (not lattice and args.precision == "fp64" and args.proposal == "grid"
                              and args.walkers is None and args.steps >= 5) else 0

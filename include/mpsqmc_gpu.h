@@ -230,6 +230,29 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
 int mpsqmc_set_option(mpsqmc_ctx *ctx, int option, long value);
 int mpsqmc_get_option(mpsqmc_ctx *ctx, int option, long *value);
 
+/* Walks split over ranks, one context per rank and GPU: the reference's MPI path through
+ * MPSQMC2::Walk (MPSQMC2.cpp:465-511 with USE_MPI_IN_MPSQMC) and PopulationBalancing
+ * (MPSQMC2.cpp:778-934).  A step is mpsqmc_step_propagate on every rank, a sum of the five
+ * local sums over the ranks (the reference's MPI Allreduce calls), then mpsqmc_step_control on
+ * every rank; mpsqmc_walk on one rank is the same as the pair with its own sums.
+ *   mpsqmc_step_propagate: one step's propagation, local energies and energy-history update;
+ *     local_sums = {sum w, sum w E, sum of Ehist/step, sum of (Ehist/step)^2, walker count}.
+ *     A rank may hold no walkers.
+ *   mpsqmc_step_control: statistics from the global sums and ndesired_total (scaling =
+ *     ndesired_total / sum w, E_T, E_P, fluctuation metric), then this rank's population control
+ *     with that scaling.  stats: sum_weight, E_P, E_T, omega and scaling are global, the walker
+ *     counts this rank's.
+ *   mpsqmc_export_walkers / mpsqmc_import_walkers: move the last k walkers (logical order) out
+ *     as records of mpsqmc_record_size doubles (weight, overlap, energy history, bond dims, site
+ *     tensors), or append k records; records are device memory (or memory the device can read
+ *     and write).  Exported walkers are left-normalised first. */
+int mpsqmc_step_propagate(mpsqmc_ctx *ctx, double local_sums[5]);
+int mpsqmc_step_control(mpsqmc_ctx *ctx, const double global_sums[5], long ndesired_total,
+                        mpsqmc_step_stats *stats);
+long mpsqmc_record_size(const mpsqmc_ctx *ctx);
+int mpsqmc_export_walkers(mpsqmc_ctx *ctx, int k, double *records);
+int mpsqmc_import_walkers(mpsqmc_ctx *ctx, int k, const double *records);
+
 /* Learned proposal (no counterpart in the reference).  The network maps 32 features of a
  * coupling (4 C_kl / ov and 4 M / ov: the overlap-ratio coefficients and the 16 closures of the
  * environment branches) through two hidden layers of 128 (ReLU) to logits over the G grid points.

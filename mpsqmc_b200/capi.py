@@ -39,7 +39,8 @@ EXPORTED = [
     "mpsqmc_get_trace", "mpsqmc_last_timing", "mpsqmc_local_energy_noalloc", "mpsqmc_set_step",
     "mpsqmc_set_option", "mpsqmc_get_option", "mpsqmc_set_walkers_dims", "mpsqmc_get_walker_dims",
     "mpsqmc_compress_walkers", "mpsqmc_autotune", "mpsqmc_proposal_params", "mpsqmc_proposal_loss_grad",
-    "mpsqmc_proposal_stats",
+    "mpsqmc_proposal_stats", "mpsqmc_step_propagate", "mpsqmc_step_control", "mpsqmc_record_size",
+    "mpsqmc_export_walkers", "mpsqmc_import_walkers",
 ]
 
 
@@ -130,6 +131,11 @@ def load(build_if_missing: bool = True):
         "mpsqmc_proposal_params": (C.c_int, [P, fp, fp, C.POINTER(C.c_long)]),
         "mpsqmc_proposal_loss_grad": (C.c_int, [P, C.c_int, fp, fp, dp, fp]),
         "mpsqmc_proposal_stats": (C.c_int, [P, dp, ip]),
+        "mpsqmc_step_propagate": (C.c_int, [P, dp]),
+        "mpsqmc_step_control": (C.c_int, [P, dp, C.c_long, C.POINTER(StepStats)]),
+        "mpsqmc_record_size": (C.c_long, [P]),
+        "mpsqmc_export_walkers": (C.c_int, [P, C.c_int, P]),
+        "mpsqmc_import_walkers": (C.c_int, [P, C.c_int, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -268,12 +274,44 @@ class Engine:
         check(self.lib.mpsqmc_energy(self._ctx, C.byref(e)))
         return e.value
 
+    @staticmethod
+    def _stats(s):
+        return dict(step=s.step, n_walkers=s.n_walkers, n_after=s.n_after, sum_weight=s.sum_weight,
+                    avg_weight=s.avg_weight, E_P=s.E_P, E_T=s.E_T, omega=s.omega, scaling=s.scaling, draws=s.draws)
+
     def walk(self, nsteps: int):
         st = (StepStats * max(nsteps, 1))()
         check(self.lib.mpsqmc_walk(self._ctx, nsteps, st))
-        return [dict(step=s.step, n_walkers=s.n_walkers, n_after=s.n_after, sum_weight=s.sum_weight,
-                     avg_weight=s.avg_weight, E_P=s.E_P, E_T=s.E_T, omega=s.omega, scaling=s.scaling,
-                     draws=s.draws) for s in st[:nsteps]]
+        return [self._stats(s) for s in st[:nsteps]]
+
+    # walks split over ranks
+    def step_propagate(self):
+        """One step's propagation; this population's five sums (Sum w, Sum w E, Sum e, Sum e^2, N)."""
+        out = np.zeros(5)
+        check(self.lib.mpsqmc_step_propagate(self._ctx, _dp(out)))
+        return out
+
+    def step_control(self, global_sums, ndesired_total: int):
+        g = np.ascontiguousarray(global_sums, dtype=np.float64)
+        st = StepStats()
+        check(self.lib.mpsqmc_step_control(self._ctx, _dp(g), int(ndesired_total), C.byref(st)))
+        return self._stats(st)
+
+    def record_size(self) -> int:
+        return int(self.lib.mpsqmc_record_size(self._ctx))
+
+    def export_walkers(self, k: int, records_ptr: int):
+        """The last k walkers into k records at a device address (e.g. a torch tensor's data_ptr())."""
+        check(self.lib.mpsqmc_export_walkers(self._ctx, int(k), C.c_void_p(records_ptr)))
+
+    def import_walkers(self, k: int, records_ptr: int):
+        check(self.lib.mpsqmc_import_walkers(self._ctx, int(k), C.c_void_p(records_ptr)))
+
+    @property
+    def n_walkers(self) -> int:
+        n = C.c_int(0)
+        check(self.lib.mpsqmc_get_walkers(self._ctx, C.byref(n), None, None, None, None))
+        return n.value
 
     def set_step(self, completed_steps: int):
         check(self.lib.mpsqmc_set_step(self._ctx, completed_steps))

@@ -24,6 +24,7 @@
 #include "compress.cuh"
 #include "legacy.cuh"
 #include "proposal.cuh"
+#include "population.cuh"
 
 namespace {
 
@@ -132,6 +133,10 @@ struct mpsqmc_ctx {
   int resample = MPSQMC_RESAMPLE_THRESHOLD;
   int canon_interval = 16;              // QR-free general sweep, LeftNormalize every K steps (0: off)
   bool gauge_dirty = false;             // the last step left the walkers un-normalised (QR-free)
+  // walks split over ranks: between mpsqmc_step_propagate and mpsqmc_step_control
+  bool split_pending = false, split_canon = false;
+  int split_launches = 0;
+  double *d_sums = nullptr;             // [0..4] this rank's sums, [8..13] the global ones
   long nloff = 0;                       // its left norm environment inside a CTA's scratch
   int *d_ncop = nullptr;                // copies per walker in the branching step
   int *d_wdims = nullptr;               // per slot: the walker's bond dims [capacity][L+1]
@@ -319,7 +324,7 @@ int check_err(mpsqmc_ctx *c) {
 }
 
 void free_all(mpsqmc_ctx *c) {
-  void *ptrs[] = {c->d_pw, c->d_pm, c->d_pv, c->d_pg, c->d_pwb, c->d_pt, c->d_pb, c->d_ploss, c->d_pfeat,
+  void *ptrs[] = {c->d_sums, c->d_pw, c->d_pm, c->d_pv, c->d_pg, c->d_pwb, c->d_pt, c->d_pb, c->d_ploss, c->d_pfeat,
                   c->d_ptarget, c->d_ph1, c->d_ph2, c->d_pz, c->d_pdz, c->d_pdh2, c->d_pdh1, c->d_trial32, c->d_aT, c->d_bW, c->d_toff, c->d_woff, c->d_roff, c->d_nroff, c->d_trial, c->d_walkers,
                   c->d_slot_of, c->d_slot_new, c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
                   c->d_flag_pos, c->d_ncur, c->d_weight, c->d_overlap, c->d_ehist, c->d_energy,
@@ -1017,9 +1022,12 @@ static int enqueue_legacy_step(mpsqmc_ctx *c, int *launches) {
   CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(int) * mq::kNumCtr, c->stream));
   // one uniform per walker for the term choice (MPSQMC.cpp:342), in walker order
   mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, c->d_ncur, 0, 1, c->d_uni);
-  CK(cudaEventRecordWithFlags(c->ev[0], c->stream, cudaEventRecordExternal));
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(c->stream, &cap));
+  const unsigned evflags = (cap == cudaStreamCaptureStatusActive) ? cudaEventRecordExternal : 0u;
+  CK(cudaEventRecordWithFlags(c->ev[0], c->stream, evflags));
   mq::legacy_step_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p, lp);
-  CK(cudaEventRecordWithFlags(c->ev[1], c->stream, cudaEventRecordExternal));
+  CK(cudaEventRecordWithFlags(c->ev[1], c->stream, evflags));
   // LeftNormalize + overlap + sign of the walkers a term hit (MPSQMC.cpp:355-362)
   mq::Dev ps = p;
   ps.sel = c->d_changed;
@@ -1043,8 +1051,10 @@ static int enqueue_legacy_step(mpsqmc_ctx *c, int *launches) {
 
 // canon: the QR-free sweep's step that also restores the left-canonical form (LeftNormalize,
 // overlap and sign of Walker::setOverlap) after the couplings.
-static int enqueue_step(mpsqmc_ctx *c, int *launches, bool canon) {
-  if (c->projector == MPSQMC_PROJECTOR_MPO_TERMS) return enqueue_legacy_step(c, launches);
+static int enqueue_control(mpsqmc_ctx *c, const double *ext, int *launches);
+
+// The propagation part of a step: everything before the statistics.
+static int enqueue_propagation(mpsqmc_ctx *c, int *launches, bool canon) {
   mq::Dev p = make_dev(c);
   const int grid = c->max_ctas;
   CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(int) * mq::kNumCtr, c->stream));
@@ -1056,8 +1066,11 @@ static int enqueue_step(mpsqmc_ctx *c, int *launches, bool canon) {
     n += 1;
   }
   // external event records: they become event-record nodes under capture, so they time the
-  // step kernel inside the graph
-  CK(cudaEventRecordWithFlags(c->ev[0], c->stream, cudaEventRecordExternal));
+  // step kernel inside the graph (outside a capture they are plain records)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(c->stream, &cap));
+  const unsigned evflags = (cap == cudaStreamCaptureStatusActive) ? cudaEventRecordExternal : 0u;
+  CK(cudaEventRecordWithFlags(c->ev[0], c->stream, evflags));
   const bool gen = general_sweep(c);
   if (mixed(c)) {
     if (c->precision == MPSQMC_PRECISION_TF32)
@@ -1068,7 +1081,7 @@ static int enqueue_step(mpsqmc_ctx *c, int *launches, bool canon) {
     mq::walker_step_general_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
   else
     mq::walker_step_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
-  CK(cudaEventRecordWithFlags(c->ev[1], c->stream, cudaEventRecordExternal));
+  CK(cudaEventRecordWithFlags(c->ev[1], c->stream, evflags));
   if (field) {
     // single-site propagator after the couplings, setOverlap, and the local energy of the
     // resulting state (MPSQMC2.cpp:597-598, then 698)
@@ -1087,8 +1100,25 @@ static int enqueue_step(mpsqmc_ctx *c, int *launches, bool canon) {
     const int rc = enqueue_training(c, c->d_ncur, true, &n);
     if (rc) return rc;
   }
+  CK(cudaGetLastError());
+  *launches = n - 5;  // the five statistics and branching launches are enqueue_control's
+  return 0;
+}
+
+static int enqueue_step(mpsqmc_ctx *c, int *launches, bool canon) {
+  if (c->projector == MPSQMC_PROJECTOR_MPO_TERMS) return enqueue_legacy_step(c, launches);
+  int a = 0, b = 0;
+  int rc = enqueue_propagation(c, &a, canon);
+  if (!rc) rc = enqueue_control(c, nullptr, &b);
+  *launches = a + b;
+  return rc;
+}
+
+// Statistics, population control and the step's read-back (ext: sums over all ranks, or nullptr).
+static int enqueue_control(mpsqmc_ctx *c, const double *ext, int *launches) {
+  mq::Dev p = make_dev(c);
   mq::stats_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->Ndesired, c->dtau, 1, c->d_flag_pos, c->d_sw,
-                                              c->pc_interval, c->resample);
+                                              c->pc_interval, c->resample, ext);
   mq::mt_generate_kernel<<<1, 1024, 0, c->stream>>>(c->d_mt, &c->d_sd->n_flag, 0, 1, c->d_ubr);
   mq::branch_kernel<<<1, 1024, 0, c->stream>>>(p, c->d_sd, c->d_flag_pos, c->d_sw, c->d_ubr, c->d_slot_new,
                                                c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
@@ -1099,7 +1129,7 @@ static int enqueue_step(mpsqmc_ctx *c, int *launches, bool canon) {
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->h_sd, c->d_sd, sizeof(mq::StepDev), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  *launches = n;
+  *launches = 5;
   return 0;
 }
 
@@ -1122,6 +1152,33 @@ static int build_graph(mpsqmc_ctx *c, bool canon) {
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(MPSQMC_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   c->graph_trace = c->trace_on;
+  return 0;
+}
+
+// Host bookkeeping after a step's read-back: errors, random-stream position, population size.
+static int finish_step(mpsqmc_ctx *c, int N, int step, bool canon, const mq::StepDev &sd, int err,
+                       mpsqmc_step_stats *o) {
+  if (err & mq::kErrNumeric) return fail(MPSQMC_E_NUMERIC, "non-finite weight, overlap or energy");
+  if (err & mq::kErrCapacity) return fail(MPSQMC_E_CAPACITY, "population control exceeded the walker capacity");
+  const int per_walker = (c->projector == MPSQMC_PROJECTOR_MPO_TERMS) ? 1 : c->nC;
+  const unsigned long long dr = (unsigned long long)N * per_walker + (unsigned long long)sd.n_flag;
+  c->draws += dr;
+  c->last_n_before = N;
+  c->last_n_after = sd.n_new;
+  c->n_cur = sd.n_new;
+  c->gauge_dirty = qr_free(c) && !canon && c->h == 0.0;
+  if (o) {
+    o->step = step;
+    o->n_walkers = N;
+    o->n_after = sd.n_new;
+    o->sum_weight = sd.sumw;
+    o->avg_weight = N > 0 ? sd.sumw / N : 0.0;
+    o->E_P = sd.EP;
+    o->E_T = sd.ET;
+    o->omega = sd.omega;
+    o->scaling = sd.scaling;
+    o->draws = dr;
+  }
   return 0;
 }
 
@@ -1162,28 +1219,8 @@ int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
     kernel_ms += ms;
-    if (err & mq::kErrNumeric) return fail(MPSQMC_E_NUMERIC, "non-finite weight, overlap or energy");
-    if (err & mq::kErrCapacity) return fail(MPSQMC_E_CAPACITY, "population control exceeded the walker capacity");
-    const int per_walker = (c->projector == MPSQMC_PROJECTOR_MPO_TERMS) ? 1 : c->nC;
-    const unsigned long long dr = (unsigned long long)N * per_walker + (unsigned long long)sd.n_flag;
-    c->draws += dr;
-    c->last_n_before = N;
-    c->last_n_after = sd.n_new;
-    c->n_cur = sd.n_new;
-    c->gauge_dirty = qr_free(c) && !canon && c->h == 0.0;
-    if (stats) {
-      mpsqmc_step_stats &o = stats[s];
-      o.step = step;
-      o.n_walkers = N;
-      o.n_after = sd.n_new;
-      o.sum_weight = sd.sumw;
-      o.avg_weight = sd.sumw / N;
-      o.E_P = sd.EP;
-      o.E_T = sd.ET;
-      o.omega = sd.omega;
-      o.scaling = sd.scaling;
-      o.draws = dr;
-    }
+    const int rc = finish_step(c, N, step, canon, sd, err, stats ? &stats[s] : nullptr);
+    if (rc) return rc;
     if (sd.n_new == 0) return fail(MPSQMC_E_EXTINCT, "population control removed every walker");
   }
   CK(cudaEventRecord(c->ev[3], c->stream));
@@ -1480,6 +1517,88 @@ int mpsqmc_get_option(mpsqmc_ctx *c, int option, long *value) {
     default:
       return fail(MPSQMC_E_ARG, "unknown option");
   }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Walks split over ranks (population.cuh)
+// ---------------------------------------------------------------------------------------------
+int mpsqmc_step_propagate(mpsqmc_ctx *c, double local_sums[5]) {
+  if (!c || !local_sums) return fail(MPSQMC_E_ARG, "null argument");
+  if (c->projector != MPSQMC_PROJECTOR_TROTTER)
+    return fail(MPSQMC_E_UNSUPPORTED, "split steps run the Trotter projector");
+  if (c->split_pending) return fail(MPSQMC_E_ARG, "mpsqmc_step_control is due first");
+  if (c->trace_on) return fail(MPSQMC_E_UNSUPPORTED, "the per-coupling trace is recorded by mpsqmc_walk only");
+  CK(cudaSetDevice(c->device));
+  if (!c->d_sums && dalloc(&c->d_sums, 16)) return MPSQMC_E_CUDA;
+  const int step = ++c->step_count;
+  c->split_canon = qr_free(c) && step % canon_every(c) == 0;
+  int n = 0;
+  int rc = enqueue_propagation(c, &n, c->split_canon);
+  if (rc) return rc;
+  mq::local_sums_kernel<<<1, 1024, 0, c->stream>>>(make_dev(c), c->d_sd, c->d_sums);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(local_sums, c->d_sums, sizeof(double) * mq::kNumSums, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->split_pending = true;
+  c->split_launches = n + 1;
+  return check_err(c);
+}
+
+int mpsqmc_step_control(mpsqmc_ctx *c, const double global_sums[5], long ndesired_total, mpsqmc_step_stats *stats) {
+  if (!c || !global_sums) return fail(MPSQMC_E_ARG, "null argument");
+  if (!c->split_pending) return fail(MPSQMC_E_ARG, "mpsqmc_step_propagate is due first");
+  if (ndesired_total < 1 || !(global_sums[0] > 0.0) || !(global_sums[4] >= 1.0))
+    return fail(MPSQMC_E_ARG, "global sums need a positive weight sum, walker count and target");
+  CK(cudaSetDevice(c->device));
+  double ext[6];
+  std::copy(global_sums, global_sums + 5, ext);
+  ext[5] = (double)ndesired_total;
+  CK(cudaMemcpyAsync(c->d_sums + 8, ext, sizeof ext, cudaMemcpyHostToDevice, c->stream));
+  const int N = c->n_cur;
+  int n = 0;
+  int rc = enqueue_control(c, c->d_sums + 8, &n);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  c->split_pending = false;
+  c->last_launches = c->split_launches + n;
+  return finish_step(c, N, c->step_count, c->split_canon, *c->h_sd, *c->h_err, stats);
+}
+
+long mpsqmc_record_size(const mpsqmc_ctx *c) { return c ? mq::record_doubles(c->L, c->wsize) : -1; }
+
+int mpsqmc_export_walkers(mpsqmc_ctx *c, int k, double *records) {
+  if (!c || (!records && k > 0)) return fail(MPSQMC_E_ARG, "null argument");
+  if (k < 0 || k > c->n_cur) return fail(MPSQMC_E_ARG, "export count outside [0, walkers]");
+  if (c->split_pending) return fail(MPSQMC_E_ARG, "mpsqmc_step_control is due first");
+  if (k == 0) return 0;
+  int rc = restore_canonical(c);
+  if (rc) return rc;
+  CK(cudaSetDevice(c->device));
+  mq::Dev p = make_dev(c);
+  mq::export_walkers_kernel<<<std::min(k, 4 * c->sm_count), 256, 0, c->stream>>>(p, c->d_sd, k,
+                                                                                  mq::record_doubles(c->L, c->wsize),
+                                                                                  records);
+  mq::population_count_kernel<<<1, 256, 0, c->stream>>>(c->d_sd, c->d_ncur, c->d_slot_of, c->d_free, -k);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  c->n_cur -= k;
+  return 0;
+}
+
+int mpsqmc_import_walkers(mpsqmc_ctx *c, int k, const double *records) {
+  if (!c || (!records && k > 0)) return fail(MPSQMC_E_ARG, "null argument");
+  if (k < 0 || c->n_cur + k > c->capacity) return fail(MPSQMC_E_CAPACITY, "import beyond the walker capacity");
+  if (c->split_pending) return fail(MPSQMC_E_ARG, "mpsqmc_step_control is due first");
+  if (k == 0) return 0;
+  CK(cudaSetDevice(c->device));
+  mq::Dev p = make_dev(c);
+  mq::import_walkers_kernel<<<std::min(k, 4 * c->sm_count), 256, 0, c->stream>>>(
+      p, c->d_sd, c->d_free, c->d_slot_of, k, mq::record_doubles(c->L, c->wsize), records);
+  mq::population_count_kernel<<<1, 256, 0, c->stream>>>(c->d_sd, c->d_ncur, c->d_slot_of, c->d_free, k);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  c->n_cur += k;
+  return 0;
 }
 
 int mpsqmc_proposal_params(mpsqmc_ctx *c, float *out, const float *in, long *n_params) {

@@ -896,9 +896,11 @@ enum : int { kResampleThreshold = 0, kResampleComb = 1, kResampleLegacy = 2 };
 // advances sd->step, so a captured step graph needs no per-step argument.
 // Uniforms needed by the branching (n_flag): one per walker whose scaled weight leaves
 // [0.25, 1.5] (threshold), one per resampling (comb), none on steps without population control.
+// ext (a walk split over ranks): the sums of all ranks' walkers [Sum w, Sum w E, Sum e, Sum e^2,
+// N, Ndesired of all ranks] replace this rank's own, whose history local_sums_kernel updated.
 __global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Ndesired, double dtau,
                                                      int update_history, int *flag_pos, double *sw_out,
-                                                     int interval, int mode) {
+                                                     int interval, int mode, const double *ext = nullptr) {
   const int step = sd->step + 1;
   const bool branch_now = (step % interval) == 0;
   __shared__ double dbuf[32];
@@ -910,14 +912,15 @@ __global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Nde
     sw += wt;
     num += wt * p.energy[w];
   }
-  const double sumw_full = block_sum_d(sw, dbuf);
-  const double numer = block_sum_d(num, dbuf);
+  const double sumw_full = ext ? ext[0] : block_sum_d(sw, dbuf);
+  const double numer = ext ? ext[1] : block_sum_d(num, dbuf);
   // the MPO-term projector sums the weights into an int (MPSQMC.cpp:364-366)
   const double sumw = (mode == kResampleLegacy) ? (double)(int)sumw_full : sumw_full;
-  const double avgW = sumw / N;
-  const double scaling = Ndesired / (N * avgW);
+  const double Nall = ext ? ext[4] : (double)N;
+  const double avgW = sumw / Nall;
+  const double scaling = (ext ? ext[5] : (double)Ndesired) / (Nall * avgW);
   double se = 0.0, se2 = 0.0;
-  if (update_history) {
+  if (update_history && !ext) {
     for (int w = threadIdx.x; w < N; w += 1024) {
       const int slot = p.slot_of[w];
       const double h = p.ehist[slot] + p.energy[w];
@@ -927,8 +930,8 @@ __global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Nde
       se2 += e * e;
     }
   }
-  const double sE = block_sum_d(se, dbuf);
-  const double sE2 = block_sum_d(se2, dbuf);
+  const double sE = ext ? ext[2] : block_sum_d(se, dbuf);
+  const double sE2 = ext ? ext[3] : block_sum_d(se2, dbuf);
   // flags: walkers whose scaled weight leaves [0.25, 1.5] draw one uniform, in walker order
   int nflag_total = 0;
   for (int base = 0; base < N; base += 1024) {
@@ -950,7 +953,7 @@ __global__ void __launch_bounds__(1024) stats_kernel(Dev p, StepDev *sd, int Nde
     sd->scaling = scaling;
     sd->ET = log(scaling) / dtau;
     sd->EP = numer / sumw_full;
-    sd->omega = update_history ? (sE2 - sE * sE / N) / N : 0.0;
+    sd->omega = update_history ? (sE2 - sE * sE / Nall) / Nall : 0.0;
     sd->n_flag = (branch_now && mode == kResampleComb) ? 1 : nflag_total;
     if (!(isfinite(sumw) && sumw > 0.0 && isfinite(numer))) atomicOr(p.err, kErrNumeric);
   }
