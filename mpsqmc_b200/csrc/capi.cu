@@ -90,7 +90,7 @@ struct mpsqmc_ctx {
   int L = 0, d = 2, nC = 0, G = 0, nJ = 0, Ndesired = 0, capacity = 0;
   double dtau = 0.0, h = 0.0;
   std::vector<int> aT, bW;
-  std::vector<long> toff, woff, roff, nroff;
+  std::vector<long> toff, woff, roff, nroff, zoff;
   long wsize = 0, wstride = 0, scr_stride = 0, foff = 0, gwoff = -1;
   long scr_base = 0;                    // scratch doubles per CTA before the matrix work buffers
   long all_doubles = 0, big_doubles = 0;  // work buffers: all of them / the matrix ones
@@ -118,7 +118,7 @@ struct mpsqmc_ctx {
         *d_pdz = nullptr, *d_pdh2 = nullptr, *d_pdh1 = nullptr;
   // device memory
   int *d_aT = nullptr, *d_bW = nullptr;
-  long *d_toff = nullptr, *d_woff = nullptr, *d_roff = nullptr, *d_nroff = nullptr;
+  long *d_toff = nullptr, *d_woff = nullptr, *d_roff = nullptr, *d_nroff = nullptr, *d_zoff = nullptr;
   double *d_trial = nullptr, *d_walkers = nullptr;
   int *d_slot_of = nullptr, *d_slot_new = nullptr, *d_free = nullptr, *d_copy_src = nullptr,
       *d_copy_dst = nullptr, *d_parent = nullptr, *d_flag_pos = nullptr, *d_ncur = nullptr;
@@ -235,6 +235,7 @@ mq::Dev make_dev(mpsqmc_ctx *c) {
   p.scr_stride = c->scr_stride;
   p.roff = c->d_roff;
   p.nroff = c->d_nroff;
+  p.zoff = c->d_zoff;
   p.foff = c->foff;
   p.trace = c->trace_on ? c->d_trace : nullptr;
   p.err = c->d_err;
@@ -324,7 +325,7 @@ int check_err(mpsqmc_ctx *c) {
 }
 
 void free_all(mpsqmc_ctx *c) {
-  void *ptrs[] = {c->d_sums, c->d_pw, c->d_pm, c->d_pv, c->d_pg, c->d_pwb, c->d_pt, c->d_pb, c->d_ploss, c->d_pfeat,
+  void *ptrs[] = {c->d_zoff, c->d_sums, c->d_pw, c->d_pm, c->d_pv, c->d_pg, c->d_pwb, c->d_pt, c->d_pb, c->d_ploss, c->d_pfeat,
                   c->d_ptarget, c->d_ph1, c->d_ph2, c->d_pz, c->d_pdz, c->d_pdh2, c->d_pdh1, c->d_trial32, c->d_aT, c->d_bW, c->d_toff, c->d_woff, c->d_roff, c->d_nroff, c->d_trial, c->d_walkers,
                   c->d_slot_of, c->d_slot_new, c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
                   c->d_flag_pos, c->d_ncur, c->d_weight, c->d_overlap, c->d_ehist, c->d_energy,
@@ -370,7 +371,8 @@ int layout_workspace(mpsqmc_ctx *c, bool force_global) {
   if (c->smem_bytes > c->smem_optin)
     return fail(MPSQMC_E_UNSUPPORTED, "grid too large for the shared-memory budget of one CTA");
   const void *kernels[] = {(const void *)mq::walker_step_kernel, (const void *)mq::set_overlap_kernel,
-                           (const void *)mq::energy_kernel, (const void *)mq::walker_step_general_kernel,
+                           (const void *)mq::energy_kernel, (const void *)mq::walker_step_general_kernel<true>,
+                           (const void *)mq::walker_step_general_kernel<false>,
                            (const void *)mq::energy_general_kernel, (const void *)mq::legacy_step_kernel};
   for (const void *k : kernels)
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes));
@@ -383,11 +385,12 @@ int layout_workspace(mpsqmc_ctx *c, bool force_global) {
   const long mixed_all = mq::smem_bytes_f32(c->L, c->maxA, c->maxB, c->G, c->pa, c->pb, nullptr, nullptr, nullptr,
                                             &big_floats, mlp);
   c->smem_bytes_mixed = global ? (size_t)(mixed_all - (long)sizeof(float) * big_floats) : (size_t)mixed_all;
-  const void *mk[] = {(const void *)mq::walker_step_mixed_kernel<1>, (const void *)mq::walker_step_mixed_kernel<3>};
+  const void *mk[] = {(const void *)mq::walker_step_mixed_kernel<1, true>, (const void *)mq::walker_step_mixed_kernel<3, true>,
+                      (const void *)mq::walker_step_mixed_kernel<1, false>, (const void *)mq::walker_step_mixed_kernel<3, false>};
   for (const void *k : mk)
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes_mixed));
   int occm = 1;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occm, mq::walker_step_mixed_kernel<3>, mq::kThreads,
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occm, mq::walker_step_mixed_kernel<3, true>, mq::kThreads,
                                                    c->smem_bytes_mixed));
   c->max_ctas_mixed = std::max(1, std::min(occm, 2)) * c->sm_count;
   return 0;
@@ -572,7 +575,15 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   c->choff = ro + 2L * 4 * c->maxA * c->maxB;
   c->loff = c->choff + (2L + 3L * nslots) * c->maxA * c->maxB;
   c->nloff = c->loff + ((2L * (3L * c->nC + L + 1) + 31) & ~31L);
-  c->scr_base = c->nloff + (((long)c->pb * c->maxB + 31) & ~31L);
+  {  // nearest-neighbour couplings: right branches Z[k] (4 blocks of a_k x b_k) of every site
+    long zo = c->nloff + (((long)c->pb * c->maxB + 31) & ~31L);
+    c->zoff.resize(L);
+    for (int k = 0; k < L; ++k) {
+      c->zoff[k] = zo;
+      if (nn) zo += (4L * c->aT[k] * c->bW[k] + 3) & ~3L;
+    }
+    c->scr_base = zo;
+  }
   for (int s = 0; s < 2; ++s)
     for (int t = 0; t < 2; ++t) {
       c->opSx[s + 2 * t] = op_sx(d, s, t);
@@ -602,7 +613,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   const int cap = c->capacity;
   int rc = 0;
   rc |= dalloc(&c->d_aT, L + 1) | dalloc(&c->d_bW, L + 1) | dalloc(&c->d_toff, L) | dalloc(&c->d_woff, L) |
-        dalloc(&c->d_roff, L + 1) | dalloc(&c->d_nroff, L + 1) | dalloc(&c->d_trial, to) | dalloc(&c->d_walkers, (size_t)cap * c->wstride) |
+        dalloc(&c->d_roff, L + 1) | dalloc(&c->d_nroff, L + 1) | dalloc(&c->d_zoff, L) | dalloc(&c->d_trial, to) | dalloc(&c->d_walkers, (size_t)cap * c->wstride) |
         dalloc(&c->d_slot_of, cap) | dalloc(&c->d_slot_new, cap) | dalloc(&c->d_free, cap) |
         dalloc(&c->d_copy_src, cap) | dalloc(&c->d_copy_dst, cap) | dalloc(&c->d_parent, cap) |
         dalloc(&c->d_flag_pos, cap) | dalloc(&c->d_ncur, 1) | dalloc(&c->d_weight, cap) |
@@ -634,6 +645,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
             up(c->d_toff, c->toff.data(), sizeof(long) * L) && up(c->d_woff, c->woff.data(), sizeof(long) * L) &&
             up(c->d_roff, c->roff.data(), sizeof(long) * (L + 1)) &&
             up(c->d_nroff, c->nroff.data(), sizeof(long) * (L + 1)) &&
+            up(c->d_zoff, c->zoff.data(), sizeof(long) * L) &&
             up(c->d_trial, cfg->trial, sizeof(double) * to) && up(c->d_trial32, trial32.data(), sizeof(float) * to) &&
             up(c->d_bond_c, bond_c.data(), sizeof(int) * (L - 1)) &&
             up(c->d_bond_j, bond_j.data(), sizeof(int) * (L - 1)) &&
@@ -1073,13 +1085,19 @@ static int enqueue_propagation(mpsqmc_ctx *c, int *launches, bool canon) {
   CK(cudaEventRecordWithFlags(c->ev[0], c->stream, evflags));
   const bool gen = general_sweep(c);
   if (mixed(c)) {
-    if (c->precision == MPSQMC_PRECISION_TF32)
-      mq::walker_step_mixed_kernel<1><<<c->max_ctas_mixed, mq::kThreads, c->smem_bytes_mixed, c->stream>>>(p);
-    else
-      mq::walker_step_mixed_kernel<3><<<c->max_ctas_mixed, mq::kThreads, c->smem_bytes_mixed, c->stream>>>(p);
-  } else if (gen)
-    mq::walker_step_general_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
-  else
+    const int g = c->max_ctas_mixed;
+    const size_t sm = c->smem_bytes_mixed;
+    if (c->precision == MPSQMC_PRECISION_TF32) {
+      if (c->nn) mq::walker_step_mixed_kernel<1, true><<<g, mq::kThreads, sm, c->stream>>>(p);
+      else mq::walker_step_mixed_kernel<1, false><<<g, mq::kThreads, sm, c->stream>>>(p);
+    } else {
+      if (c->nn) mq::walker_step_mixed_kernel<3, true><<<g, mq::kThreads, sm, c->stream>>>(p);
+      else mq::walker_step_mixed_kernel<3, false><<<g, mq::kThreads, sm, c->stream>>>(p);
+    }
+  } else if (gen) {
+    if (c->nn) mq::walker_step_general_kernel<true><<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+    else mq::walker_step_general_kernel<false><<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+  } else
     mq::walker_step_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
   CK(cudaEventRecordWithFlags(c->ev[1], c->stream, evflags));
   if (field) {

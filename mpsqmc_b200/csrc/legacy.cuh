@@ -81,9 +81,8 @@ __global__ void __launch_bounds__(kThreads, 1) legacy_step_kernel(Dev p, LegacyD
           for (int q = 0; q < kN2; ++q)
             transfer_in_place(p, s, Bm, am, am1, bm, bm1, s.Nxt, p.pb, s.sbC, s.Pb + q * s.sbX, p.pa);
         }
-        load_site(s.Nxt, p.pb, s.sbC, W + s.woff[j], s.bW[j], s.bW[j + 1]);
         __syncthreads();
-        closures(p, s, j, scr + p.roff[j + 1]);
+        closures(p, s, j, W, scr);
         if (tid < 3) {  // <Psi_T| A_i A_j |phi> for A = Sx, iSy, Sz
           const double *op = legacy_op(p, tid + 1);
           double v = 0.0;

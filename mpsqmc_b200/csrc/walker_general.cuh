@@ -8,7 +8,9 @@
 //      still-valid one when an earlier coupling changed a site beyond j;
 //   2. four left branches P[s,t] = B_i[s]^T L C[t] on the centre, carried through the middle
 //      sites i+1..j-1 by ordinary transfer steps, four right branches at j and 16 closures give
-//      C_kl = <Psi_T|(sqrt(s_k)U_k)_i (sqrt(s_l)V_l)_j|phi> (MPSQMC2.cpp:540-549);
+//      C_kl = <Psi_T|(sqrt(s_k)U_k)_i (sqrt(s_l)V_l)_j|phi> (MPSQMC2.cpp:540-549); for
+//      nearest-neighbour couplings the right branches come from the right-environment sweep, so
+//      the closures are dot products only;
 //   3. PDF, weight, CDF sample (551-588), O1 on the centre and O2 on site j (MPSstate.cpp:575-633).
 // Then one Householder QR moves the centre to i+1, and the final site i enters the left
 // environments: the trial overlap and the energy channels of the compact MPO of
@@ -51,8 +53,11 @@ __device__ __forceinline__ const T *trial_of(const Dev &p) {
 }
 
 // R[k] = sum_s B_k[s] R[k+1] A_k[s]^T from the walker's site k as stored in global memory.
-// Uses Nxt and Xb.  Ends with a barrier.
-template <typename T, int NP = 0>
+// With ZB (nearest-neighbour couplings) also the right branches of site k,
+// Z[s' + 2 t'] = B_k[s'] R[k+1] A_k[t']^T (a_k x b_k, ld a_k, block stride a_k * (the slot
+// layout's b_k)), and R[k] = Z[0] + Z[3]: the coupling (k-1, k) then closes its left branches
+// against Z[k] without products of its own (closures).  Uses Nxt and Xb.  Ends with a barrier.
+template <typename T, int NP = 0, bool ZB = false>
 static __device__ void right_env_step(const Dev &p, SmemT<T> &s, const double *W, T *scr, int k) {
   const int d = kMaxD;
   const int al = p.aT[k], ar = p.aT[k + 1], bl = s.bW[k], br = s.bW[k + 1];
@@ -60,13 +65,24 @@ static __device__ void right_env_step(const Dev &p, SmemT<T> &s, const double *W
   __syncthreads();
   const T *Rn = scr + p.roff[k + 1];
   T *Rk = scr + p.roff[k];
+  T *Z = scr + p.zoff[k];
+  const long zb = (long)al * p.bW[k];
   const T *Bk = trial_of<T>(p) + p.toff[k];
   for (int sg = 0; sg < d; ++sg)
     gemm_t<NP>(ar, bl, br, T(1), Rn, ar, false, s.Nxt + sg * s.sbC, p.pb, true, T(0), s.Xb + sg * s.sbX, p.pa);
   __syncthreads();
-  for (int sg = 0; sg < d; ++sg)
-    gemm_t<NP>(al, bl, ar, T(1), Bk + (long)sg * al * ar, al, false, s.Xb + sg * s.sbX, p.pa, false,
-               sg == 0 ? T(0) : T(1), Rk, al);
+  if constexpr (ZB) {
+    for (int sg = 0; sg < d; ++sg)
+      for (int tau = 0; tau < d; ++tau)
+        gemm_t<NP>(al, bl, ar, T(1), Bk + (long)sg * al * ar, al, false, s.Xb + tau * s.sbX, p.pa, false, T(0),
+                   Z + (sg + d * tau) * zb, al);
+    __syncthreads();
+    for (int q = threadIdx.x; q < al * bl; q += kThreads) Rk[q] = Z[q] + Z[3 * zb + q];
+  } else {
+    for (int sg = 0; sg < d; ++sg)
+      gemm_t<NP>(al, bl, ar, T(1), Bk + (long)sg * al * ar, al, false, s.Xb + sg * s.sbX, p.pa, false,
+                 sg == 0 ? T(0) : T(1), Rk, al);
+  }
   __syncthreads();
 }
 
@@ -180,10 +196,49 @@ static __device__ void env_update_general(const Dev &p, SmemT<T> &s, int k, cons
   __syncthreads();
 }
 
-// Closures of the four left branches in Pb (cut j, a_j x b_j) with the right branches of site j
-// (walker site in Nxt, R[j+1] at Rn): M[p + 4q] = <P_p, B_j[s'] R[j+1] A_j[t']^T>, q = s' + 2t'.
+// Closures of the four left branches in Pb (cut j, a_j x b_j) with the right branches Z of site
+// j (right_env_step): M[p + 4q] = <P_p, Z[q]> = <P_p, B_j[s'] R[j+1] A_j[t']^T>, q = s' + 2t'.
+// Sixteen dot products in one pass, reduced in FP64.  Ends with a barrier.
 template <typename T, int NP = 0>
-static __device__ void closures(const Dev &p, SmemT<T> &s, int j, const T *Rn) {
+static __device__ void closures_z(const Dev &p, SmemT<T> &s, int j, const T *Z) {
+  const int aj = p.aT[j], bj = s.bW[j];
+  const long zb = (long)aj * p.bW[j];
+  double v[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = 0.0;
+  for (int e = threadIdx.x; e < aj * bj; e += kThreads) {
+    const int m = e % aj, n = e / aj;
+    T pk[4], zq[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) pk[k] = s.Pb[k * s.sbX + m + p.pa * n];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) zq[q] = Z[q * zb + e];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k + 4 * q] += (double)pk[k] * (double)zq[q];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 16; ++q)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < 16; ++q) s.red[q * kWarps + warp] = v[q];
+  __syncthreads();
+  if (threadIdx.x < 16) {
+    double sum = 0.0;
+    for (int w = 0; w < kWarps; ++w) sum += s.red[threadIdx.x * kWarps + w];
+    s.M[threadIdx.x] = sum;
+  }
+  __syncthreads();
+}
+
+// The same closures for couplings of any range: the right branches of site j (walker site in
+// Nxt, R[j+1] at Rn) formed and dotted with P in one pass of products.
+template <typename T, int NP = 0>
+static __device__ void closures_products(const Dev &p, SmemT<T> &s, int j, const T *Rn) {
   const int d = kMaxD;
   const int aj = p.aT[j], a2 = p.aT[j + 1], bj = s.bW[j], b2 = s.bW[j + 1];
   const T *Bj = trial_of<T>(p) + p.toff[j];
@@ -198,6 +253,19 @@ static __device__ void closures(const Dev &p, SmemT<T> &s, int j, const T *Rn) {
       cta_closure16<false>(aj, bj, a2, Bj, aj, (long)aj * a2, s.Xb, p.pa, s.sbX, s.Pb, p.pa, s.sbX, s.red, s.M);
   } else {
     cta_closure16_tf32<NP>(aj, bj, a2, Bj, aj, (long)aj * a2, s.Xb, p.pa, s.sbX, s.Pb, p.pa, s.sbX, s.red, s.M);
+  }
+}
+
+// The 16 closures of coupling (i, j), left branches in Pb: against the stored right branches of
+// site j (ZB) or formed here (site j from W, R[j+1] from the scratch).  Uses Nxt and Xb.
+template <typename T, int NP = 0, bool ZB = false>
+static __device__ void closures(const Dev &p, SmemT<T> &s, int j, const double *W, T *scr) {
+  if constexpr (ZB) {
+    closures_z<T, NP>(p, s, j, scr + p.zoff[j]);
+  } else {
+    load_site(s.Nxt, p.pb, s.sbC, W + s.woff[j], s.bW[j], s.bW[j + 1]);
+    __syncthreads();
+    closures_products<T, NP>(p, s, j, scr + p.roff[j + 1]);
   }
 }
 
@@ -402,7 +470,7 @@ static __device__ double norm_from_centre(const Dev &p, SmemT<T> &s, const doubl
 #ifndef MQ_DEVICE_ONLY
 
 // The walker step (all walkers of the population, one CTA per walker at a time).
-template <typename T, int NP>
+template <typename T, int NP, bool ZB>
 __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
   constexpr bool kMixed = !std::is_same<T, double>::value;
   SmemT<T> s;
@@ -424,7 +492,7 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
       scr[p.roff[L]] = T(1);
       if (Nl != nullptr) Nl[0] = T(1);
     }
-    for (int k = L - 1; k >= 1; --k) right_env_step<T, NP>(p, s, W, scr, k);
+    for (int k = L - 1; k >= 1; --k) right_env_step<T, NP, ZB>(p, s, W, scr, k);
     int rv = 1;  // R[k] is valid for k >= rv
     // centre on site 0: overlap <Psi_T|phi> (the stored walker is normalised, overlap > 0)
     double ov;
@@ -454,9 +522,9 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
       bool branches_kept = false;
       for (int c = p.site_c0[i]; c < p.site_c0[i + 1]; ++c) {
         const int j = p.cp_j[c];
-        while (rv > j + 1) {
+        while (rv > (ZB ? j : j + 1)) {  // R[j+1] (and the right branches of site j) up to date
           --rv;
-          right_env_step<T, NP>(p, s, W, scr, rv);
+          right_env_step<T, NP, ZB>(p, s, W, scr, rv);
         }
         // left branches P[s + d t] = B_i[s]^T Lenv C[t] (a_{i+1} x b_{i+1})
         for (int tau = 0; tau < d; ++tau)
@@ -477,24 +545,17 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
           for (int q = 0; q < kN2; ++q)
             transfer_in_place<T, NP>(p, s, Bm, am, am1, bm, bm1, s.Nxt, p.pb, s.sbC, s.Pb + q * s.sbX, p.pa);
         }
-        // right branches at j, closures, sample
+        // closures with the right branches of site j, sample, site operators
         const int bj = s.bW[j], bj1 = s.bW[j + 1];
-        load_site(s.Nxt, p.pb, s.sbC, W + s.woff[j], bj, bj1);
         __syncthreads();
-        closures<T, NP>(p, s, j, scr + p.roff[j + 1]);
+        closures<T, NP, ZB>(p, s, j, W, scr);
         const double num = sample_coupling(p, s, w, c, p.cp_q[c], ov, wt);
         apply_site_op(s.Cen, p.pb, s.sbC, bl, br, s.O1);
-        if constexpr (kMixed) {
-          // the walker itself stays FP64: the operators act on its copy in HBM as well, the FP32
-          // centre only feeds the contractions
-          apply_site_op_stored(W + s.woff[i], bl, br, s.O1);
-          apply_site_op_stored(W + s.woff[j], bj, bj1, s.O2);
-          __syncthreads();
-        } else {
-          apply_site_op(s.Nxt, p.pb, s.sbC, bj, bj1, s.O2);
-          __syncthreads();
-          store_site(W + s.woff[j], s.Nxt, p.pb, s.sbC, bj, bj1);
-        }
+        // O2 acts on site j as stored in HBM; in the mixed sweep the walker itself stays FP64, so
+        // O1 acts on its stored site i as well (the FP32 centre only feeds the contractions)
+        if constexpr (kMixed) apply_site_op_stored(W + s.woff[i], bl, br, s.O1);
+        apply_site_op_stored(W + s.woff[j], bj, bj1, s.O2);
+        __syncthreads();
         if (rv < j + 1) rv = j + 1;
         ov = num;
         branches_kept = (j == i + 1) && (p.trace == nullptr);
@@ -637,17 +698,20 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
   }
 }
 
+// ZB: nearest-neighbour couplings, right branches stored per site (a separate instantiation, so
+// the register allocation of each sweep carries one closure path only).
+template <bool ZB>
 __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p) {
   extern __shared__ double smem_raw[];
-  general_step<double, 0>(p, smem_raw);
+  general_step<double, 0, ZB>(p, smem_raw);
 }
 
 // Mixed precision: FP32 work buffers, TF32 tensor cores (NP passes), always QR-free.  Half the
 // shared memory of the FP64 sweep, so two CTAs fit on an SM where the FP64 sweep fits one.
-template <int NP>
+template <int NP, bool ZB>
 __global__ void __launch_bounds__(kThreads, 2) walker_step_mixed_kernel(Dev p) {
   extern __shared__ double smem_raw[];
-  general_step<float, NP>(p, smem_raw);
+  general_step<float, NP, ZB>(p, smem_raw);
 }
 
 // <Psi_T|H|phi> / overlap for every walker (any coupling range), tensors as stored.

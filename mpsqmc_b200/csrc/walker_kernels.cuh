@@ -68,6 +68,7 @@ struct Dev {
   long scr_stride;
   const long *roff;    // right-environment offsets [L+1] inside a CTA's scratch
   const long *nroff;   // norm-environment offsets [L+1] inside a CTA's scratch
+  const long *zoff;    // right-branch offsets [L] inside a CTA's scratch (general sweep)
   long foff;           // compact-MPO environments (2 x 4 x maxA*maxB) inside the scratch
   double *trace;       // optional [N][nC][kTraceStride]
   int *err;            // device error word (bit flags)
