@@ -426,7 +426,8 @@ def main():
             plain = this if (args.precision, args.proposal) == ("fp64", "grid") else arm("fp64", "grid")
             vn = {"plain_fp64_grid": plain, "vn_ratio_vs_plain_fp64": {}, "throughput_ratio_vs_plain_fp64": {}}
             arms = [this["arm"]] if this is not plain else []
-            arms += [x for x in args.vn_arms.split(",") if x and x not in arms and x != "fp64/grid"]
+            named = [x if "/" in x else x + "/grid" for x in args.vn_arms.split(",") if x]
+            arms += [x for x in named if x not in arms and x != "fp64/grid"]
             for name in arms:
                 r = this if name == this["arm"] else arm(*name.split("/"))
                 vn[name] = r

@@ -3,7 +3,10 @@
 // energy file follow MPSQMC2.cpp:449-498, 613-686 and 749-758.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <fstream>
+#include <string>
+#include <utility>
 #include <vector>
 
 #include "MPSQMC2.h"
@@ -110,6 +113,37 @@ void MPSQMC2::Setup(MPSstate *trial) {
     cerr << "MPSQMC2: GPU engine unavailable: " << mpsqmc_last_error() << endl;
     ctx = nullptr;
     return;
+  }
+  // engine options from the environment, so that an unchanged main.cpp can choose them:
+  //   MPSQMC_PRECISION = fp64 | tf32 | tf32x3, MPSQMC_CANONICAL_INTERVAL = K,
+  //   MPSQMC_POPCONTROL_INTERVAL = K, MPSQMC_RESAMPLING = threshold | comb
+  {
+    struct Named {
+      const char *var;
+      int option;
+      const char *names[3];
+      long values[3];
+    };
+    const Named named[] = {
+        {"MPSQMC_PRECISION", MPSQMC_OPT_PRECISION, {"fp64", "tf32", "tf32x3"},
+         {MPSQMC_PRECISION_FP64, MPSQMC_PRECISION_TF32, MPSQMC_PRECISION_TF32X3}},
+        {"MPSQMC_RESAMPLING", MPSQMC_OPT_RESAMPLING, {"threshold", "comb", nullptr},
+         {MPSQMC_RESAMPLE_THRESHOLD, MPSQMC_RESAMPLE_COMB, 0}}};
+    for (const Named &o : named) {
+      const char *v = getenv(o.var);
+      if (!v) continue;
+      int k = 0;
+      while (k < 3 && o.names[k] && std::string(v) != o.names[k]) ++k;
+      if (k == 3 || !o.names[k] || mpsqmc_set_option(ctx, o.option, o.values[k]) != MPSQMC_OK)
+        cerr << "MPSQMC2: ignoring " << o.var << "=" << v << endl;
+    }
+    const std::pair<const char *, int> counts[] = {{"MPSQMC_CANONICAL_INTERVAL", MPSQMC_OPT_CANONICAL_INTERVAL},
+                                                   {"MPSQMC_POPCONTROL_INTERVAL", MPSQMC_OPT_POPCONTROL_INTERVAL}};
+    for (const auto &o : counts) {
+      const char *v = getenv(o.first);
+      if (v && mpsqmc_set_option(ctx, o.second, std::atol(v)) != MPSQMC_OK)
+        cerr << "MPSQMC2: ignoring " << o.first << "=" << v << endl;
+    }
   }
   const int N = totalNDesiredWalkers;
   std::vector<double> all((size_t)N * w0.size()), ones(N, 1.0), zeros(N, 0.0);

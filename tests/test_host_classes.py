@@ -104,18 +104,21 @@ def test_reference_main_links_unchanged(tmp_path):
 
 
 @pytest.mark.gpu
-def test_dropin_walk_runs_main_call_sequence(tmp_path):
+@pytest.mark.parametrize("options", [{}, {"MPSQMC_PRECISION": "tf32x3", "MPSQMC_CANONICAL_INTERVAL": "4"}])
+def test_dropin_walk_runs_main_call_sequence(tmp_path, options):
     """main.cpp's call sequence (MPSstate from file, HeisenbergMPO, Marsaglia grid, MPSQMC2::Walk)
-    on the GPU engine: console lines and the energy file of the reference, energies of the trial."""
+    on the GPU engine: console lines and the energy file of the reference, energies of the trial.
+    Engine options reach an unchanged caller through the environment."""
     exe = compile_cpp(os.path.join(ROOT, "tests", "cpp", "dropin_walk.cpp"), str(tmp_path / "dropin_walk"))
     z = load_golden("trials")
     po.write_mps(str(tmp_path / "trial.mps"), po.MPS(z["L10D8_dims"], z["L10D8_data"]))
     (tmp_path / "output" / "Heisenberg1D").mkdir(parents=True)
     steps, N = 6, 16
     r = subprocess.run([exe, "trial.mps", "4", str(N), "0.05", str(steps)], cwd=tmp_path, capture_output=True,
-                       text=True, env={**os.environ, "MPSQMC_SEED": "20131015"}, timeout=300)
+                       text=True, env={**os.environ, "MPSQMC_SEED": "20131015", **options}, timeout=300)
     assert r.returncode == 0, r.stderr
     assert "GPU engine unavailable" not in r.stderr and "MPSQMC::Walk" not in r.stderr
+    assert "ignoring" not in r.stderr
     meta = load_golden("walk_L10D8_DW4")["meta"]
     E0 = float(r.stdout.split("Energy at start = ")[1].split()[0])
     assert E0 == pytest.approx(meta["E0"], rel=1e-10)    # same trial, same compressed walkers
