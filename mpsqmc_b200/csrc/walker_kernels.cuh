@@ -82,7 +82,7 @@ struct Dev {
   const int *eopen;        // [L]: slot of the channel that site k opens, or -1
   long choff;              // energy channels inside a CTA's scratch: 2 "done" + 3 per slot
   long gwoff;              // matrix work buffers inside a CTA's scratch, or -1 (shared memory)
-  // QR-free general sweep: sites are stored as they leave the centre (rescaled to unit Frobenius
+  // QR-free general sweep: sites are stored as they leave the centre (rescaled to an isometry's Frobenius
   // norm) and a left norm environment (maxB x maxB, ld pb) inside the scratch gives the norm
   long nloff;              // its offset inside a CTA's scratch, or -1 (Householder QR per site)
   // learned proposal (proposal.cuh)
