@@ -99,6 +99,7 @@ struct mpsqmc_ctx {
   bool global_work = false;             // matrix work buffers in global scratch
   int maxA = 1, maxB = 1, pa = 4, pb = 4, pq = 4;
   size_t smem_bytes = 0;
+  size_t smem_bytes_noqr = 0;           // the QR-free general sweep's (no Householder buffers)
   int sm_count = 1, max_ctas = 1;
   // mixed-precision sweep (FP32 work buffers, TF32 tensor cores): its own shared memory and grid
   int precision = MPSQMC_PRECISION_FP64;
@@ -368,6 +369,10 @@ int layout_workspace(mpsqmc_ctx *c, bool force_global) {
     c->smem_bytes = sizeof(double) * (size_t)(all - c->big_doubles);
   }
   c->global_work = global;
+  c->smem_bytes_noqr = global ? c->smem_bytes
+                              : sizeof(double) * (size_t)mq::smem_doubles(c->L, c->maxA, c->maxB, c->G, c->pa, c->pb,
+                                                                          c->pq, nullptr, nullptr, nullptr, nullptr,
+                                                                          mlp, false);
   if (c->smem_bytes > c->smem_optin)
     return fail(MPSQMC_E_UNSUPPORTED, "grid too large for the shared-memory budget of one CTA");
   const void *kernels[] = {(const void *)mq::walker_step_kernel, (const void *)mq::set_overlap_kernel,
@@ -1095,8 +1100,9 @@ static int enqueue_propagation(mpsqmc_ctx *c, int *launches, bool canon) {
       else mq::walker_step_mixed_kernel<3, false><<<g, mq::kThreads, sm, c->stream>>>(p);
     }
   } else if (gen) {
-    if (c->nn) mq::walker_step_general_kernel<true><<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
-    else mq::walker_step_general_kernel<false><<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
+    const size_t sm = qr_free(c) ? c->smem_bytes_noqr : c->smem_bytes;
+    if (c->nn) mq::walker_step_general_kernel<true><<<grid, mq::kThreads, sm, c->stream>>>(p);
+    else mq::walker_step_general_kernel<false><<<grid, mq::kThreads, sm, c->stream>>>(p);
   } else
     mq::walker_step_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
   CK(cudaEventRecordWithFlags(c->ev[1], c->stream, evflags));

@@ -474,7 +474,8 @@ template <typename T, int NP, bool ZB>
 __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
   constexpr bool kMixed = !std::is_same<T, double>::value;
   SmemT<T> s;
-  carve(p, s, smem_raw);
+  if constexpr (kMixed) carve(p, s, smem_raw);
+  else carve(p, s, smem_raw, p.nloff < 0);  // the QR-free sweep has no Householder buffers
   const int L = p.L, d = kMaxD, tid = threadIdx.x;
   const int N = *p.n_cur;
   T *scr = reinterpret_cast<T *>(p.scratch) + (long)blockIdx.x * p.scr_stride;

@@ -122,7 +122,7 @@ using Smem = SmemT<double>;
 // (if given) receives the size of the matrix buffers.  mlp: the learned proposal's buffers.
 __host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, int pa, int pb, int pq,
                                               Smem *s, double *base, double *big = nullptr,
-                                              long *big_doubles = nullptr, bool mlp = false) {
+                                              long *big_doubles = nullptr, bool mlp = false, bool qr = true) {
   long off = 0, boff = 0;
   double *dummy;
   auto take = [&](double *&p, long n) {
@@ -169,8 +169,13 @@ __host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, i
   take_big(s ? s->Xb : dummy, (long)pa * maxB * d);
   take_big(s ? s->Pb : dummy, (long)pa * maxB * kN2);
   take_big(s ? s->Qt : dummy, (long)pa * maxB);
-  take_big(s ? s->QRb : dummy, (long)pq * maxB);
-  take_big(s ? s->Rf : dummy, (long)pb * maxB);
+  if (qr) {  // the Householder panel and R factor, last: the QR-free sweep goes without them
+    take_big(s ? s->QRb : dummy, (long)pq * maxB);
+    take_big(s ? s->Rf : dummy, (long)pb * maxB);
+  } else if (s) {
+    s->QRb = nullptr;
+    s->Rf = nullptr;
+  }
   if (big_doubles) *big_doubles = boff;
   if (s) {
     s->sbC = pb * maxB;
@@ -246,10 +251,11 @@ __host__ __device__ inline long smem_bytes_f32(int L, int maxA, int maxB, int G,
 
 // Carve the work buffers of the calling CTA (shared memory, plus its global scratch when the
 // matrix buffers do not fit on chip).
-__device__ __forceinline__ void carve(const Dev &p, Smem &s, double *smem_raw) {
+// qr: the kernel uses the Householder buffers (all but the QR-free general sweep).
+__device__ __forceinline__ void carve(const Dev &p, Smem &s, double *smem_raw, bool qr = true) {
   double *big = (p.gwoff >= 0) ? p.scratch + (long)blockIdx.x * p.scr_stride + p.gwoff : nullptr;
   smem_doubles(p.L, p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw, big, nullptr,
-               p.prop_mode != 0 || p.prop_collect != 0);
+               p.prop_mode != 0 || p.prop_collect != 0, qr);
 }
 // Mixed precision: the CTA's scratch is read as floats with the same element offsets.
 __device__ __forceinline__ void carve(const Dev &p, SmemT<float> &s, double *smem_raw) {
