@@ -35,7 +35,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="chain64", choices=["chain64", "snake6x6", "snake8x8"],
+    ap.add_argument("--workload", default="chain64", choices=["chain64", "snake6x6", "snake6x6_dmrg", "snake8x8"],
                     help="chain64: the L=64 chain (default line); snake6x6 / snake8x8: the 2D lattices "
                          "(walkers compressed on the device; no CPU baseline or e2e)")
     ap.add_argument("--walkers", type=int, default=None)
@@ -280,8 +280,10 @@ def main():
         wl = getattr(workloads, args.workload)(Nw=args.walkers) if args.walkers else getattr(workloads, args.workload)()
         cfg = {"workload": f"{wl.name}: {wl.W}x{wl.H} open Heisenberg lattice on the snake path (L={wl.L}, "
                            f"{len(wl.couplings()[0])} couplings), D_T={wl.DT}, D_W in {wl.Ds}, {wl.Nw} walkers/GPU, "
-                           f"dtau={wl.dtau}, Marsaglia(4) grid, FP64; seeded random left-normalised trial of the "
-                           f"D_T shape, walkers = trial compressed on the device",
+                           f"dtau={wl.dtau}, Marsaglia(4) grid, FP64; "
+                           + (f"trial: DMRG ground state at D_T={wl.DT} (E={wl.trial_energy():.10f})"
+                              if wl.trial_file else "seeded random left-normalised trial of the D_T shape")
+                           + ", walkers = trial compressed on the device",
                "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.Ds, "dtau": wl.dtau,
                "parallelism": f"{'split walk' if args.sharded else 'replicas'} x{world}", "sweep": args.sweep,
                "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
@@ -382,9 +384,13 @@ def main():
     vn_steps = max(args.vn, vn_compare)
     if vn_steps > 0:
         from mpsqmc_b200 import analysis
-        e_ref = None
+        e_ref, e_src = None, None
         if not lattice:
             e_ref = float(np.load(os.path.join(ROOT, "mpsqmc_b200", "data", "trial_L64D64.npz"))["energy"])
+            e_src = "DMRG D=64 energy of the trial (mpsqmc_b200/data)"
+        elif wl.trial_energy() is not None:
+            e_ref = wl.trial_energy()
+            e_src = f"DMRG D={wl.DT} energy of the trial (mpsqmc_b200/data; a variational upper bound)"
 
         def vn_of(e, throughput):
             more = e.walk(vn_steps)
@@ -392,7 +398,7 @@ def main():
             r["throughput_per_gpu"] = throughput
             if e_ref is not None:
                 r["E_ref"] = e_ref
-                r["E_ref_source"] = "DMRG D=64 energy of the trial (mpsqmc_b200/data)"
+                r["E_ref_source"] = e_src
                 r["abs_err_per_site"] = abs(r["E_mean"] - e_ref) / wl.L
             return r
 

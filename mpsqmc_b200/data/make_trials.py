@@ -1,0 +1,39 @@
+"""Regenerate the stored trial states of the named workloads (mpsqmc_b200/workloads.py).
+
+    python mpsqmc_b200/data/make_trials.py [chain64] [snake6x6]
+
+chain64:  trial_L64D64.npz, the open L=64 Heisenberg chain at D_T = 64;
+snake6x6: trial_snake6x6_D64.npz, the open 6x6 lattice on the snake path at D_T = 64.
+
+Both come from the compact-MPO two-site DMRG (mpsqmc_b200/dmrg.py, seed 7), left-normalised,
+in the reference's storage layout, with the DMRG energy beside them.
+"""
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from mpsqmc_b200 import dmrg, problem as pb  # noqa: E402
+
+
+def make(name: str) -> None:
+    t = time.time()
+    if name == "chain64":
+        m, e = dmrg.dmrg(64, 64)
+        out = "trial_L64D64.npz"
+    elif name == "snake6x6":
+        m, e = dmrg.dmrg(36, 64, couplings=pb.snake(6, 6))
+        out = "trial_snake6x6_D64.npz"
+    else:
+        raise SystemExit(f"unknown trial {name!r}")
+    np.savez(os.path.join(HERE, out), dims=m.dims, data=m.data, energy=e)
+    print(f"{out}: E = {e:.12f} ({time.time() - t:.0f} s)")
+
+
+if __name__ == "__main__":
+    for n in sys.argv[1:] or ["chain64", "snake6x6"]:
+        make(n)

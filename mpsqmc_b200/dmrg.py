@@ -1,4 +1,5 @@
-"""Trial-state generator: two-site DMRG with a compact (bond dimension 5) MPO.
+"""Trial-state generator: two-site DMRG with a compact MPO (bond dimension 5 on a chain,
+2 + 3 x (open sites) for couplings of any range, e.g. 2D lattices on a snake path).
 
 The reference's DMRG (DMRG.cpp:13-604) rebuilds the full generic MPO product every step, whose
 bond grows to (2 + 3 L/2) * D_T, which is out of reach for L = 64, D_T = 64.  This host-side
@@ -43,6 +44,62 @@ def chain_mpo(L: int, J: np.ndarray, h: float = 0.0, d: int = 2) -> list[np.ndar
     return Ws
 
 
+def coupling_mpo(L: int, ci, cj, cJ, h: float = 0.0, d: int = 2) -> list[np.ndarray]:
+    """Compact MPO of H = sum_c J_c S_i.S_j - h sum_k S^z_k for couplings (i < j) of any range.
+
+    Channels on the cut before site k: 0 = done, then (Sx, iSy, Sz) of every site i < k that still
+    has a partner j >= k (in order of i), last = nothing placed yet.  Site k closes the channels
+    of its partners i (J_ik times Sx, -iSy, Sz on site k), carries on the ones that stay open,
+    opens its own when it has a partner beyond k, and places the field.  Same layout as chain_mpo:
+    W[k] of shape (w_in, w_out, d_out, d_in)."""
+    sz, sx, isy = spin_ops(d)
+    ops = (sx, isy, sz)
+    eye = np.eye(d)
+    last = [-1] * L
+    J = {}
+    for i, j, c in zip(ci, cj, cJ):
+        i, j = int(i), int(j)
+        last[i] = max(last[i], j)
+        J[(i, j)] = J.get((i, j), 0.0) + float(c)
+    opened = [[i for i in range(k) if last[i] >= k] for k in range(L + 1)]  # open sites on cut k
+    Ws = []
+    for k in range(L):
+        inn, out = opened[k], opened[k + 1]
+        w_in, w_out = 2 + 3 * len(inn), 2 + 3 * len(out)
+        W = np.zeros((w_in, w_out, d, d))
+        W[0, 0] = eye
+        W[w_in - 1, w_out - 1] = eye
+        W[w_in - 1, 0] = -h * sz
+        for q, i in enumerate(inn):
+            Jik = J.get((i, k), 0.0)
+            for a in range(3):
+                if Jik != 0.0:
+                    W[1 + 3 * q + a, 0] = (-Jik if a == 1 else Jik) * ops[a]
+                if i in out:
+                    W[1 + 3 * q + a, 1 + 3 * out.index(i) + a] = eye
+        if k in out:
+            r = out.index(k)
+            for a in range(3):
+                W[w_in - 1, 1 + 3 * r + a] = ops[a]
+        if k == 0:
+            W = W[w_in - 1:w_in]
+        if k == L - 1:
+            W = W[:, 0:1]
+        Ws.append(W)
+    return Ws
+
+
+def mpo_energy(m: MPS, Ws) -> float:
+    """<m|H|m> / <m|m> of an MPS in the reference layout with the MPO Ws."""
+    A = [m.site(k).transpose(1, 0, 2) for k in range(m.L)]  # (Dl, s, Dr)
+    E = np.ones((1, 1, 1))
+    N = np.ones((1, 1))
+    for k in range(m.L):
+        E = _left_env(E, A[k], Ws[k])
+        N = np.einsum("ab,asc,bsd->cd", N, A[k], A[k])
+    return float(E[0, 0, 0] / N[0, 0])
+
+
 def _left_env(Lprev, A, W):
     # Lprev (a, w, A'), A (A', s, C) ket, bra = A (real)
     t = np.tensordot(Lprev, A, axes=([2], [0]))            # a w s C
@@ -70,13 +127,17 @@ def _heff(Lenv, W1, W2, Renv, shape):
 
 
 def dmrg(L: int, D: int, J=1.0, h: float = 0.0, sweeps: int = 8, tol: float = 1e-10, seed: int = 7,
-         schedule=None, verbose: bool = False):
-    """Ground state of the open Heisenberg chain as an MPS of bond dimension <= D.
+         schedule=None, verbose: bool = False, couplings=None):
+    """Ground state of the open Heisenberg chain (or, with couplings = (ci, cj, cJ), of any
+    coupling list) as an MPS of bond dimension <= D.
 
     Returns (MPS in reference layout, left-normalized; energy)."""
     d = 2
-    Jv = np.full(L - 1, float(J)) if np.isscalar(J) else np.asarray(J, dtype=np.float64)
-    Ws = chain_mpo(L, Jv, h, d)
+    if couplings is not None:
+        Ws = coupling_mpo(L, *couplings, h=h, d=d)
+    else:
+        Jv = np.full(L - 1, float(J)) if np.isscalar(J) else np.asarray(J, dtype=np.float64)
+        Ws = chain_mpo(L, Jv, h, d)
     rng = np.random.default_rng(seed)
     dims0 = virtual_dims(L, min(D, 4), d)
     A = [rng.standard_normal((dims0[k], d, dims0[k + 1])) for k in range(L)]

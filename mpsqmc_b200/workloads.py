@@ -4,6 +4,10 @@ chain64   L=64 open Heisenberg chain, J=1, h=0, D_T=64 trial (compact-MPO DMRG, 
           walkers = trial compressed to D_W=32 plus i.i.d. N(0, 1e-3) noise per element, dtau=0.01,
           2048 walkers, Marsaglia(4) grid (240 points).
 chain16   L=16 chain, D_T=D_W=16 trial from the reference's DMRG, 128 walkers, dtau=0.01.
+snake6x6, snake8x8   open 6x6 / 8x8 lattices on the snake path with seeded random trials of the
+          D_T bond profile (throughput: the work per walker-step does not depend on the trial).
+snake6x6_dmrg   the open 6x6 lattice with its ground-state trial from the compact-MPO DMRG at
+          D_T = 64 (mpsqmc_b200/data, made by data/make_trials.py), walkers of D_W in {16, 32, 64}.
 """
 from __future__ import annotations
 
@@ -136,10 +140,17 @@ class LatticeWorkload:
     Nw: int
     dtau: float
     seed: int = 20131015
+    trial_file: str | None = None  # a DMRG trial in mpsqmc_b200/data (else a random one)
 
     @property
     def L(self):
         return self.W * self.H
+
+    def trial_energy(self):
+        """The DMRG energy of the stored trial (a variational upper bound), or None."""
+        if not self.trial_file:
+            return None
+        return float(np.load(os.path.join(DATA, self.trial_file))["energy"])
 
     def couplings(self):
         return pb.snake(self.W, self.H)
@@ -149,6 +160,9 @@ class LatticeWorkload:
         return rng.choice(np.asarray(self.Ds, dtype=np.int32), size=self.Nw)
 
     def trial(self):
+        if self.trial_file:
+            z = np.load(os.path.join(DATA, self.trial_file))
+            return pb.MPS(z["dims"].astype(np.int32), z["data"])
         rng = np.random.default_rng(self.seed)
         dims = pb.virtual_dims(self.L, self.DT)
         data = rng.normal(size=int(sum(dims[k] * dims[k + 1] * 2 for k in range(self.L))))
@@ -158,6 +172,12 @@ class LatticeWorkload:
 def snake6x6(Nw: int = 1024) -> LatticeWorkload:
     """6x6 open lattice, D_T = 128, walkers of D_W drawn uniformly from {16, 32, 64, 128}, dtau 0.005."""
     return LatticeWorkload("snake6x6", 6, 6, 128, [16, 32, 64, 128], Nw, 0.005)
+
+
+def snake6x6_dmrg(Nw: int = 1024) -> LatticeWorkload:
+    """6x6 open lattice with its DMRG ground-state trial (D_T = 64), walkers of D_W drawn from
+    {16, 32, 64}, dtau 0.005."""
+    return LatticeWorkload("snake6x6_dmrg", 6, 6, 64, [16, 32, 64], Nw, 0.005, trial_file="trial_snake6x6_D64.npz")
 
 
 def snake8x8(Nw: int = 4096) -> LatticeWorkload:

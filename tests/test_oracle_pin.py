@@ -176,3 +176,57 @@ def test_snake_couplings_match_reference_list():
         np.testing.assert_array_equal(ci, z["coup_i"])
         np.testing.assert_array_equal(cj, z["coup_j"])
         np.testing.assert_array_equal(cJ, z["coup_J"])
+
+
+def test_compact_mpo_of_any_couplings():
+    """mpsqmc_b200.dmrg.coupling_mpo: on a chain it is the chain MPO; on the 3x3 snake its
+    <m|H|m> is the oracle's energy numerator of the same (left-normalised) state."""
+    import numpy as np
+    from mpsqmc_b200 import dmrg, problem as pb
+    from oracle import pyoracle as po
+    rng = np.random.default_rng(1)
+
+    def rand_mps(L, D):
+        dims = pb.virtual_dims(L, D)
+        return pb.MPS(dims, rng.normal(size=int(sum(dims[k] * dims[k + 1] * 2 for k in range(L)))))
+
+    ci, cj, cJ = pb.chain(6)
+    m = rand_mps(6, 4)
+    assert dmrg.mpo_energy(m, dmrg.coupling_mpo(6, ci, cj, cJ, 0.3)) == pytest.approx(
+        dmrg.mpo_energy(m, dmrg.chain_mpo(6, cJ, 0.3)), rel=1e-13)
+    ci, cj, cJ = pb.snake(3, 3)
+    ln = pb.left_normalize(rand_mps(9, 4))
+    e = po.energy_numerator(po.MPS(ln.dims, ln.data), po.MPS(ln.dims, ln.data), ci, cj, cJ)
+    assert dmrg.mpo_energy(ln, dmrg.coupling_mpo(9, ci, cj, cJ)) == pytest.approx(e, rel=1e-12)
+
+
+def test_lattice_dmrg_reaches_ed():
+    """Two-site DMRG with the compact MPO of the open 3x3 snake lattice at D = 16 (exact bond
+    dimension) reaches the ED ground energy; the 4x4 at D = 16 stays variational and close."""
+    from mpsqmc_b200 import dmrg, problem as pb
+    from oracle import ed
+    c33 = pb.snake(3, 3)
+    _, e = dmrg.dmrg(9, 16, couplings=c33)
+    assert e == pytest.approx(ed.ground_energy_couplings(9, *c33), abs=1e-9)
+    c44 = pb.snake(4, 4)
+    m, e = dmrg.dmrg(16, 16, couplings=c44)
+    e0 = -9.189207065192948
+    assert e0 - 1e-10 <= e < e0 + 0.1
+    assert dmrg.mpo_energy(m, dmrg.coupling_mpo(16, *c44)) == pytest.approx(e, rel=1e-9)
+
+
+def test_stored_lattice_trial_is_the_dmrg_state():
+    """The 6x6 workload's stored trial: left-normalised, bond dims within D_T = 64, and its
+    energy under the lattice's compact MPO is the stored DMRG energy (a variational bound)."""
+    import numpy as np
+    from mpsqmc_b200 import dmrg, workloads
+    wl = workloads.snake6x6_dmrg()
+    m = wl.trial()
+    assert m.L == 36 and int(max(m.dims)) == wl.DT
+    e = dmrg.mpo_energy(m, dmrg.coupling_mpo(36, *wl.couplings()))
+    assert e == pytest.approx(wl.trial_energy(), rel=1e-9)
+    assert -0.62 * 36 < e < -0.55 * 36
+    for k in range(m.L - 1):
+        A = m.site(k)  # [sigma, Dl, Dr]
+        G = sum(A[s].T @ A[s] for s in range(2))
+        np.testing.assert_allclose(G, np.eye(G.shape[0]), atol=1e-10)
