@@ -470,19 +470,20 @@ static __device__ double norm_from_centre(const Dev &p, SmemT<T> &s, const doubl
 #ifndef MQ_DEVICE_ONLY
 
 // The walker step (all walkers of the population, one CTA per walker at a time).
-template <typename T, int NP, bool ZB>
+// QF: the QR-free sweep (p.nloff >= 0), a separate instantiation from the one with the QR per site.
+template <typename T, int NP, bool ZB, bool QF>
 __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
   constexpr bool kMixed = !std::is_same<T, double>::value;
   SmemT<T> s;
   if constexpr (kMixed) carve(p, s, smem_raw);
-  else carve(p, s, smem_raw, p.nloff < 0);  // the QR-free sweep has no Householder buffers
+  else carve(p, s, smem_raw, !QF);  // the QR-free sweep has no Householder buffers
   const int L = p.L, d = kMaxD, tid = threadIdx.x;
   const int N = *p.n_cur;
   T *scr = reinterpret_cast<T *>(p.scratch) + (long)blockIdx.x * p.scr_stride;
   const long fm = (long)p.maxA * p.maxB;
   T *Fdone[2] = {scr + p.choff, scr + p.choff + fm};
   T *Fch = scr + p.choff + 2 * fm;
-  T *Nl = (p.nloff >= 0) ? scr + p.nloff : nullptr;  // left norm environment (QR-free sweep)
+  T *Nl = QF ? scr + p.nloff : nullptr;  // left norm environment (QR-free sweep)
   const T *trial = trial_of<T>(p);
   for (int w = next_walker(s, p.ctr + kCtrStep); w < N; w = next_walker(s, p.ctr + kCtrStep)) {
     const int slot = p.slot_of[w];
@@ -491,7 +492,7 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
     // right environments of the walker as stored
     if (tid == 0) {
       scr[p.roff[L]] = T(1);
-      if (Nl != nullptr) Nl[0] = T(1);
+      if (QF) Nl[0] = T(1);
     }
     for (int k = L - 1; k >= 1; --k) right_env_step<T, NP, ZB>(p, s, W, scr, k);
     int rv = 1;  // R[k] is valid for k >= rv
@@ -578,7 +579,7 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
         }
         __syncthreads();
       }
-      if (i < L - 1 && Nl != nullptr) {
+      if (QF && i < L - 1) {
         // QR-free: the centre itself becomes the final site i, rescaled to the Frobenius norm of
         // an isometry (sqrt(br)) so that the tensor scales cannot drift over the steps (the
         // overlap takes the same factor), and the left norm environment takes it in:
@@ -629,7 +630,7 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
         load_site(s.Cen, p.pb, s.sbC, W + s.woff[i + 1], br, s.bW[i + 2]);
         __syncthreads();
       } else if (i < L - 1) {
-        if constexpr (std::is_same<T, double>::value) {
+        if constexpr (std::is_same<T, double>::value && !QF) {
           // QR of the centre: Q is the final site i, R moves into site i+1
           for (int q = tid; q < bl * br; q += kThreads) {
             const int r = q % bl, cc = q / bl;
@@ -664,7 +665,7 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
           const T *cs = s.Cen + (q / bl) * s.sbC;
           const double *ws = Wi + (q / bl) * bl;  // the FP64 walker (mixed sweep)
           const double x = kMixed ? ws[q % bl] : (double)cs[q % bl];
-          if (Nl == nullptr) {
+          if (!QF) {
             part += x * x;
           } else {  // x (Nl c)_r
             double y = 0.0;
@@ -701,10 +702,10 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
 
 // ZB: nearest-neighbour couplings, right branches stored per site (a separate instantiation, so
 // the register allocation of each sweep carries one closure path only).
-template <bool ZB>
+template <bool ZB, bool QF>
 __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p) {
   extern __shared__ double smem_raw[];
-  general_step<double, 0, ZB>(p, smem_raw);
+  general_step<double, 0, ZB, QF>(p, smem_raw);
 }
 
 // Mixed precision: FP32 work buffers, TF32 tensor cores (NP passes), always QR-free.  Half the
@@ -712,7 +713,7 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p)
 template <int NP, bool ZB>
 __global__ void __launch_bounds__(kThreads, 2) walker_step_mixed_kernel(Dev p) {
   extern __shared__ double smem_raw[];
-  general_step<float, NP, ZB>(p, smem_raw);
+  general_step<float, NP, ZB, true>(p, smem_raw);
 }
 
 // <Psi_T|H|phi> / overlap for every walker (any coupling range), tensors as stored.
