@@ -376,10 +376,9 @@ int layout_workspace(mpsqmc_ctx *c, bool force_global) {
   if (c->smem_bytes > c->smem_optin)
     return fail(MPSQMC_E_UNSUPPORTED, "grid too large for the shared-memory budget of one CTA");
   const void *kernels[] = {(const void *)mq::walker_step_kernel, (const void *)mq::set_overlap_kernel,
-                           (const void *)mq::energy_kernel, (const void *)mq::walker_step_general_kernel<true, true>,
-                           (const void *)mq::walker_step_general_kernel<false, true>,
-                           (const void *)mq::walker_step_general_kernel<true, false>,
-                           (const void *)mq::walker_step_general_kernel<false, false>,
+                           (const void *)mq::energy_kernel, (const void *)mq::walker_step_general_kernel<true, 1>,
+                           (const void *)mq::walker_step_general_kernel<true, 2>,
+                           (const void *)mq::walker_step_general_kernel<false, 0>,
                            (const void *)mq::energy_general_kernel, (const void *)mq::legacy_step_kernel};
   for (const void *k : kernels)
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes));
@@ -1102,15 +1101,10 @@ static int enqueue_propagation(mpsqmc_ctx *c, int *launches, bool canon) {
       else mq::walker_step_mixed_kernel<3, false><<<g, mq::kThreads, sm, c->stream>>>(p);
     }
   } else if (gen) {
-    if (qr_free(c)) {
-      const size_t sm = c->smem_bytes_noqr;
-      if (c->nn) mq::walker_step_general_kernel<true, true><<<grid, mq::kThreads, sm, c->stream>>>(p);
-      else mq::walker_step_general_kernel<false, true><<<grid, mq::kThreads, sm, c->stream>>>(p);
-    } else {
-      const size_t sm = c->smem_bytes;
-      if (c->nn) mq::walker_step_general_kernel<true, false><<<grid, mq::kThreads, sm, c->stream>>>(p);
-      else mq::walker_step_general_kernel<false, false><<<grid, mq::kThreads, sm, c->stream>>>(p);
-    }
+    const size_t sm = qr_free(c) ? c->smem_bytes_noqr : c->smem_bytes;
+    if (!c->nn) mq::walker_step_general_kernel<false, 0><<<grid, mq::kThreads, sm, c->stream>>>(p);
+    else if (qr_free(c)) mq::walker_step_general_kernel<true, 1><<<grid, mq::kThreads, sm, c->stream>>>(p);
+    else mq::walker_step_general_kernel<true, 2><<<grid, mq::kThreads, sm, c->stream>>>(p);
   } else
     mq::walker_step_kernel<<<grid, mq::kThreads, c->smem_bytes, c->stream>>>(p);
   CK(cudaEventRecordWithFlags(c->ev[1], c->stream, evflags));

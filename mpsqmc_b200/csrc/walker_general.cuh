@@ -470,9 +470,12 @@ static __device__ double norm_from_centre(const Dev &p, SmemT<T> &s, const doubl
 #ifndef MQ_DEVICE_ONLY
 
 // The walker step (all walkers of the population, one CTA per walker at a time).
-// QF: the QR-free sweep (p.nloff >= 0), a separate instantiation from the one with the QR per site.
-template <typename T, int NP, bool ZB, bool QF>
+// QM: 1 the QR-free sweep, 2 the QR per site, 0 either, chosen by p.nloff at run time.  The chain
+// sweeps run as separate instantiations (fewer registers spilled); for couplings of any range
+// one instantiation choosing at run time measured faster.
+template <typename T, int NP, bool ZB, int QM>
 __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
+  const bool QF = QM == 1 || (QM == 0 && p.nloff >= 0);
   constexpr bool kMixed = !std::is_same<T, double>::value;
   SmemT<T> s;
   if constexpr (kMixed) carve(p, s, smem_raw);
@@ -630,7 +633,7 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
         load_site(s.Cen, p.pb, s.sbC, W + s.woff[i + 1], br, s.bW[i + 2]);
         __syncthreads();
       } else if (i < L - 1) {
-        if constexpr (std::is_same<T, double>::value && !QF) {
+        if constexpr (std::is_same<T, double>::value && QM != 1) {
           // QR of the centre: Q is the final site i, R moves into site i+1
           for (int q = tid; q < bl * br; q += kThreads) {
             const int r = q % bl, cc = q / bl;
@@ -702,10 +705,10 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
 
 // ZB: nearest-neighbour couplings, right branches stored per site (a separate instantiation, so
 // the register allocation of each sweep carries one closure path only).
-template <bool ZB, bool QF>
+template <bool ZB, int QM>
 __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p) {
   extern __shared__ double smem_raw[];
-  general_step<double, 0, ZB, QF>(p, smem_raw);
+  general_step<double, 0, ZB, QM>(p, smem_raw);
 }
 
 // Mixed precision: FP32 work buffers, TF32 tensor cores (NP passes), always QR-free.  Half the
@@ -713,7 +716,7 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p)
 template <int NP, bool ZB>
 __global__ void __launch_bounds__(kThreads, 2) walker_step_mixed_kernel(Dev p) {
   extern __shared__ double smem_raw[];
-  general_step<float, NP, ZB, true>(p, smem_raw);
+  general_step<float, NP, ZB, 1>(p, smem_raw);
 }
 
 // <Psi_T|H|phi> / overlap for every walker (any coupling range), tensors as stored.
