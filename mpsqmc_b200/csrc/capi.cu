@@ -377,6 +377,7 @@ int layout_workspace(mpsqmc_ctx *c, bool force_global) {
     return fail(MPSQMC_E_UNSUPPORTED, "grid too large for the shared-memory budget of one CTA");
   const void *kernels[] = {(const void *)mq::walker_step_kernel, (const void *)mq::set_overlap_kernel,
                            (const void *)mq::energy_kernel, (const void *)mq::walker_step_general_kernel<true, 1>,
+                           (const void *)mq::walker_step_general_kernel<true, 1, false>,
                            (const void *)mq::walker_step_general_kernel<true, 2>,
                            (const void *)mq::walker_step_general_kernel<false, 0>,
                            (const void *)mq::energy_general_kernel, (const void *)mq::legacy_step_kernel};
@@ -1103,6 +1104,8 @@ static int enqueue_propagation(mpsqmc_ctx *c, int *launches, bool canon) {
   } else if (gen) {
     const size_t sm = qr_free(c) ? c->smem_bytes_noqr : c->smem_bytes;
     if (!c->nn) mq::walker_step_general_kernel<false, 0><<<grid, mq::kThreads, sm, c->stream>>>(p);
+    else if (qr_free(c) && !c->trace_on)
+      mq::walker_step_general_kernel<true, 1, false><<<grid, mq::kThreads, sm, c->stream>>>(p);
     else if (qr_free(c)) mq::walker_step_general_kernel<true, 1><<<grid, mq::kThreads, sm, c->stream>>>(p);
     else mq::walker_step_general_kernel<true, 2><<<grid, mq::kThreads, sm, c->stream>>>(p);
   } else

@@ -470,12 +470,14 @@ static __device__ double norm_from_centre(const Dev &p, SmemT<T> &s, const doubl
 #ifndef MQ_DEVICE_ONLY
 
 // The walker step (all walkers of the population, one CTA per walker at a time).
-// QM: 1 the QR-free sweep, 2 the QR per site, 0 either, chosen by p.nloff at run time.  The chain
-// sweeps run as separate instantiations (fewer registers spilled); for couplings of any range
-// one instantiation choosing at run time measured faster.
-template <typename T, int NP, bool ZB, int QM>
+// QM: 1 the QR-free sweep, 2 the QR per site, 0 either, chosen by p.nloff at run time.  TR: the
+// per-coupling trace is compiled in (recorded when p.trace is set).  The chain sweeps run as
+// separate instantiations (fewer registers spilled); for couplings of any range one
+// instantiation choosing at run time measured faster.
+template <typename T, int NP, bool ZB, int QM, bool TR = true>
 __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
   const bool QF = QM == 1 || (QM == 0 && p.nloff >= 0);
+  const bool traced = TR && p.trace != nullptr;
   constexpr bool kMixed = !std::is_same<T, double>::value;
   SmemT<T> s;
   if constexpr (kMixed) carve(p, s, smem_raw);
@@ -515,7 +517,7 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
     }
     double wt = p.weight[slot];
     double nrm_prev = 1.0;  // trace mode: norm of the walker before the current coupling
-    if (p.trace != nullptr) nrm_prev = sqrt(norm_from_centre<T, NP>(p, s, W, scr, 0));
+    if (traced) nrm_prev = sqrt(norm_from_centre<T, NP>(p, s, W, scr, 0));
     if (tid == 0) s.Lenv[0] = T(1);
     int cur = 0;
     __syncthreads();
@@ -563,8 +565,8 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
         __syncthreads();
         if (rv < j + 1) rv = j + 1;
         ov = num;
-        branches_kept = (j == i + 1) && (p.trace == nullptr);
-        if (p.trace != nullptr) {
+        branches_kept = (j == i + 1) && !traced;
+        if (traced) {
           // the reference normalises after every coupling: report C of the normalised walker
           // and the normalised overlap (the walk itself does not need the norm)
           __syncthreads();
@@ -705,10 +707,10 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
 
 // ZB: nearest-neighbour couplings, right branches stored per site (a separate instantiation, so
 // the register allocation of each sweep carries one closure path only).
-template <bool ZB, int QM>
+template <bool ZB, int QM, bool TR = true>
 __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p) {
   extern __shared__ double smem_raw[];
-  general_step<double, 0, ZB, QM>(p, smem_raw);
+  general_step<double, 0, ZB, QM, TR>(p, smem_raw);
 }
 
 // Mixed precision: FP32 work buffers, TF32 tensor cores (NP passes), always QR-free.  Half the
@@ -716,7 +718,7 @@ __global__ void __launch_bounds__(kThreads, 1) walker_step_general_kernel(Dev p)
 template <int NP, bool ZB>
 __global__ void __launch_bounds__(kThreads, 2) walker_step_mixed_kernel(Dev p) {
   extern __shared__ double smem_raw[];
-  general_step<float, NP, ZB, 1>(p, smem_raw);
+  general_step<float, NP, ZB, 1, true>(p, smem_raw);
 }
 
 // <Psi_T|H|phi> / overlap for every walker (any coupling range), tensors as stored.
