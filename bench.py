@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--proposal", default="grid", choices=["grid", "learned"],
                     help="auxiliary-field proposal: the exact grid PDF, or the learned network (trained online "
                          "on the grid walk for --train-steps steps first; exact-ratio reweighting)")
-    ap.add_argument("--train-steps", type=int, default=30)
+    ap.add_argument("--train-steps", type=int, default=100)
     ap.add_argument("--canon", type=int, default=None, metavar="K",
                     help="QR-free sweep, left-normalise every K steps (0: Householder QR per site; "
                          "default: the engine's, 16)")
