@@ -35,9 +35,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="chain64", choices=["chain64", "snake6x6", "snake6x6_dmrg", "snake8x8"],
+    ap.add_argument("--workload", default="chain64", choices=["chain64", "snake6x6", "snake6x6_dmrg", "snake8x8",
+                                                               "snake8x8_dmrg"],
                     help="chain64: the L=64 chain (default line); snake6x6 / snake8x8: the 2D lattices "
-                         "(walkers compressed on the device; no CPU baseline or e2e)")
+                         "(walkers compressed on the device; no CPU baseline or e2e); *_dmrg: with "
+                         "their DMRG ground-state trials")
     ap.add_argument("--walkers", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -55,6 +57,9 @@ def parse():
                     help="auxiliary-field proposal: the exact grid PDF, or the learned network (trained online "
                          "on the grid walk for --train-steps steps first; exact-ratio reweighting)")
     ap.add_argument("--train-steps", type=int, default=100)
+    ap.add_argument("--proposal-mix", type=int, default=None, metavar="ALPHA",
+                    help="learned proposal: thousandths of the exact PDF in the defensive mixture it draws "
+                         "from (default: the engine's, 100)")
     ap.add_argument("--canon", type=int, default=None, metavar="K",
                     help="QR-free sweep, left-normalise every K steps (0: Householder QR per site; "
                          "default: the engine's, 16)")
@@ -76,9 +81,11 @@ PRECISIONS = {"fp64": 0, "tf32": 1, "tf32x3": 2}
 
 def configure(eng, args, sweep, plain=False):
     """Kernel and method options of a bench engine; plain: the FP64 grid walk (the VN yardstick)."""
-    from mpsqmc_b200.capi import (OPT_CANONICAL_INTERVAL, OPT_PRECISION, OPT_SWEEP, OPT_WORKSPACE,
-                                  WORKSPACE_GLOBAL)
+    from mpsqmc_b200.capi import (OPT_CANONICAL_INTERVAL, OPT_PRECISION, OPT_PROPOSAL_MIX, OPT_SWEEP,
+                                  OPT_WORKSPACE, WORKSPACE_GLOBAL)
     eng.set_option(OPT_SWEEP, sweep)
+    if args.proposal_mix is not None:
+        eng.set_option(OPT_PROPOSAL_MIX, args.proposal_mix)
     if args.workspace == "global":
         eng.set_option(OPT_WORKSPACE, WORKSPACE_GLOBAL)
     if args.canon is not None:
@@ -87,21 +94,35 @@ def configure(eng, args, sweep, plain=False):
         eng.set_option(OPT_PRECISION, PRECISIONS[args.precision])
 
 
-def train_proposal(eng, args):
-    """Online training of the learned proposal on the grid walk (untimed set-up); then the walk
-    samples from it.  Returns what the training did."""
-    from mpsqmc_b200.capi import OPT_PROPOSAL, OPT_PROPOSAL_TRAINING, PROPOSAL_LEARNED
+def train_proposal(make, args, sweep, seed):
+    """Online training of the learned proposal (untimed set-up) on a separate engine that walks
+    the grid walk from the start, so that the walk using the network starts where the other
+    variants start (the same imaginary time in every compared window).  Returns (network
+    parameters, what the training did), or (None, None) for the grid proposal."""
+    from mpsqmc_b200.capi import OPT_PROPOSAL_TRAINING
     if args.proposal != "learned":
-        return None
+        return None, None
+    eng = make()
+    configure(eng, args, sweep)
+    eng.set_rng(seed + 1, 0)
     eng.set_option(OPT_PROPOSAL_TRAINING, 1)
     t0 = time.perf_counter()
     st = eng.walk(args.train_steps)
     dt = time.perf_counter() - t0
     ps = eng.proposal_stats()
-    eng.set_option(OPT_PROPOSAL_TRAINING, 0)
-    eng.set_option(OPT_PROPOSAL, PROPOSAL_LEARNED)
-    return {"steps": args.train_steps, "pairs": int(sum(s["n_walkers"] for s in st)), "adam_steps": ps["updates"],
-            "final_kl": ps["loss"], "seconds": dt}
+    params = eng.proposal_params()
+    eng.close()
+    return params, {"steps": args.train_steps, "pairs": int(sum(s["n_walkers"] for s in st)),
+                    "adam_steps": ps["updates"], "final_kl": ps["loss"], "seconds": dt,
+                    "walk": "a separate engine from the same start"}
+
+
+def use_proposal(eng, params):
+    """The walk samples from the trained network (exact-ratio weights)."""
+    from mpsqmc_b200.capi import OPT_PROPOSAL, PROPOSAL_LEARNED
+    if params is not None:
+        eng.proposal_params(params)
+        eng.set_option(OPT_PROPOSAL, PROPOSAL_LEARNED)
 
 
 def dist_setup(n):
@@ -287,6 +308,7 @@ def main():
                "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.Ds, "dtau": wl.dtau,
                "parallelism": f"{'split walk' if args.sharded else 'replicas'} x{world}", "sweep": args.sweep,
                "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
+               "proposal_mix": args.proposal_mix if args.proposal_mix is not None else 100,
                "canonical_interval": args.canon if args.canon is not None else 16}
     else:
         wl = workloads.chain64(Nw=args.walkers or 2048)
@@ -296,6 +318,7 @@ def main():
                "l2": f"population ({wl.Nw * wl.walker.data.size * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
                "parallelism": f"{'split walk' if args.sharded else 'replicas'} x{world}", "sweep": args.sweep,
                "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
+               "proposal_mix": args.proposal_mix if args.proposal_mix is not None else 100,
                "canonical_interval": args.canon if args.canon is not None else 16}
 
     if args.impl == "reference":
@@ -330,21 +353,31 @@ def main():
     from mpsqmc_b200 import Engine
 
     sweep = {"auto": 0, "nearest": 1, "general": 2}[args.sweep]
+    seed = wl.seed + 7919 * rank
     if lattice:
         eng, inputs = lattice_engine(wl, local)
         walkers = None
         N = wl.Nw
         args.no_e2e = True
         args.no_cpu_baseline = True
+
+        def make():
+            return lattice_engine(wl, local)[0]
     else:
         inputs = wl.inputs()
         walkers = wl.walkers()
-        eng = Engine(device=local, **inputs)
         N = walkers.shape[0]
-        eng.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
+
+        def make():
+            e = Engine(device=local, **inputs)
+            e.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
+            return e
+
+        eng = make()
     configure(eng, args, sweep)
-    eng.set_rng(wl.seed + 7919 * rank, 0)
-    training = train_proposal(eng, args)
+    eng.set_rng(seed, 0)
+    params, training = train_proposal(make, args, sweep, seed)
+    use_proposal(eng, params)
     eng.walk(args.warmup)
     torch.cuda.synchronize()
     if pg is not None:
@@ -407,14 +440,11 @@ def main():
             proposal), warm-up, timed steps for its throughput, then the VN steps."""
             a = argparse.Namespace(**vars(args))
             a.precision, a.proposal = precision, proposal
-            if lattice:
-                e, _ = lattice_engine(wl, local)
-            else:
-                e = Engine(device=local, **inputs)
-                e.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
+            e = make()
             configure(e, a, sweep, plain=(precision == "fp64"))
-            e.set_rng(wl.seed + 7919 * rank, 0)
-            tr = train_proposal(e, a)
+            e.set_rng(seed, 0)
+            p_arm, tr = train_proposal(make, a, sweep, seed)
+            use_proposal(e, p_arm)
             e.walk(args.warmup)
             st = e.walk(args.steps)
             t = e.last_timing()
@@ -457,10 +487,7 @@ def main():
     if not args.no_e2e:
         eng2 = Engine(device=local, **inputs)
         configure(eng2, args, sweep)
-        if training:  # the trained network, as the timed engine walks with it
-            from mpsqmc_b200.capi import OPT_PROPOSAL, PROPOSAL_LEARNED
-            eng2.proposal_params(eng.proposal_params())
-            eng2.set_option(OPT_PROPOSAL, PROPOSAL_LEARNED)
+        use_proposal(eng2, params)  # the trained network, as the timed engine walks with it
         # the population in pinned host memory (both directions), as a serving caller would keep it
         host_w = torch.empty(walkers.shape, dtype=torch.float64, pin_memory=True).numpy()
         host_w[:] = walkers

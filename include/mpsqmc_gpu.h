@@ -227,6 +227,12 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
 #define MPSQMC_OPT_PROPOSAL_TRAINING 9 /* 1: every grid step also stores (features, exact PDF) of one
                                         * coupling per walker and takes one Adam step (step size
                                         * 1e-3) of the network on them (mean KL(P || q)) */
+#define MPSQMC_OPT_PROPOSAL_MIX 10   /* alpha in thousandths, 0..1000 (default 100): the learned
+                                      * proposal draws from the defensive mixture
+                                      * (1 - alpha) q + alpha P / sum P (Hesterberg, Technometrics
+                                      * 37 (1995) 185), so the weight factor P(x) / q_mix(x) is at
+                                      * most sum P / alpha and a poorly trained network cannot
+                                      * give heavy-tailed weights.  1000 samples the grid PDF. */
 int mpsqmc_set_option(mpsqmc_ctx *ctx, int option, long value);
 int mpsqmc_get_option(mpsqmc_ctx *ctx, int option, long *value);
 

@@ -30,6 +30,7 @@ PRECISION_FP64, PRECISION_TF32, PRECISION_TF32X3 = 0, 1, 2
 OPT_PROPOSAL = 8
 PROPOSAL_GRID, PROPOSAL_LEARNED = 0, 1
 OPT_PROPOSAL_TRAINING = 9
+OPT_PROPOSAL_MIX = 10  # thousandths of the exact PDF in the learned proposal's defensive mixture
 
 # Every symbol include/mpsqmc_gpu.h declares.
 EXPORTED = [

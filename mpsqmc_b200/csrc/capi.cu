@@ -110,6 +110,7 @@ struct mpsqmc_ctx {
   // and activations (allocated on first use)
   int proposal = MPSQMC_PROPOSAL_GRID;
   bool prop_train = false;
+  int prop_mix = 100;  // thousandths of the exact PDF in the learned proposal's mixture
   long nparams = 0;
   float *d_pw = nullptr, *d_pm = nullptr, *d_pv = nullptr, *d_pg = nullptr;
   __nv_bfloat16 *d_pwb = nullptr;
@@ -257,6 +258,7 @@ mq::Dev make_dev(mpsqmc_ctx *c) {
   const bool trotter = c->projector == MPSQMC_PROJECTOR_TROTTER;
   p.prop_mode = (c->proposal == MPSQMC_PROPOSAL_LEARNED && trotter && c->d_pwb) ? 1 : 0;
   p.prop_collect = (c->prop_train && c->proposal == MPSQMC_PROPOSAL_GRID && trotter && c->d_pwb) ? 1 : 0;
+  p.prop_mix = c->prop_mix * 1e-3;
   p.prop_w = c->d_pwb;
   p.prop_feat = c->d_pfeat;
   p.prop_target = c->d_ptarget;
@@ -1506,6 +1508,10 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
         if (rc) return rc;
       }
       break;
+    case MPSQMC_OPT_PROPOSAL_MIX:
+      if (value < 0 || value > 1000) return fail(MPSQMC_E_ARG, "proposal mixture is 0..1000 thousandths");
+      c->prop_mix = (int)value;
+      break;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");
   }
@@ -1542,6 +1548,9 @@ int mpsqmc_get_option(mpsqmc_ctx *c, int option, long *value) {
       return 0;
     case MPSQMC_OPT_PROPOSAL_TRAINING:
       *value = c->prop_train ? 1 : 0;
+      return 0;
+    case MPSQMC_OPT_PROPOSAL_MIX:
+      *value = c->prop_mix;
       return 0;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");

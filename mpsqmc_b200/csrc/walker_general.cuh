@@ -346,8 +346,9 @@ static __device__ double sample_coupling(const Dev &p, SmemT<T> &s, int w, int c
       s.qprop[g] = e;
       se += e;
     }
-    const double qinv = 1.0 / cta_sum(se, s.red);
-    for (int g = tid; g < p.G; g += kThreads) s.qprop[g] *= qinv;
+    // the defensive mixture (1 - alpha) q~ + alpha P / sum P: P / q_mix <= sum P / alpha
+    const double qinv = (1.0 - p.prop_mix) / cta_sum(se, s.red), pinv = pnorm > 0.0 ? p.prop_mix / pnorm : 0.0;
+    for (int g = tid; g < p.G; g += kThreads) s.qprop[g] = s.qprop[g] * qinv + s.pdf[g] * pinv;
     __syncthreads();
   }
   if (tid == 0) {

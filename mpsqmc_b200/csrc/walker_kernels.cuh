@@ -88,6 +88,7 @@ struct Dev {
   // learned proposal (proposal.cuh)
   int prop_mode;                 // 0: the exact grid PDF; 1: the network's proposal, exact-ratio weights
   int prop_collect;              // 1: store (features, PDF) of coupling w % nC of every walker w
+  double prop_mix;               // learned proposal: weight of the exact PDF in the drawn mixture
   const __nv_bfloat16 *prop_w;   // network parameters (BF16 copy)
   float *prop_feat, *prop_target;  // [capacity][32], [capacity][G]
 };

@@ -1,11 +1,12 @@
 """Regenerate the stored trial states of the named workloads (mpsqmc_b200/workloads.py).
 
-    python mpsqmc_b200/data/make_trials.py [chain64] [snake6x6]
+    python mpsqmc_b200/data/make_trials.py [chain64] [snake6x6] [snake8x8]
 
 chain64:  trial_L64D64.npz, the open L=64 Heisenberg chain at D_T = 64;
-snake6x6: trial_snake6x6_D64.npz, the open 6x6 lattice on the snake path at D_T = 64.
+snake6x6: trial_snake6x6_D64.npz, the open 6x6 lattice on the snake path at D_T = 64;
+snake8x8: trial_snake8x8_D64.npz, the open 8x8 lattice on the snake path at D_T = 64.
 
-Both come from the compact-MPO two-site DMRG (mpsqmc_b200/dmrg.py, seed 7), left-normalised,
+All come from the compact-MPO two-site DMRG (mpsqmc_b200/dmrg.py, seed 7), left-normalised,
 in the reference's storage layout, with the DMRG energy beside them.
 """
 import os
@@ -28,6 +29,9 @@ def make(name: str) -> None:
     elif name == "snake6x6":
         m, e = dmrg.dmrg(36, 64, couplings=pb.snake(6, 6))
         out = "trial_snake6x6_D64.npz"
+    elif name == "snake8x8":
+        m, e = dmrg.dmrg(64, 64, couplings=pb.snake(8, 8))
+        out = "trial_snake8x8_D64.npz"
     else:
         raise SystemExit(f"unknown trial {name!r}")
     np.savez(os.path.join(HERE, out), dims=m.dims, data=m.data, energy=e)
@@ -35,5 +39,5 @@ def make(name: str) -> None:
 
 
 if __name__ == "__main__":
-    for n in sys.argv[1:] or ["chain64", "snake6x6"]:
+    for n in sys.argv[1:] or ["chain64", "snake6x6", "snake8x8"]:
         make(n)

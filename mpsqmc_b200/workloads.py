@@ -8,6 +8,8 @@ snake6x6, snake8x8   open 6x6 / 8x8 lattices on the snake path with seeded rando
           D_T bond profile (throughput: the work per walker-step does not depend on the trial).
 snake6x6_dmrg   the open 6x6 lattice with its ground-state trial from the compact-MPO DMRG at
           D_T = 64 (mpsqmc_b200/data, made by data/make_trials.py), walkers of D_W in {16, 32, 64}.
+snake8x8_dmrg   the open 8x8 lattice with its DMRG ground-state trial at D_T = 64, walkers of D_W
+          in {32, 64}.
 """
 from __future__ import annotations
 
@@ -178,6 +180,12 @@ def snake6x6_dmrg(Nw: int = 1024) -> LatticeWorkload:
     """6x6 open lattice with its DMRG ground-state trial (D_T = 64), walkers of D_W drawn from
     {16, 32, 64}, dtau 0.005."""
     return LatticeWorkload("snake6x6_dmrg", 6, 6, 64, [16, 32, 64], Nw, 0.005, trial_file="trial_snake6x6_D64.npz")
+
+
+def snake8x8_dmrg(Nw: int = 1024) -> LatticeWorkload:
+    """8x8 open lattice with its DMRG ground-state trial (D_T = 64), walkers of D_W drawn from
+    {32, 64}, dtau 0.005."""
+    return LatticeWorkload("snake8x8_dmrg", 8, 8, 64, [32, 64], Nw, 0.005, trial_file="trial_snake8x8_D64.npz")
 
 
 def snake8x8(Nw: int = 4096) -> LatticeWorkload:

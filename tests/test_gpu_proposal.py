@@ -4,17 +4,19 @@ training, and what it changes in the walk.
 The grid PDF P(x) of one coupling is the zero-variance proposal for that coupling's weight
 factor: drawing x from P / sum P multiplies the weight by sum P whatever x is.  The learned
 proposal q~ reweights by P(x) / q~(x), whose mean over x ~ q~ is again sum P (unbiased) and whose
-spread is what q~ loses against P / sum P.  The tests check the forward pass, loss and gradient
-against oracle/mlp.py, that online training drives the loss down, and that a trained network's
-weight factors scatter far less around sum P than an untrained one's.
+spread is what q~ loses against P / sum P.  The walk draws from the defensive mixture
+q_mix = (1 - alpha) q~ + alpha P / sum P (MPSQMC_OPT_PROPOSAL_MIX), which bounds the factor by
+sum P / alpha.  The tests check the forward pass, loss and gradient against oracle/mlp.py, that
+online training drives the loss down, that a trained network's weight factors scatter far less
+around sum P than an untrained one's, and the mixture's bound.
 """
 import numpy as np
 import pytest
 
 from conftest import couplings, load_golden
 from mpsqmc_b200 import Engine
-from mpsqmc_b200.capi import (OPT_CANONICAL_INTERVAL, OPT_PROPOSAL, OPT_PROPOSAL_TRAINING, PROPOSAL_GRID,
-                              PROPOSAL_LEARNED)
+from mpsqmc_b200.capi import (E_ARG, OPT_CANONICAL_INTERVAL, OPT_PROPOSAL, OPT_PROPOSAL_MIX, OPT_PROPOSAL_TRAINING,
+                              PROPOSAL_GRID, PROPOSAL_LEARNED, MpsqmcError)
 from oracle import mlp
 
 pytestmark = pytest.mark.gpu
@@ -81,6 +83,7 @@ def test_online_training_lowers_the_loss_and_the_weight_spread():
     def factors(params, proposal):
         e, _ = chain_engine()
         e.set_option(OPT_CANONICAL_INTERVAL, 1)
+        e.set_option(OPT_PROPOSAL_MIX, 0)  # the network's own proposal
         if params is not None:
             e.proposal_params(params)
         e.set_option(OPT_PROPOSAL, proposal)
@@ -94,3 +97,31 @@ def test_online_training_lowers_the_loss_and_the_weight_spread():
     for r in (r_trained, r_untrained):
         assert abs(np.mean(r) - 1.0) < 4.0 * np.std(r) / np.sqrt(n) + 1e-12
     assert np.std(r_trained) < 0.5 * np.std(r_untrained), (np.std(r_trained), np.std(r_untrained))
+
+
+def test_defensive_mixture_bounds_the_weight_factor():
+    """An untrained network through the default mixture (alpha = 0.1): every factor within
+    sum P / alpha, still unbiased; alpha = 1 draws from P itself, so every factor is sum P."""
+    def factors(mix):
+        e, z = chain_engine()
+        e.set_option(OPT_CANONICAL_INTERVAL, 1)
+        if mix is not None:
+            e.set_option(OPT_PROPOSAL_MIX, mix)
+        assert e.get_option(OPT_PROPOSAL_MIX) == (100 if mix is None else mix)
+        e.proposal_params(mlp.init_params(z["grid"].shape[0], seed=11).astype(np.float32))
+        e.set_option(OPT_PROPOSAL, PROPOSAL_LEARNED)
+        return weight_factors(e)
+
+    e, _ = chain_engine()
+    e.set_option(OPT_CANONICAL_INTERVAL, 1)
+    pn = weight_factors(e)
+    for bad in (-1, 1001):
+        with pytest.raises(MpsqmcError) as ei:
+            e.set_option(OPT_PROPOSAL_MIX, bad)
+        assert ei.value.code == E_ARG
+    r = factors(None) / pn
+    assert np.all(r <= 10.0 * (1 + 1e-12)) and np.all(r > 0)
+    assert abs(np.mean(r) - 1.0) < 4.0 * np.std(r) / np.sqrt(len(r)) + 1e-12
+    r_net = factors(0) / pn
+    assert np.std(r) < np.std(r_net)
+    np.testing.assert_allclose(factors(1000), pn, rtol=1e-12)

@@ -215,17 +215,18 @@ def test_lattice_dmrg_reaches_ed():
     assert dmrg.mpo_energy(m, dmrg.coupling_mpo(16, *c44)) == pytest.approx(e, rel=1e-9)
 
 
-def test_stored_lattice_trial_is_the_dmrg_state():
-    """The 6x6 workload's stored trial: left-normalised, bond dims within D_T = 64, and its
+@pytest.mark.parametrize("name", ["snake6x6_dmrg", "snake8x8_dmrg"])
+def test_stored_lattice_trial_is_the_dmrg_state(name):
+    """The lattice workloads' stored trials: left-normalised, bond dims within D_T = 64, and the
     energy under the lattice's compact MPO is the stored DMRG energy (a variational bound)."""
     import numpy as np
     from mpsqmc_b200 import dmrg, workloads
-    wl = workloads.snake6x6_dmrg()
+    wl = getattr(workloads, name)()
     m = wl.trial()
-    assert m.L == 36 and int(max(m.dims)) == wl.DT
-    e = dmrg.mpo_energy(m, dmrg.coupling_mpo(36, *wl.couplings()))
+    assert m.L == wl.L and int(max(m.dims)) == wl.DT
+    e = dmrg.mpo_energy(m, dmrg.coupling_mpo(wl.L, *wl.couplings()))
     assert e == pytest.approx(wl.trial_energy(), rel=1e-9)
-    assert -0.62 * 36 < e < -0.55 * 36
+    assert -0.62 * wl.L < e < -0.55 * wl.L
     for k in range(m.L - 1):
         A = m.site(k)  # [sigma, Dl, Dr]
         G = sum(A[s].T @ A[s] for s in range(2))
