@@ -124,6 +124,7 @@ using Smem = SmemT<double>;
 __host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, int pa, int pb, int pq,
                                               Smem *s, double *base, double *big = nullptr,
                                               long *big_doubles = nullptr, bool mlp = false, bool qr = true) {
+  (void)maxA;  // the blocks are sized by the padded pa, pb
   long off = 0, boff = 0;
   double *dummy;
   auto take = [&](double *&p, long n) {
@@ -191,6 +192,7 @@ __host__ __device__ inline long smem_doubles(int L, int maxA, int maxB, int G, i
 __host__ __device__ inline long smem_bytes_f32(int L, int maxA, int maxB, int G, int pa, int pb,
                                                SmemT<float> *s, double *base, float *big = nullptr,
                                                long *big_floats = nullptr, bool mlp = false) {
+  (void)maxA;  // the blocks are sized by the padded pa, pb
   long off = 0, boff = 0;  // doubles of the small buffers; floats of the matrix buffers
   double *dummy;
   float *fdummy;

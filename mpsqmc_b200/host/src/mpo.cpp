@@ -115,7 +115,7 @@ void HeisenbergMPO::refresh() const {
   MPOdimensions[0] = 1;
   MPOdimensions[L] = 1;
   for (int b = 1; b < L; ++b) MPOdimensions[b] = 2 + 3 * (int)open[b].size();
-  auto done = [&](int b) { return 0; };
+  auto done = [](int) { return 0; };  // the "done" channel is index 0 on every bond
   auto start = [&](int b) { return b == 0 ? 0 : 1 + 3 * (int)open[b].size(); };
   auto chan = [&](int b, int i, int op) {
     for (size_t q = 0; q < open[b].size(); ++q)
