@@ -492,6 +492,12 @@ def main():
         host_w = torch.empty(walkers.shape, dtype=torch.float64, pin_memory=True).numpy()
         host_w[:] = walkers
         back_w = torch.empty((eng2.capacity, eng2.walker_size), dtype=torch.float64, pin_memory=True).numpy()
+        # untimed warm-up on this engine, as for the device-timed steps (step graphs captured, kernels
+        # loaded); the timed run then starts again from the host population
+        eng2.set_walkers(host_w, np.ones(N), None, np.zeros(N), normalize=True)
+        eng2.set_rng(wl.seed + 7919 * rank, 0)
+        eng2.walk(args.warmup)
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         eng2.set_walkers(host_w, np.ones(N), None, np.zeros(N), normalize=True)
         eng2.set_rng(wl.seed + 7919 * rank, 0)
