@@ -1,5 +1,6 @@
-"""The bench's multi-rank path on CPU: two gloo ranks aggregate their timings (max of the times,
-sum of the walker-steps), and the reference arm under torchrun runs on rank 0 only."""
+"""The bench on CPU: two gloo ranks aggregate their timings (max of the times, sum of the
+walker-steps), the reference arm under torchrun runs on rank 0 only, and the learned-proposal
+arm trains on an engine of its own."""
 import json
 import os
 import socket
@@ -58,3 +59,55 @@ def test_reference_arm_under_torchrun_prints_once():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["kind"] == "reference"
+
+
+def test_learned_arm_trains_on_a_separate_engine():
+    """The VN comparison's learned arm: the network trains on its own engine (grid walk from the
+    start, then closed) and only its parameters reach the measured engine, which has not walked."""
+    import argparse
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+    from mpsqmc_b200.capi import OPT_PROPOSAL, OPT_PROPOSAL_TRAINING, PROPOSAL_LEARNED
+
+    made = []
+
+    class Fake:
+        def __init__(self):
+            self.opts, self.steps, self.closed, self.params = {}, 0, False, None
+            made.append(self)
+
+        def set_option(self, k, v):
+            self.opts[k] = v
+
+        def set_rng(self, seed, skip):
+            self.seed = seed
+
+        def walk(self, n):
+            self.steps += n
+            return [{"n_walkers": 4}] * n
+
+        def proposal_stats(self):
+            return {"updates": self.steps, "loss": 0.5}
+
+        def proposal_params(self, p=None):
+            if p is None:
+                return np.full(3, float(len(made)))
+            self.params = p
+
+        def close(self):
+            self.closed = True
+
+    args = argparse.Namespace(proposal="learned", train_steps=7, workspace="auto", canon=None, precision="tf32x3",
+                              proposal_mix=None)
+    measured = Fake()
+    params, info = bench.train_proposal(Fake, args, 0, 11)
+    bench.use_proposal(measured, params)
+    trainer = made[1]
+    assert trainer is not measured and trainer.closed and trainer.steps == 7
+    assert trainer.opts[OPT_PROPOSAL_TRAINING] == 1
+    assert measured.steps == 0 and measured.opts[OPT_PROPOSAL] == PROPOSAL_LEARNED
+    np.testing.assert_array_equal(measured.params, params)
+    assert info["adam_steps"] == 7 and info["pairs"] == 28
+    args.proposal = "grid"
+    assert bench.train_proposal(Fake, args, 0, 11) == (None, None)
