@@ -62,6 +62,7 @@ static __device__ void right_env_step(const Dev &p, SmemT<T> &s, const double *W
   const int d = kMaxD;
   const int al = p.aT[k], ar = p.aT[k + 1], bl = s.bW[k], br = s.bW[k + 1];
   load_site(s.Nxt, p.pb, s.sbC, W + s.woff[k], bl, br);
+  if (k > 1) prefetch_l2(W + s.woff[k - 1], (long)s.bW[k - 1] * bl * kMaxD);  // the next site of the sweep
   __syncthreads();
   const T *Rn = scr + p.roff[k + 1];
   T *Rk = scr + p.roff[k];
@@ -525,6 +526,12 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
     for (int i = 0; i < L; ++i) {
       const int al = p.aT[i], ar = p.aT[i + 1], bl = s.bW[i], br = s.bW[i + 1];
       const T *Bi = trial + p.toff[i];
+      // the walker's next site, and on chains the right branches this site's coupling closes with
+      // (formed in the right-environment sweep, since evicted from L2): fetched ahead
+      if (i + 1 < L) {
+        prefetch_l2(W + s.woff[i + 1], (long)br * s.bW[i + 2] * d);
+        if constexpr (ZB) prefetch_l2(scr + p.zoff[i + 1], 4L * ar * br);
+      }
       // Pb still holds the last coupling's left branches at cut i+1 (its partner was i+1, so they
       // were not carried further, and the trace did not use Pb as scratch)
       bool branches_kept = false;
@@ -548,6 +555,7 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
         for (int m = i + 1; m < j; ++m) {
           const int am = p.aT[m], am1 = p.aT[m + 1], bm = s.bW[m], bm1 = s.bW[m + 1];
           load_site(s.Nxt, p.pb, s.sbC, W + s.woff[m], bm, bm1);
+          if (m + 1 < j) prefetch_l2(W + s.woff[m + 1], (long)bm1 * s.bW[m + 2] * d);
           __syncthreads();
           const T *Bm = trial + p.toff[m];
           for (int q = 0; q < kN2; ++q)

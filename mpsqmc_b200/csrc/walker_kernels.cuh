@@ -299,6 +299,15 @@ __device__ __forceinline__ void load_site(T *dst, int ld, int sb, const double *
     dst[s * sb + r + ld * c] = T(src[q]);
   }
 }
+// Hint the L2 to fetch the n elements at p (global memory) ahead of their use: one prefetch per
+// 128-byte line, spread over the CTA's threads.  Nothing waits for it.
+template <typename T>
+__device__ __forceinline__ void prefetch_l2(const T *p, long n) {
+  const char *b = reinterpret_cast<const char *>(p);
+  const long bytes = n * (long)sizeof(T);
+  for (long o = 128L * threadIdx.x; o < bytes; o += 128L * kThreads)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(b + o));
+}
 template <typename T>
 __device__ __forceinline__ void store_site(double *dst, const T *src, int ld, int sb, int dl, int dr) {
   const int n = dl * dr * kMaxD;
