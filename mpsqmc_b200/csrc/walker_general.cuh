@@ -541,6 +541,10 @@ __device__ __forceinline__ void general_step(const Dev &p, double *smem_raw) {
           --rv;
           right_env_step<T, NP, ZB>(p, s, W, scr, rv);
         }
+        if constexpr (!ZB) {  // what the closures read after the middle sites: site j and R[j+1]
+          if (j > i + 1) prefetch_l2(W + s.woff[j], (long)s.bW[j] * s.bW[j + 1] * d);
+          prefetch_l2(scr + p.roff[j + 1], (long)p.aT[j + 1] * s.bW[j + 1]);
+        }
         // left branches P[s + d t] = B_i[s]^T Lenv C[t] (a_{i+1} x b_{i+1})
         for (int tau = 0; tau < d; ++tau)
           gemm_t<NP>(al, br, bl, T(1), s.Lenv, p.pa, false, s.Cen + tau * s.sbC, p.pb, false, T(0),
