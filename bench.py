@@ -64,7 +64,7 @@ def parse():
                     help="QR-free sweep, left-normalise every K steps (0: Householder QR per site; "
                          "default: the engine's, 16)")
     ap.add_argument("--vn-compare", type=int, default=None, metavar="STEPS",
-                    help="variance-normalised throughput (the BASELINE metric) of the plain FP64 grid walk "
+                    help="variance-normalised throughput (the headline metric) of the plain FP64 grid walk "
                          "and of the --vn-arms variants, STEPS steps each after their timed steps, from the "
                          "same start and random stream; ratios against the plain walk (default: 300 on the "
                          "default chain64 run, else off)")

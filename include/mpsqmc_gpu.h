@@ -204,8 +204,8 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
                                          * last step did not.  Applies to the Trotter projector's
                                          * general sweep; with h != 0 the walkers are
                                          * left-normalised every step anyway. */
-#define MPSQMC_OPT_PRECISION 7       /* arithmetic of the walker-step contractions (the set_precision
-                                      * of the C ABI the north star lists): */
+#define MPSQMC_OPT_PRECISION 7       /* arithmetic of the walker-step contractions (what a
+                                      * set_precision(FP64 | TF32 | ...) entry point would select): */
 #define MPSQMC_PRECISION_FP64 0      /*   FP64 tensor cores (DMMA), the reference's arithmetic (default) */
 #define MPSQMC_PRECISION_TF32 1      /*   FP32 work buffers, one TF32 tensor-core pass per product */
 #define MPSQMC_PRECISION_TF32X3 2    /*   FP32 work buffers, three TF32 passes (head/tail split):
@@ -216,8 +216,8 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
                                       *   steps, 4 when that option is 0) and apply to the general
                                       *   sweep of the Trotter projector; the per-coupling trace is
                                       *   FP64-only (MPSQMC_E_UNSUPPORTED). */
-#define MPSQMC_OPT_PROPOSAL 8        /* how a coupling's grid point is drawn (the set_proposal of the
-                                      * north star's C ABI): */
+#define MPSQMC_OPT_PROPOSAL 8        /* how a coupling's grid point is drawn (what a
+                                      * set_proposal(GRID | LEARNED) entry point would select): */
 #define MPSQMC_PROPOSAL_GRID 0       /*   the exact grid PDF, as MPSQMC2.cpp:551-588 (default) */
 #define MPSQMC_PROPOSAL_LEARNED 1    /*   the learned proposal q: the point is drawn from q restricted
                                       *   to the PDF's support and the weight takes P(x) / q(x)
