@@ -29,6 +29,20 @@ def test_library_exports_every_declared_symbol():
     assert b"sm_100a" in lib.mpsqmc_version()
 
 
+def test_python_constants_match_the_header():
+    """Every integer constant of the binding equals the header's #define of the same name
+    (MPSQMC_ prefix), and every option, status and value the header defines is bound."""
+    hdr = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "mpsqmc_gpu.h")).read(), flags=re.S)
+    defs = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define MPSQMC_(\w+)\s+\(?(-?\d+)\)?\s*$", hdr, re.M)}
+    assert "OPT_PROPOSAL_MIX" in defs and defs["E_ARG"] == -1
+    skip = {"NOALLOC_MAX_L"}  # a size limit of the allocation-free entry point, checked in its own test
+    for name, v in defs.items():
+        if name in skip:
+            continue
+        assert hasattr(capi, name), name
+        assert getattr(capi, name) == v, (name, getattr(capi, name), v)
+
+
 def test_create_without_device_fails_loudly():
     import torch
     if torch.cuda.is_available():
