@@ -300,9 +300,13 @@ int mpsqmc_autotune(mpsqmc_ctx *ctx, int steps, int *best_sweep, int *best_works
  *   trial:   device, reference layout for trial_dims;
  *   walkers: device, walker w at walkers + w * walker_stride, reference layout for walker_dims;
  *   overlaps, energies: device, n_walkers doubles each.
- * Limits: L <= MPSQMC_NOALLOC_MAX_L, d = 2, and the environment scratch of one CTA,
- * 8 * max(trial_dims) * max(walker_dims) doubles, must fit in the array; larger problems are
- * rejected with MPSQMC_E_UNSUPPORTED and a message in mpsqmc_last_error().
+ * Limits: L <= MPSQMC_NOALLOC_MAX_L, d = 2, and one CTA's slice of the array must hold the
+ * compact-MPO environments, 8 * max(trial_dims) * max(walker_dims) doubles, plus - when they do
+ * not fit in the device's shared memory beside the small buffers (about max bond 32 x 64 on a
+ * B200) - the matrix work buffers, about 12 * (max(trial_dims) + 4) * max(walker_dims) doubles:
+ * up to trial and walker bond dimension ~180 in the 8 MiB array.  Larger problems are rejected
+ * with MPSQMC_E_UNSUPPORTED and a message in mpsqmc_last_error(), also when n_walkers is 0.
+ * The bond tables travel as a kernel argument: a call issues no host-to-device copy.
  * The first call on a device (with that device current) looks up the array's device address
  * and raises the kernel's shared-memory limit; make that first call before any stream capture.
  * Every call reuses the same array and leaves its contents behind; each call writes every

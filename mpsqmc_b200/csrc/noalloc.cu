@@ -2,10 +2,12 @@
 // allocate device memory.  All scratch lives in one file-scope device array (g_noalloc_scratch);
 // the caller supplies the inputs and the output buffer.
 //
-// Array layout: [ Tables (bond dims, site offsets, bond couplings) | per-CTA environments ].
-// The host never dereferences the array's name (in host code it is only a stand-in symbol): at
-// the first call on a device, with that device current, cudaGetSymbolAddress gives the device
-// address, which is kept per device and passed to the kernel.
+// Array layout: per-CTA slices of [ compact-MPO environments | matrix work buffers, when they do
+// not fit in shared memory ].  The bond-dimension tables travel as a kernel parameter, so a call
+// issues no host-to-device copy.  The host never dereferences the array's name (in host code it
+// is only a stand-in symbol): at the first call on a device, with that device current,
+// cudaGetSymbolAddress gives the device address, which is kept per device and passed to the
+// kernel.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,7 +39,6 @@ struct Tables {
   long woff[kMaxL];
   double bondJ[kMaxL];
 };
-constexpr size_t kTablesDoubles = (sizeof(Tables) + 255) / 256 * 256 / sizeof(double);
 
 struct DeviceSetup {
   bool ready = false;
@@ -49,14 +50,18 @@ constexpr int kMaxDevices = 64;
 DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mutex;
 
+// tab: the bond tables by value (a __grid_constant__ parameter, read in place).  big_off >= 0:
+// the matrix work buffers sit at that offset of the CTA's slice instead of shared memory.
 __global__ void __launch_bounds__(mq::kThreads, 1)
-    energy_noalloc_kernel(mq::Dev p, const double *walkers, long wstride, const double *ov,
-                          double *out, int N) {
+    energy_noalloc_kernel(mq::Dev p, const __grid_constant__ Tables tab, long big_off, const double *walkers,
+                          long wstride, const double *ov, double *out, int N) {
   extern __shared__ double smem_raw[];
   mq::Smem s;
-  mq::smem_doubles(p.L, p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw);
+  double *slice = p.scratch + (long)blockIdx.x * p.scr_stride;
+  mq::smem_doubles(p.L, p.maxA, p.maxB, p.G, p.pa, p.pb, p.pq, &s, smem_raw, big_off >= 0 ? slice + big_off : nullptr,
+                   nullptr, false, false);
   const int L = p.L, tid = threadIdx.x;
-  double *Fbuf = p.scratch + (long)blockIdx.x * p.scr_stride;
+  double *Fbuf = slice;
   const int fst = 4 * p.maxA * p.maxB;
   for (int w = blockIdx.x; w < N; w += gridDim.x) {
     const double *W = walkers + (long)w * wstride;
@@ -64,9 +69,9 @@ __global__ void __launch_bounds__(mq::kThreads, 1)
     __syncthreads();
     int cur = 0;
     for (int k = 0; k < L; ++k) {
-      const int al = p.aT[k], ar = p.aT[k + 1], bl = p.bW[k], br = p.bW[k + 1];
-      mq::env_update(p, s, p.trial + p.toff[k], al, ar, bl, br, W + p.woff[k], bl, bl * br,
-                     Fbuf + cur * fst, Fbuf + (1 - cur) * fst, (k > 0) ? p.bondJ[k - 1] : 0.0, k == 0);
+      const int al = tab.aT[k], ar = tab.aT[k + 1], bl = tab.bW[k], br = tab.bW[k + 1];
+      mq::env_update(p, s, p.trial + tab.toff[k], al, ar, bl, br, W + tab.woff[k], bl, bl * br,
+                     Fbuf + cur * fst, Fbuf + (1 - cur) * fst, (k > 0) ? tab.bondJ[k - 1] : 0.0, k == 0);
       cur = 1 - cur;
     }
     if (tid == 0) out[w] = Fbuf[cur * fst] / ov[w];
@@ -151,14 +156,20 @@ extern "C" int mpsqmc_local_energy_noalloc(const mpsqmc_energy_layout *lay, cons
     wo += (long)tab.bW[k] * tab.bW[k + 1] * 2;
   }
   if (walker_stride < wo) return err(MPSQMC_E_ARG, "walker_stride smaller than one walker");
-  const long per_cta = ((2L * 4 * maxA * maxB) + 31) & ~31L;
-  const long avail = (long)kScratchDoubles - (long)kTablesDoubles;
-  if (per_cta > avail)
-    return err(MPSQMC_E_UNSUPPORTED, "bond dimensions need " + std::to_string(per_cta * 8) +
+  // per CTA: the compact-MPO environments (2 x 4 blocks, ld maxA) and, when they do not fit in
+  // shared memory beside the small buffers, the matrix work buffers (no Householder panel)
+  const int pa = mq::padld(maxA), pb = mq::padld(maxB), pq = mq::padld(2 * maxB);
+  long big_doubles = 0;
+  double one = 0.0;
+  const long smem_small = mq::smem_doubles(L, maxA, maxB, 1, pa, pb, pq, nullptr, nullptr, &one, &big_doubles,
+                                           false, false);
+  const long env_doubles = ((2L * 4 * maxA * maxB) + 31) & ~31L;
+  const long avail = (long)kScratchDoubles;
+  if (device < 0 || device >= kMaxDevices) return err(MPSQMC_E_ARG, "device ordinal out of range");
+  if (env_doubles > avail)
+    return err(MPSQMC_E_UNSUPPORTED, "bond dimensions need " + std::to_string(env_doubles * 8) +
                                          " bytes of scratch per CTA; the static array holds " +
                                          std::to_string(avail * 8));
-  if (device < 0 || device >= kMaxDevices) return err(MPSQMC_E_ARG, "device ordinal out of range");
-  if (n_walkers == 0) return 0;
 
   int prev = -1;
   if (cudaGetDevice(&prev) != cudaSuccess) return err(MPSQMC_E_NODEVICE, "no CUDA device");
@@ -166,47 +177,42 @@ extern "C" int mpsqmc_local_energy_noalloc(const mpsqmc_energy_layout *lay, cons
   DeviceSetup *st = nullptr;
   int rc = setup_device(device, &st);
   if (rc == 0) {
-    mq::Dev p;
-    std::memset(&p, 0, sizeof p);
-    p.L = L;
-    p.d = 2;
-    p.G = 1;
-    p.maxA = maxA;
-    p.maxB = maxB;
-    p.pa = mq::padld(maxA);
-    p.pb = mq::padld(maxB);
-    p.pq = mq::padld(2 * maxB);
-    Tables *dtab = reinterpret_cast<Tables *>(st->scratch);
-    p.aT = dtab->aT;
-    p.bW = dtab->bW;
-    p.toff = dtab->toff;
-    p.woff = dtab->woff;
-    p.bondJ = dtab->bondJ;
-    p.trial = trial;
-    p.h = lay->h;
-    for (int a = 0; a < 2; ++a)
-      for (int b = 0; b < 2; ++b) {
-        p.opSz[a + 2 * b] = (a == b) ? (a == 0 ? -0.5 : 0.5) : 0.0;
-        p.opSx[a + 2 * b] = (a != b) ? 0.5 : 0.0;
-        p.opISy[a + 2 * b] = (a == b + 1) ? 0.5 : ((a + 1 == b) ? -0.5 : 0.0);
-      }
-    p.scratch = st->scratch + kTablesDoubles;
-    p.scr_stride = per_cta;
-    const size_t smem = sizeof(double) * (size_t)mq::smem_doubles(p.L, maxA, maxB, 1, p.pa, p.pb, p.pq, nullptr, nullptr);
-    if ((int)smem > st->smem_optin) {
+    const bool on_chip = (smem_small + big_doubles) * (long)sizeof(double) <= (long)st->smem_optin;
+    const long per_cta = on_chip ? env_doubles : env_doubles + ((big_doubles + 31) & ~31L);
+    const size_t smem = sizeof(double) * (size_t)(on_chip ? smem_small + big_doubles : smem_small);
+    if (per_cta > avail) {
+      rc = err(MPSQMC_E_UNSUPPORTED, "bond dimensions need " + std::to_string(per_cta * 8) +
+                                         " bytes of scratch per CTA; the static array holds " +
+                                         std::to_string(avail * 8));
+    } else if ((int)smem > st->smem_optin) {
       rc = err(MPSQMC_E_UNSUPPORTED, "bond dimensions exceed the shared-memory budget of one CTA");
-    } else {
+    } else if (n_walkers > 0) {
+      mq::Dev p;
+      std::memset(&p, 0, sizeof p);
+      p.L = L;
+      p.d = 2;
+      p.G = 1;
+      p.maxA = maxA;
+      p.maxB = maxB;
+      p.pa = pa;
+      p.pb = pb;
+      p.pq = pq;
+      p.trial = trial;
+      p.h = lay->h;
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+          p.opSz[a + 2 * b] = (a == b) ? (a == 0 ? -0.5 : 0.5) : 0.0;
+          p.opSx[a + 2 * b] = (a != b) ? 0.5 : 0.0;
+          p.opISy[a + 2 * b] = (a == b + 1) ? 0.5 : ((a + 1 == b) ? -0.5 : 0.0);
+        }
+      p.scratch = st->scratch;
+      p.scr_stride = per_cta;
       cudaStream_t s = static_cast<cudaStream_t>(stream);
-      cudaError_t e = cudaMemcpyAsync(st->scratch, &tab, sizeof tab, cudaMemcpyHostToDevice, s);
-      if (e != cudaSuccess) {
-        rc = err(MPSQMC_E_CUDA, std::string("table upload: ") + cudaGetErrorString(e));
-      } else {
-        const int grid = (int)std::max(1L, std::min({(long)n_walkers, (long)st->sm_count, avail / per_cta}));
-        energy_noalloc_kernel<<<grid, mq::kThreads, smem, s>>>(p, walkers, walker_stride, overlaps, energies,
-                                                             n_walkers);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) rc = err(MPSQMC_E_CUDA, std::string("launch: ") + cudaGetErrorString(e));
-      }
+      const int grid = (int)std::max(1L, std::min({(long)n_walkers, (long)st->sm_count, avail / per_cta}));
+      energy_noalloc_kernel<<<grid, mq::kThreads, smem, s>>>(p, tab, on_chip ? -1L : env_doubles, walkers,
+                                                           walker_stride, overlaps, energies, n_walkers);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) rc = err(MPSQMC_E_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     }
   }
   if (prev >= 0 && prev != device) cudaSetDevice(prev);

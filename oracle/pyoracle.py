@@ -23,6 +23,12 @@ HARNESS_PATH = os.path.join(HERE, "_ref", "ref_harness")
 _lib = None
 
 
+def ref_dir() -> str | None:
+    """The reference source tree named by MPSQMC_REF_DIR, or None when it is unset or absent."""
+    d = os.environ.get("MPSQMC_REF_DIR")
+    return d if d and os.path.isfile(os.path.join(d, "MPSQMC2.cpp")) else None
+
+
 def build(ref: bool = False) -> None:
     """Compile the oracle library (and the reference harness when the reference tree exists)."""
     targets = ["oracle"] + (["ref"] if ref else [])

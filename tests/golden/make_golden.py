@@ -24,7 +24,9 @@ sys.path.insert(0, ROOT)
 from oracle import pyoracle as po  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
-REF_DIR = os.environ.get("MPSQMC_REF_DIR", "/root/reference")
+REF_DIR = po.ref_dir()
+if REF_DIR is None:
+    sys.exit("set MPSQMC_REF_DIR to the reference source tree")
 SEED = 20131015
 
 

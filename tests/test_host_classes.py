@@ -15,7 +15,7 @@ from oracle import pyoracle as po
 
 HOST_INC = os.path.join(ROOT, "mpsqmc_b200", "host", "include")
 PKG = os.path.join(ROOT, "mpsqmc_b200")
-REF_DIR = os.environ.get("MPSQMC_REF_DIR", "/root/reference")
+REF_DIR = po.ref_dir() or ""
 
 
 def compile_cpp(src: str, out: str) -> str:
@@ -96,7 +96,7 @@ def test_mpo_energy_matches_oracle(selftest):
     assert e == pytest.approx(float(z["L16D16_energy"]), rel=1e-11)
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF_DIR, "main.cpp")), reason="reference tree not present")
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_DIR, "main.cpp")), reason="MPSQMC_REF_DIR (the reference tree) not set")
 def test_reference_main_links_unchanged(tmp_path):
     """The reference's own main.cpp builds against these headers and libraries without edits."""
     exe = compile_cpp(os.path.join(REF_DIR, "main.cpp"), str(tmp_path / "main_dropin"))
