@@ -216,6 +216,16 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
                                       *   steps, 4 when that option is 0) and apply to the general
                                       *   sweep of the Trotter projector; the per-coupling trace is
                                       *   FP64-only (MPSQMC_E_UNSUPPORTED). */
+#define MPSQMC_PRECISION_TF32X3_TC 3 /*   the walker-batched sweep on the tcgen05 tensor cores: all
+                                      *   walkers move through the sites in lockstep and every
+                                      *   contraction of the step is one batched tcgen05 product
+                                      *   (TMA-fed, FP32 accumulators in TMEM) over the population,
+                                      *   three TF32 passes (FP32 accuracy).  Same FP64 parts and
+                                      *   QR-free sweep as TF32X3.  Needs walkers of one bond
+                                      *   profile (MPSQMC_E_UNSUPPORTED otherwise) and the grid
+                                      *   proposal; its trace records C/ov, the factor, uniform,
+                                      *   index, weight and the overlap ratio per coupling. */
+#define MPSQMC_PRECISION_TF32_TC 4   /*   the same with one TF32 pass per product */
 #define MPSQMC_OPT_PROPOSAL 8        /* how a coupling's grid point is drawn (what a
                                       * set_proposal(GRID | LEARNED) entry point would select): */
 #define MPSQMC_PROPOSAL_GRID 0       /*   the exact grid PDF, as MPSQMC2.cpp:551-588 (default) */
@@ -282,6 +292,25 @@ int mpsqmc_proposal_stats(mpsqmc_ctx *ctx, double *last_loss, int *updates);
  * walker bond dims, couplings, projector) for later contexts of this process, which then skip the
  * measurement.  best_* (may be NULL) receive the chosen option values. */
 int mpsqmc_autotune(mpsqmc_ctx *ctx, int steps, int *best_sweep, int *best_workspace);
+
+/* ---------------------------------------------------------------------------------------------
+ * One batched FP32 product on the tcgen05 tensor cores (the building block of the walker-batched
+ * mixed-precision sweep; no counterpart in the reference, whose products are dgemm_ calls, e.g.
+ * MPSstate.cpp:271-274).  For z < Z:
+ *   D_z[m, n] = alpha * sum_k A_{z/adiv}[m, k] B_{z/bdiv}[n, k]   (+ D_z[m, n] when beta = 1)
+ * with A_x[m, k] = A[k + m lda + x a_zstride], B_x[n, k] = B[k + n ldb + x b_zstride] (k
+ * contiguous) and D_z[m, n] = D[z dz + m dm + n dn]; adiv / bdiv = 0: the operand is shared by
+ * every z.  bstack > 1 (A shared) puts bstack consecutive z side by side in one tile of N.
+ * Operands are read in whole tiles and must be zero padded: k up to K rounded up to 32 (lda, ldb
+ * cover it), A rows up to a multiple of 64 (M <= 64) or 128, B rows up to a multiple of the tile
+ * width (N rounded up to 16, at most 256) when bstack = 1, and a_zcount / b_zcount operand
+ * entries allocated (B: at least Z rounded up to bstack when stacked).  Strides are multiples of 4
+ * and pointers 16-byte aligned.  passes = 3: FP32-accurate (head/tail TF32 split), 1: TF32.
+ * Device pointers; asynchronous on `stream`.  *err (device int) receives bit 4 if a pipeline wait
+ * timed out.  Returns 0 or a negative status. */
+int mpsqmc_tc_gemm(float *D, const float *A, const float *B, int M, int N, int K, long lda, long a_zstride,
+                   int adiv, long a_zcount, long ldb, long b_zstride, int bdiv, long b_zcount, int Z, int bstack,
+                   float alpha, int beta, int passes, long dz, long dm, long dn, int *err, void *stream);
 
 /* ---------------------------------------------------------------------------------------------
  * Local energies without any device allocation.  No counterpart in the reference.

@@ -62,7 +62,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         build_host()
         return LIB
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    units = [os.path.join(CSRC, f) for f in ("capi.cu", "noalloc.cu")]
+    units = [os.path.join(CSRC, f) for f in ("capi.cu", "noalloc.cu", "batched.cu")]
     cmd = [nvcc, *NVCC_FLAGS, *units, "-o", LIB + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

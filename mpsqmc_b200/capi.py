@@ -26,7 +26,7 @@ OPT_PROJECTOR = 5
 PROJECTOR_TROTTER, PROJECTOR_MPO_TERMS = 0, 1
 OPT_CANONICAL_INTERVAL = 6
 OPT_PRECISION = 7
-PRECISION_FP64, PRECISION_TF32, PRECISION_TF32X3 = 0, 1, 2
+PRECISION_FP64, PRECISION_TF32, PRECISION_TF32X3, PRECISION_TF32X3_TC, PRECISION_TF32_TC = 0, 1, 2, 3, 4
 OPT_PROPOSAL = 8
 PROPOSAL_GRID, PROPOSAL_LEARNED = 0, 1
 OPT_PROPOSAL_TRAINING = 9
@@ -37,7 +37,7 @@ EXPORTED = [
     "mpsqmc_create", "mpsqmc_destroy", "mpsqmc_last_error", "mpsqmc_version", "mpsqmc_walker_size",
     "mpsqmc_set_walkers", "mpsqmc_get_walkers", "mpsqmc_set_rng", "mpsqmc_get_rng_draws",
     "mpsqmc_energy", "mpsqmc_walk", "mpsqmc_last_step_walkers", "mpsqmc_set_trace",
-    "mpsqmc_get_trace", "mpsqmc_last_timing", "mpsqmc_local_energy_noalloc", "mpsqmc_set_step",
+    "mpsqmc_get_trace", "mpsqmc_last_timing", "mpsqmc_local_energy_noalloc", "mpsqmc_set_step", "mpsqmc_tc_gemm",
     "mpsqmc_set_option", "mpsqmc_get_option", "mpsqmc_set_walkers_dims", "mpsqmc_get_walker_dims",
     "mpsqmc_compress_walkers", "mpsqmc_autotune", "mpsqmc_proposal_params", "mpsqmc_proposal_loss_grad",
     "mpsqmc_proposal_stats", "mpsqmc_step_propagate", "mpsqmc_step_control", "mpsqmc_record_size",
@@ -129,6 +129,9 @@ def load(build_if_missing: bool = True):
         "mpsqmc_get_option": (C.c_int, [P, C.c_int, C.POINTER(C.c_long)]),
         "mpsqmc_local_energy_noalloc": (C.c_int, [C.POINTER(EnergyLayout), P, P, C.c_long, P, C.c_int, P,
                                                   C.c_int, P]),
+        "mpsqmc_tc_gemm": (C.c_int, [P, P, P, C.c_int, C.c_int, C.c_int, C.c_long, C.c_long, C.c_int, C.c_long,
+                                     C.c_long, C.c_long, C.c_int, C.c_long, C.c_int, C.c_int, C.c_float, C.c_int,
+                                     C.c_int, C.c_long, C.c_long, C.c_long, P, P]),
         "mpsqmc_proposal_params": (C.c_int, [P, fp, fp, C.POINTER(C.c_long)]),
         "mpsqmc_proposal_loss_grad": (C.c_int, [P, C.c_int, fp, fp, dp, fp]),
         "mpsqmc_proposal_stats": (C.c_int, [P, dp, ip]),
@@ -386,3 +389,11 @@ def local_energy_noalloc(*, L, trial_dims, walker_dims, ci, cj, cJ, h, trial_ptr
                        ci=_ip(keep[2]), cj=_ip(keep[3]), cJ=_dp(keep[4]), h=h)
     return lib.mpsqmc_local_energy_noalloc(C.byref(lay), trial_ptr, walkers_ptr, walker_stride, overlaps_ptr,
                                            n_walkers, energies_ptr, device, stream)
+
+
+def tc_gemm(*, D, A, B, M, N, K, lda, a_zstride, adiv, a_zcount, ldb, b_zstride, bdiv, b_zcount, Z, bstack=1,
+            alpha=1.0, beta=0, passes=3, dz, dm, dn, err, stream=None):
+    """Call mpsqmc_tc_gemm on device buffers (raw addresses): one batched FP32 product on the
+    tcgen05 tensor cores, D_z = alpha A_{z/adiv} B_{z/bdiv}^T (+ D_z).  Returns the status."""
+    return load().mpsqmc_tc_gemm(D, A, B, M, N, K, lda, a_zstride, adiv, a_zcount, ldb, b_zstride, bdiv, b_zcount,
+                                 Z, bstack, alpha, beta, passes, dz, dm, dn, err, stream)

@@ -25,6 +25,7 @@
 #include "legacy.cuh"
 #include "proposal.cuh"
 #include "population.cuh"
+#include "batched.h"
 
 namespace {
 
@@ -180,6 +181,14 @@ struct mpsqmc_ctx {
   bool graph_trace = false;
   mq::StepDev *h_sd = nullptr;  // pinned copies read back after every step
   int *h_err = nullptr;
+  // walker-batched tcgen05 sweep (MPSQMC_PRECISION_TF32X3_TC / TF32_TC): host copies of the
+  // coupling and channel tables, and the plan (its buffers hold bcap walkers)
+  std::vector<int> h_ci, h_cj, h_cq, h_ech_off, h_ech_slot, h_ech_cont, h_eopen;
+  std::vector<double> h_ech_J;
+  int nslots = 0;
+  mq::bs::Plan *bplan = nullptr;
+  int bplan_passes = 0;
+  int bcap = 0;
 };
 
 namespace {
@@ -280,6 +289,11 @@ bool qr_free(const mpsqmc_ctx *c) {
   return (c->canon_interval > 0 || mixed(c)) && general_sweep(c) && c->projector == MPSQMC_PROJECTOR_TROTTER;
 }
 
+// The walker-batched sweep on the tcgen05 tensor cores (batched.h).
+bool tc_sweep(const mpsqmc_ctx *c) {
+  return (c->precision == MPSQMC_PRECISION_TF32X3_TC || c->precision == MPSQMC_PRECISION_TF32_TC) && mixed(c);
+}
+
 // Steps between two left-normalisations of the QR-free sweep.
 constexpr int kMixedCanonInterval = 4;  // default of the mixed-precision sweep
 int canon_every(const mpsqmc_ctx *c) { return c->canon_interval > 0 ? c->canon_interval : kMixedCanonInterval; }
@@ -321,6 +335,7 @@ int check_err(mpsqmc_ctx *c) {
   int e = 0;
   CK(cudaMemcpyAsync(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (e & mq::bs::kErrTimeout) return fail(MPSQMC_E_CUDA, "a tcgen05 pipeline wait timed out");
   if (e & mq::kErrCapacity)
     return fail(MPSQMC_E_CAPACITY, "population control exceeded the walker capacity");
   if (e & mq::kErrNumeric) return fail(MPSQMC_E_NUMERIC, "non-finite weight, overlap or energy");
@@ -328,6 +343,10 @@ int check_err(mpsqmc_ctx *c) {
 }
 
 void free_all(mpsqmc_ctx *c) {
+  if (c->bplan) {
+    mq::bs::destroy(c->bplan);
+    c->bplan = nullptr;
+  }
   void *ptrs[] = {c->d_zoff, c->d_sums, c->d_pw, c->d_pm, c->d_pv, c->d_pg, c->d_pwb, c->d_pt, c->d_pb, c->d_ploss, c->d_pfeat,
                   c->d_ptarget, c->d_ph1, c->d_ph2, c->d_pz, c->d_pdz, c->d_pdh2, c->d_pdh1, c->d_trial32, c->d_aT, c->d_bW, c->d_toff, c->d_woff, c->d_roff, c->d_nroff, c->d_trial, c->d_walkers,
                   c->d_slot_of, c->d_slot_new, c->d_free, c->d_copy_src, c->d_copy_dst, c->d_parent,
@@ -506,6 +525,7 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
     ech_cont.push_back(0);
   }
 
+  std::vector<int> h_ci(cfg->ci, cfg->ci + cfg->nC), h_cj(cfg->cj, cfg->cj + cfg->nC);
   // Terms of the MPO-term projector, in the order HeisenbergMPO::findNonZeroContributions lists
   // them (HeisenbergMPO.cpp:456-553): per coupling J Sx Sx, -J iSy iSy, J Sz Sz; then -h Sz on
   // every site.  slot: where the sweep stores the term's overlap without prefactor.
@@ -547,6 +567,15 @@ int mpsqmc_create(const mpsqmc_config *cfg, mpsqmc_ctx **out) {
   c->h = cfg->h;
   c->nn = nn;
   c->nterms = (int)term_pref.size();
+  c->h_ci = h_ci;
+  c->h_cj = h_cj;
+  c->h_cq = cp_q;
+  c->h_ech_off = ech_off;
+  c->h_ech_slot = ech_slot;
+  c->h_ech_cont = ech_cont;
+  c->h_eopen = eopen;
+  c->h_ech_J = ech_J;
+  c->nslots = nslots;
   c->aT.assign(cfg->trial_dims, cfg->trial_dims + L + 1);
   c->bW.assign(cfg->walker_dims, cfg->walker_dims + L + 1);
   c->toff.resize(L);
@@ -1075,6 +1104,86 @@ static int enqueue_legacy_step(mpsqmc_ctx *c, int *launches) {
 static int enqueue_control(mpsqmc_ctx *c, const double *ext, int *launches);
 
 // The propagation part of a step: everything before the statistics.
+// The walker-batched sweep's plan, built before any stream capture: the population must share
+// the slot layout's bond profile (branching keeps it), and the grid proposal samples.
+static int ensure_batched(mpsqmc_ctx *c) {
+  if (!tc_sweep(c)) return 0;
+  if (c->proposal != MPSQMC_PROPOSAL_GRID || c->prop_train)
+    return fail(MPSQMC_E_UNSUPPORTED, "the tcgen05 sweep samples the grid PDF (no learned proposal or training)");
+  const int L = c->L, N = c->n_cur;
+  std::vector<int> dims((size_t)std::max(1, N) * (L + 1));
+  std::vector<int> slots(std::max(1, N));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(slots.data(), c->d_slot_of, sizeof(int) * N, cudaMemcpyDeviceToHost));
+  std::vector<int> all((size_t)c->capacity * (L + 1));
+  CK(cudaMemcpy(all.data(), c->d_wdims, sizeof(int) * all.size(), cudaMemcpyDeviceToHost));
+  for (int w = 0; w < N; ++w)
+    for (int k = 0; k <= L; ++k)
+      if (all[(size_t)slots[w] * (L + 1) + k] != c->bW[k])
+        return fail(MPSQMC_E_UNSUPPORTED, "the tcgen05 sweep needs every walker in the slot layout's bond profile");
+  const int passes = c->precision == MPSQMC_PRECISION_TF32_TC ? 1 : 3;
+  if (c->bplan && c->bplan_passes == passes) return 0;
+  if (c->bplan) {
+    mq::bs::destroy(c->bplan);
+    c->bplan = nullptr;
+  }
+  mq::bs::Problem pr;
+  pr.L = L;
+  pr.nC = c->nC;
+  pr.G = c->G;
+  pr.aT = c->aT;
+  pr.bW = c->bW;
+  pr.toff = c->toff;
+  pr.woff = c->woff;
+  pr.ci = c->h_ci;
+  pr.cj = c->h_cj;
+  pr.cq = c->h_cq;
+  pr.ech_off = c->h_ech_off;
+  pr.ech_slot = c->h_ech_slot;
+  pr.ech_cont = c->h_ech_cont;
+  pr.eopen = c->h_eopen;
+  pr.ech_J = c->h_ech_J;
+  pr.nslots = c->nslots;
+  pr.h = c->h;
+  for (int k = 0; k < 4; ++k) {
+    pr.opSx[k] = c->opSx[k];
+    pr.opISy[k] = c->opISy[k];
+    pr.opSz[k] = c->opSz[k];
+  }
+  pr.trial = c->d_trial;
+  pr.walkers = c->d_walkers;
+  pr.wstride = c->wstride;
+  pr.slot_of = c->d_slot_of;
+  pr.n_cur = c->d_ncur;
+  pr.weight = c->d_weight;
+  pr.overlap = c->d_overlap;
+  pr.energy = c->d_energy;
+  pr.ov_out = c->d_ovout;
+  pr.wt_out = c->d_wtout;
+  pr.uni = c->d_uni;
+  pr.tabU = c->d_tabU;
+  pr.tabSq = c->d_tabSq;
+  pr.tabVT = c->d_tabVT;
+  pr.grid = c->d_grid;
+  pr.err = c->d_err;
+  pr.passes = passes;
+  // buffers for the whole slot capacity when they fit in half the free memory, else for 1.5x the
+  // target population (a step with more walkers then stops with MPSQMC_E_CAPACITY)
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  pr.capacity = c->capacity;
+  if (mq::bs::bytes_needed(pr) > free_b / 2)
+    pr.capacity = std::min(c->capacity, std::max(64, (3 * c->Ndesired + 1) / 2));
+  if (mq::bs::bytes_needed(pr) > free_b * 9 / 10)
+    return fail(MPSQMC_E_CAPACITY, "the tcgen05 sweep's work buffers do not fit in device memory");
+  const int rc = mq::bs::build(pr, &c->bplan);
+  if (rc) return rc;
+  c->bplan_passes = passes;
+  c->bcap = pr.capacity;
+  drop_graphs(c);
+  return 0;
+}
+
 static int enqueue_propagation(mpsqmc_ctx *c, int *launches, bool canon) {
   mq::Dev p = make_dev(c);
   const int grid = c->max_ctas;
@@ -1093,7 +1202,12 @@ static int enqueue_propagation(mpsqmc_ctx *c, int *launches, bool canon) {
   const unsigned evflags = (cap == cudaStreamCaptureStatusActive) ? cudaEventRecordExternal : 0u;
   CK(cudaEventRecordWithFlags(c->ev[0], c->stream, evflags));
   const bool gen = general_sweep(c);
-  if (mixed(c)) {
+  if (tc_sweep(c)) {
+    int nb = 0;
+    const int rc = mq::bs::enqueue(c->bplan, c->stream, c->trace_on ? c->d_trace : nullptr, &nb);
+    if (rc) return rc;
+    n += nb - 1;
+  } else if (mixed(c)) {
     const int g = c->max_ctas_mixed;
     const size_t sm = c->smem_bytes_mixed;
     if (c->precision == MPSQMC_PRECISION_TF32) {
@@ -1189,6 +1303,7 @@ static int build_graph(mpsqmc_ctx *c, bool canon) {
 // Host bookkeeping after a step's read-back: errors, random-stream position, population size.
 static int finish_step(mpsqmc_ctx *c, int N, int step, bool canon, const mq::StepDev &sd, int err,
                        mpsqmc_step_stats *o) {
+  if (err & mq::bs::kErrTimeout) return fail(MPSQMC_E_CUDA, "a tcgen05 pipeline wait timed out");
   if (err & mq::kErrNumeric) return fail(MPSQMC_E_NUMERIC, "non-finite weight, overlap or energy");
   if (err & mq::kErrCapacity) return fail(MPSQMC_E_CAPACITY, "population control exceeded the walker capacity");
   const int per_walker = (c->projector == MPSQMC_PROJECTOR_MPO_TERMS) ? 1 : c->nC;
@@ -1221,8 +1336,12 @@ int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
   if (c->trace_on && !c->d_trace) {
     if (dalloc(&c->d_trace, (size_t)c->capacity * c->nC * mq::kTraceStride)) return MPSQMC_E_CUDA;
   }
-  if (c->trace_on && mixed(c))
-    return fail(MPSQMC_E_UNSUPPORTED, "the per-coupling trace is recorded by the FP64 sweep only");
+  if (c->trace_on && mixed(c) && !tc_sweep(c))
+    return fail(MPSQMC_E_UNSUPPORTED, "the per-coupling trace is recorded by the FP64 and tcgen05 sweeps only");
+  {
+    const int rc = ensure_batched(c);
+    if (rc) return rc;
+  }
   if (c->use_graph && c->graph_trace != c->trace_on) drop_graphs(c);
   int per_step = 0;
   double kernel_ms = 0.0;
@@ -1480,9 +1599,13 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
       c->canon_interval = (int)value;
       break;
     case MPSQMC_OPT_PRECISION:
-      if (value != MPSQMC_PRECISION_FP64 && value != MPSQMC_PRECISION_TF32 && value != MPSQMC_PRECISION_TF32X3)
-        return fail(MPSQMC_E_ARG, "unknown precision");
+      if (value < MPSQMC_PRECISION_FP64 || value > MPSQMC_PRECISION_TF32_TC) return fail(MPSQMC_E_ARG, "unknown precision");
       c->precision = (int)value;
+      if (c->bplan && !tc_sweep(c)) {
+        CK(cudaStreamSynchronize(c->stream));
+        mq::bs::destroy(c->bplan);
+        c->bplan = nullptr;
+      }
       break;
     case MPSQMC_OPT_PROPOSAL:
       if (value != MPSQMC_PROPOSAL_GRID && value != MPSQMC_PROPOSAL_LEARNED) return fail(MPSQMC_E_ARG, "unknown proposal");
@@ -1568,6 +1691,10 @@ int mpsqmc_step_propagate(mpsqmc_ctx *c, double local_sums[5]) {
   if (c->trace_on) return fail(MPSQMC_E_UNSUPPORTED, "the per-coupling trace is recorded by mpsqmc_walk only");
   CK(cudaSetDevice(c->device));
   if (!c->d_sums && dalloc(&c->d_sums, 16)) return MPSQMC_E_CUDA;
+  {
+    const int rc = ensure_batched(c);
+    if (rc) return rc;
+  }
   const int step = ++c->step_count;
   c->split_canon = qr_free(c) && step % canon_every(c) == 0;
   int n = 0;

@@ -1,0 +1,463 @@
+// Batched FP32 products on the 5th-generation tensor cores (tcgen05, kind::tf32) for the
+// walker-batched mixed-precision sweep (sm_100a).
+//
+//   D_z[m, n] = alpha * sum_k A_{z/adiv}[m, k] * B_{z/bdiv}[n, k]  (+ D_z[m, n] when beta)
+//
+// Both operands are K-major FP32 matrices (k contiguous) read by TMA (cp.async.bulk.tensor, no
+// multicast, tensor maps over this GPU's memory only) into 128-byte-swizzled shared-memory tiles
+// of 32 k-values, the canonical K-major SWIZZLE_128B layout of the UMMA descriptors.  A divisor
+// of 0 makes the operand shared by the whole batch (the trial tensor); B may stack `bstack`
+// consecutive batch entries along N in one tile, so that products with a shared A become one
+// wide GEMM (M = trial bond, N = walkers x walker bond).
+//
+// Precision: with passes = 3 every tile is split in shared memory into an exactly-TF32 head
+// (low 13 mantissa bits cleared) and a tail (x - head), and the accumulator takes
+// A_hi B_hi + A_hi B_lo + A_lo B_hi: about FP32 accuracy (relative error ~2^-21 per product term)
+// with FP32 accumulation in TMEM.  passes = 1 runs A_hi B_hi only (TF32).
+//
+// Roles (384 threads, one CTA per SM, persistent over tiles):
+//   warp 0      TMA producer (one lane), ring of kStages shared-memory stages;
+//   warp 1      TMEM owner and MMA issuer (one lane); two accumulators of tn columns;
+//   warps 2-7   head/tail split of each landed stage (passes = 3);
+//   warps 8-11  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM lanes 32 (w % 4)...),
+//               alpha/beta and the store to D.
+// Every mbarrier wait is bounded: on expiry the kernel sets bit kTcErrTimeout in *err, every role
+// leaves its loop, the CTA waits (bounded) for its loads in flight, frees TMEM and returns.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mq {
+namespace tc {
+
+constexpr int kThreads = 384;
+constexpr int kStages = 2;
+constexpr int kKC = 32;                 // k-values per stage (128 bytes of FP32: one swizzle row)
+constexpr int kMaxTN = 256;
+constexpr int kErrTimeout = 4;          // bit in the device error word (batched.h: bs::kErrTimeout)
+constexpr unsigned long long kWaitNs = 2000000000ull;  // a pipeline wait gives up after 2 s
+
+enum Epilogue : int { kStore = 0, kDot4 = 1 };
+
+struct alignas(64) GemmParams {
+  CUtensorMap tmA;   // 3D (k, row, z): FP32, box (32, tm, 1), SWIZZLE_128B
+  CUtensorMap tmB;   // 3D (k, row, z): FP32, box (32, brows, bstack), SWIZZLE_128B
+  int M, N, K;       // per batch entry
+  int tm, tn;        // MMA M (64 or 128) and tile N (multiple of 16, <= 256)
+  int adiv, bdiv;    // operand batch coordinate = z / div; 0: shared (coordinate 0)
+  int brows;         // B rows per batch entry loaded per tile (N when bstack > 1, else tn)
+  int bstack;        // batch entries per N tile (>= 1)
+  int Z;             // batch entries (if zcount: per unit of *zcount)
+  const int *zcount; // optional device count: Z_total = Z * *zcount
+  float alpha;
+  int beta;          // 1: accumulate into D
+  int passes;        // 1 or 3
+  float *D;
+  long dz, dm, dn;   // D_z[m, n] = D[z dz + m dm + n dn]
+  int epi;           // kStore, or kDot4: out[z] += sum_mn D_z[m,n] * E_{z,q}[m,n] for q < 4 (no store)
+  const float *E;    // kDot4 operands: E_{z,q}[m, n] = E[z ez + q eq + m em + n en]
+  long ez, eq, em, en;
+  double *dot;       // kDot4: dot[z * dstride + doff + q], FP64 accumulation (atomic)
+  int dstride, doff;
+  int *err;          // device error word
+};
+
+// ---------------------------------------------------------------------------------------------
+// PTX helpers
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n.reg .pred p;\n"
+      "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n"
+      "selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the phase of `parity` to complete.  Returns false (and flags the error) when
+// kWaitNs pass or another role already gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = now_ns();
+  unsigned n = 0;
+  while (!mbar_try(bar, parity)) {
+    if (((++n) & 63) == 0) {
+      if (*abort_flag) return false;
+      if (now_ns() - t0 > kWaitNs) {
+        *abort_flag = 1;
+        atomicOr(err, kErrTimeout);
+        return false;
+      }
+    }
+  }
+  return true;
+}
+
+// Bounded wait used at teardown (no abort flag).
+__device__ __forceinline__ void mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  const unsigned long long t0 = now_ns();
+  while (!mbar_try(bar, parity) && now_ns() - t0 < kWaitNs) {
+  }
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major, 128-byte swizzle: 8-row groups of 1024 bytes (stride byte offset 1024), version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;                  // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;        // stride byte offset
+  d |= (uint64_t)1 << 46;                  // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                  // SWIZZLE_128B
+  return d;
+}
+
+// kind::tf32, FP32 accumulator, both operands K-major.
+__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Tile bookkeeping (identical in every role)
+// ---------------------------------------------------------------------------------------------
+struct Tiling {
+  int mt, nt, total;  // m tiles, n tiles, all tiles
+  int Zt;             // batch entries
+};
+
+__device__ __forceinline__ Tiling tiling(const GemmParams &p) {
+  Tiling t;
+  t.Zt = p.Z * (p.zcount ? *p.zcount : 1);
+  t.mt = (p.M + p.tm - 1) / p.tm;
+  if (p.bstack > 1) t.nt = (t.Zt + p.bstack - 1) / p.bstack;
+  else t.nt = t.Zt * ((p.N + p.tn - 1) / p.tn);
+  t.total = t.mt * t.nt;
+  return t;
+}
+
+// tile -> m0, the first batch entry z0, n0 (row of B within z0; 0 when stacked)
+__device__ __forceinline__ void tile_coords(const GemmParams &p, const Tiling &t, int tile, int &m0, int &z0, int &n0) {
+  const int mi = tile % t.mt, ni = tile / t.mt;
+  m0 = mi * p.tm;
+  if (p.bstack > 1) {
+    z0 = ni * p.bstack;
+    n0 = 0;
+  } else {
+    const int per = (p.N + p.tn - 1) / p.tn;
+    z0 = ni / per;
+    n0 = (ni % per) * p.tn;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The kernel
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ GemmParams p) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ uint64_t bar_full[kStages], bar_conv[kStages], bar_empty[kStages];
+  __shared__ uint64_t bar_tfull[2], bar_tempty[2], bar_drain;
+  __shared__ uint32_t tmem_base;
+  __shared__ volatile int abort_flag;
+  __shared__ int issued[kStages];  // loads issued per stage (for the drain at exit)
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t a_bytes = (uint32_t)p.tm * 128, b_bytes = (uint32_t)p.tn * 128;
+  const uint32_t stage_bytes = 2 * (a_bytes + b_bytes);
+  const uint32_t b_load = (uint32_t)p.brows * p.bstack * 128;  // bytes one B box brings
+  const Tiling t = tiling(p);
+  const int nk = (p.K + kKC - 1) / kKC;
+  const int tcols = p.tn <= 16 ? 32 : (p.tn <= 32 ? 64 : (p.tn <= 64 ? 128 : (p.tn <= 128 ? 256 : 512)));
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&bar_full[s], 1);
+      mbar_init(&bar_conv[s], 6);
+      mbar_init(&bar_empty[s], 1);
+      issued[s] = 0;
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&bar_tfull[b], 1);
+      mbar_init(&bar_tempty[b], 4);
+    }
+    mbar_init(&bar_drain, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(tcols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < t.total && ok; tile += gridDim.x) {
+        int m0, z0, n0;
+        tile_coords(p, t, tile, m0, z0, n0);
+        const int za = p.adiv ? z0 / p.adiv : 0;
+        const int zb = p.bdiv ? z0 / p.bdiv : 0;
+        for (int kc = 0; kc < nk; ++kc) {
+          if (!mbar_wait(&bar_empty[s], ph ^ 1, &abort_flag, p.err)) {
+            ok = false;
+            break;
+          }
+          uint8_t *st = base + s * stage_bytes;
+          mbar_expect_tx(&bar_full[s], a_bytes + b_load);
+          tma_load_3d(st, &p.tmA, &bar_full[s], kc * kKC, m0, za);
+          tma_load_3d(st + 2 * a_bytes, &p.tmB, &bar_full[s], kc * kKC, n0, zb);
+          issued[s] += 1;
+          if (++s == kStages) {
+            s = 0;
+            ph ^= 1;
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      int acc = 0;
+      uint32_t aph[2] = {0, 0};
+      const uint32_t idesc = instr_desc(p.tm, p.tn);
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < t.total && ok; tile += gridDim.x) {
+        if (!mbar_wait(&bar_tempty[acc], aph[acc] ^ 1, &abort_flag, p.err)) break;
+        tc_fence_after();
+        const uint32_t dt = tmem + (uint32_t)(acc * p.tn);
+        for (int kc = 0; kc < nk; ++kc) {
+          uint64_t *wb = (p.passes == 3) ? &bar_conv[s] : &bar_full[s];
+          if (!mbar_wait(wb, ph, &abort_flag, p.err)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          uint8_t *st = base + s * stage_bytes;
+          const uint32_t ahi = smem_u32(st), alo = ahi + a_bytes, bhi = ahi + 2 * a_bytes, blo = bhi + b_bytes;
+#pragma unroll
+          for (int kk = 0; kk < kKC / 8; ++kk) {
+            const uint32_t off = kk * 32;  // 8 TF32 values = 32 bytes inside the swizzle row
+            const uint32_t first = (kc == 0 && kk == 0) ? 0u : 1u;
+            mma_tf32(dt, smem_desc(ahi + off), smem_desc(bhi + off), idesc, first);
+            if (p.passes == 3) {
+              mma_tf32(dt, smem_desc(ahi + off), smem_desc(blo + off), idesc, 1u);
+              mma_tf32(dt, smem_desc(alo + off), smem_desc(bhi + off), idesc, 1u);
+            }
+          }
+          mma_commit(&bar_empty[s]);  // frees the stage once these products are done
+          if (++s == kStages) {
+            s = 0;
+            ph ^= 1;
+          }
+        }
+        if (!ok) break;
+        mma_commit(&bar_tfull[acc]);
+        aph[acc] ^= 1;
+        acc ^= 1;
+      }
+    }
+  } else if (warp < 8) {
+    // ---------------- head/tail split ----------------
+    if (p.passes == 3) {
+      const int ct = threadIdx.x - 64;  // 0 .. 191
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < t.total && ok; tile += gridDim.x) {
+        for (int kc = 0; kc < nk; ++kc) {
+          if (!mbar_wait(&bar_full[s], ph, &abort_flag, p.err)) {
+            ok = false;
+            break;
+          }
+          uint8_t *st = base + s * stage_bytes;
+          // A: [hi | lo] then B: [hi | lo]; 16-byte vectors
+          const int na = (int)(a_bytes / 16), nb = (int)(b_bytes / 16);
+          for (int v = ct; v < na + nb; v += 192) {
+            uint8_t *hp = (v < na) ? st + 16 * v : st + 2 * a_bytes + 16 * (v - na);
+            uint8_t *lp = hp + ((v < na) ? a_bytes : b_bytes);
+            float4 x = *reinterpret_cast<float4 *>(hp);
+            float4 h, l;
+            h.x = __uint_as_float(__float_as_uint(x.x) & 0xFFFFE000u);
+            h.y = __uint_as_float(__float_as_uint(x.y) & 0xFFFFE000u);
+            h.z = __uint_as_float(__float_as_uint(x.z) & 0xFFFFE000u);
+            h.w = __uint_as_float(__float_as_uint(x.w) & 0xFFFFE000u);
+            l.x = x.x - h.x;
+            l.y = x.y - h.y;
+            l.z = x.z - h.z;
+            l.w = x.w - h.w;
+            *reinterpret_cast<float4 *>(hp) = h;
+            *reinterpret_cast<float4 *>(lp) = l;
+          }
+          fence_proxy_async();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&bar_conv[s]);
+          if (++s == kStages) {
+            s = 0;
+            ph ^= 1;
+          }
+        }
+      }
+    }
+  } else {
+    // ---------------- epilogue ----------------
+    const int q = warp & 3;  // TMEM lane quarter of this warp
+    int acc = 0;
+    uint32_t aph[2] = {0, 0};
+    for (int tile = blockIdx.x; tile < t.total; tile += gridDim.x) {
+      int m0, z0, n0;
+      tile_coords(p, t, tile, m0, z0, n0);
+      if (!mbar_wait(&bar_tfull[acc], aph[acc], &abort_flag, p.err)) break;
+      tc_fence_after();
+      // accumulator row of this thread: M = 128 -> lane 32q + l; M = 64 -> lanes 16 per quarter
+      const int row = (p.tm == 128) ? (32 * q + lane) : (lane < 16 ? 16 * q + lane : -1);
+      const int m = m0 + row;
+      const bool mrow = row >= 0 && m < p.M;
+      double dsum[4] = {0.0, 0.0, 0.0, 0.0};
+      int zlast = -1;
+      for (int c0 = 0; c0 < p.tn; c0 += 16) {
+        float v[16];
+        __syncwarp();  // tcgen05.ld is warp-collective
+        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * p.tn + c0), v);
+        if (!mrow) continue;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int j = c0 + i;
+          int z, n;
+          if (p.bstack > 1) {
+            if (j >= p.N * p.bstack) continue;  // rows past the stacked box: stale shared memory
+            z = z0 + j / p.N;
+            n = j % p.N;
+          } else {
+            z = z0;
+            n = n0 + j;
+          }
+          if (z >= t.Zt || n >= p.N) continue;
+          const float x = p.alpha * v[i];
+          if (p.epi == kStore) {
+            float *d = p.D + (long)z * p.dz + (long)m * p.dm + (long)n * p.dn;
+            *d = p.beta ? *d + x : x;
+          } else {
+            if (z != zlast) {
+              if (zlast >= 0)
+#pragma unroll
+                for (int qq = 0; qq < 4; ++qq) atomicAdd(p.dot + (long)zlast * p.dstride + p.doff + qq, dsum[qq]);
+              dsum[0] = dsum[1] = dsum[2] = dsum[3] = 0.0;
+              zlast = z;
+            }
+            const float *e = p.E + (long)z * p.ez + (long)m * p.em + (long)n * p.en;
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) dsum[qq] += (double)x * (double)e[qq * p.eq];
+          }
+        }
+      }
+      if (p.epi == kDot4 && zlast >= 0)
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) atomicAdd(p.dot + (long)zlast * p.dstride + p.doff + qq, dsum[qq]);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bar_tempty[acc]);
+      aph[acc] ^= 1;
+      acc ^= 1;
+    }
+  }
+
+  // ---------------- teardown ----------------
+  __syncthreads();
+  if (threadIdx.x == 0 && abort_flag) {
+    // the loads issued into each stage complete its full barrier in order: wait (bounded) for
+    // the last one, so that no copy lands in shared memory after the CTA has gone
+    for (int s = 0; s < kStages; ++s) {
+      if (issued[s] == 0) continue;
+      mbar_wait_bounded(&bar_full[s], (uint32_t)((issued[s] - 1) & 1));
+    }
+  }
+  if (warp == 1 && lane == 0) {
+    // every product this CTA issued has finished writing TMEM before it is freed
+    mma_commit(&bar_drain);
+    mbar_wait_bounded(&bar_drain, 0);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols));
+  }
+}
+
+__host__ __device__ constexpr int smem_bytes(int tm, int tn) { return kStages * 2 * (tm + tn) * 128 + 1024; }
+
+}  // namespace tc
+}  // namespace mq

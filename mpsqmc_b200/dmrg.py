@@ -201,3 +201,150 @@ def dmrg(L: int, D: int, J=1.0, h: float = 0.0, sweeps: int = 8, tol: float = 1e
     A[L - 1] /= np.linalg.norm(A[L - 1])
     sites = [a.transpose(1, 0, 2) for a in A]  # [sigma, Dl, Dr]
     return MPS.from_sites(sites, d), E
+
+
+# --------------------------------------------------------------------------------------------
+# The same two-site sweeps on the GPU (set-up code: the D_T = 256 trials of the 8x8 lattice)
+# --------------------------------------------------------------------------------------------
+def _lanczos_lowest(mv, x0, maxit: int = 60, tol: float = 1e-9):
+    """Lowest eigenpair of the symmetric operator mv by Lanczos with full reorthogonalisation,
+    started from x0 (all vectors on x0's device, FP64).  Stops when the residual estimate
+    |beta_m s_m| falls below tol * max(1, |theta|)."""
+    import torch
+    from scipy.linalg import eigh_tridiagonal
+
+    n = x0.numel()
+    m = min(maxit, n)
+    V = torch.empty((m, n), dtype=x0.dtype, device=x0.device)
+    V[0] = x0 / torch.linalg.vector_norm(x0)
+    alphas, betas = [], []
+    w = mv(V[0])
+    a = float(torch.dot(w, V[0]))
+    alphas.append(a)
+    w = w - a * V[0]
+    theta, s = np.array([a]), np.ones((1, 1))
+    k = 1
+    for k in range(1, m):
+        w = w - V[:k].T @ (V[:k] @ w)
+        b = float(torch.linalg.vector_norm(w))
+        if b < 1e-14:
+            break
+        V[k] = w / b
+        betas.append(b)
+        w = mv(V[k]) - b * V[k - 1]
+        a = float(torch.dot(w, V[k]))
+        alphas.append(a)
+        w = w - a * V[k]
+        if k % 3 == 0 or k == m - 1:
+            theta, s = eigh_tridiagonal(np.array(alphas), np.array(betas), select="i", select_range=(0, 0))
+            res = abs(float(torch.linalg.vector_norm(w - V[:k + 1].T @ (V[:k + 1] @ w)))) * abs(s[-1, 0])
+            if res < tol * max(1.0, abs(theta[0])):
+                break
+    kk = len(alphas)
+    theta, s = eigh_tridiagonal(np.array(alphas), np.array(betas[:kk - 1]), select="i", select_range=(0, 0))
+    coef = torch.as_tensor(s[:, 0], dtype=x0.dtype, device=x0.device)
+    x = V[:kk].T @ coef
+    return float(theta[0]), x / torch.linalg.vector_norm(x)
+
+
+def dmrg_device(L: int, D: int, couplings=None, J=1.0, h: float = 0.0, init: MPS | None = None, schedule=None,
+                sweeps: int = 6, tol: float = 1e-8, seed: int = 7, device: str = "cuda", verbose: bool = False):
+    """dmrg() with every contraction, eigensolver vector and SVD on a GPU in FP64 (torch).
+
+    The effective-Hamiltonian matvec, environments and truncation are those of dmrg(); the lowest
+    eigenvector comes from a Lanczos solver (full reorthogonalisation) on the device.  init: a
+    starting MPS (e.g. a stored trial of smaller bond dimension); else a seeded random one.
+    Returns (MPS in reference layout, left-normalised; energy of the last two-site solve)."""
+    import torch
+
+    dev = torch.device(device)
+    f64 = torch.float64
+    d = 2
+    if couplings is not None:
+        Ws = coupling_mpo(L, *couplings, h=h, d=d)
+    else:
+        Jv = np.full(L - 1, float(J)) if np.isscalar(J) else np.asarray(J, dtype=np.float64)
+        Ws = chain_mpo(L, Jv, h, d)
+    W = [torch.as_tensor(w, dtype=f64, device=dev) for w in Ws]
+    if init is None:
+        rng = np.random.default_rng(seed)
+        dims0 = virtual_dims(L, min(D, 4), d)
+        A = [torch.as_tensor(rng.standard_normal((dims0[k], d, dims0[k + 1])), dtype=f64, device=dev)
+             for k in range(L)]
+    else:
+        A = [torch.as_tensor(init.site(k).transpose(1, 0, 2).copy(), dtype=f64, device=dev) for k in range(L)]
+    td = lambda a, b, axes: torch.tensordot(a, b, dims=axes)  # noqa: E731
+
+    def left_env(Lp, a, w):
+        t = td(Lp, a, ([2], [0]))
+        t = td(t, w, ([1, 2], [0, 3]))
+        return td(a, t, ([0, 1], [0, 3])).permute(0, 2, 1).contiguous()
+
+    def right_env(Rn, a, w):
+        t = td(a, Rn, ([2], [2]))
+        t = td(t, w, ([1, 3], [3, 1]))
+        return td(a, t, ([1, 2], [3, 1])).permute(0, 2, 1).contiguous()
+
+    for k in range(L - 1, 0, -1):  # right-normalise the start
+        m = A[k].reshape(A[k].shape[0], -1)
+        q, r = torch.linalg.qr(m.T)
+        A[k] = q.T.reshape(-1, d, A[k].shape[2])
+        A[k - 1] = td(A[k - 1], r.T, ([2], [0]))
+    A[0] = A[0] / torch.linalg.vector_norm(A[0])
+    one = torch.ones((1, 1, 1), dtype=f64, device=dev)
+    R = [None] * (L + 1)
+    R[L] = one
+    for k in range(L - 1, 0, -1):
+        R[k] = right_env(R[k + 1], A[k], W[k])
+    Lenvs = [None] * (L + 1)
+    Lenvs[0] = one
+    if schedule is None:
+        start = max(a.shape[2] for a in A)
+        schedule = [x for x in (8, 16, 32, 64, 128, 256, 512) if start < x < D] + [D] * sweeps
+
+    def solve(k):
+        th = td(A[k], A[k + 1], ([2], [0]))
+        shape = th.shape
+        Le, W1, W2, Re = Lenvs[k], W[k], W[k + 1], R[k + 2]
+
+        def mv(x):
+            t = td(Le, x.reshape(shape), ([2], [0]))
+            t = td(t, W1, ([1, 2], [0, 3]))
+            t = td(t, W2, ([3, 1], [0, 3]))
+            return td(t, Re, ([1, 3], [2, 1])).reshape(-1)
+
+        e, v = _lanczos_lowest(mv, th.reshape(-1))
+        return e, v.reshape(shape[0] * d, d * shape[3]), shape
+
+    def split(mat, shape, Dcur):
+        u, s, vt = torch.linalg.svd(mat, full_matrices=False)
+        keep = max(1, min(Dcur, int(torch.count_nonzero(s > 1e-14 * s[0]))))
+        return u[:, :keep], s[:keep], vt[:keep], keep
+
+    E_prev, E = None, 0.0
+    for sweep, Dcur in enumerate(schedule):
+        for k in range(0, L - 1):
+            E, mat, shape = solve(k)
+            u, s, vt, keep = split(mat, shape, Dcur)
+            A[k] = u.reshape(shape[0], d, keep)
+            A[k + 1] = (s[:, None] * vt).reshape(keep, d, shape[3])
+            Lenvs[k + 1] = left_env(Lenvs[k], A[k], W[k])
+        for k in range(L - 2, -1, -1):
+            E, mat, shape = solve(k)
+            u, s, vt, keep = split(mat, shape, Dcur)
+            A[k] = (u * s[None, :]).reshape(shape[0], d, keep)
+            A[k + 1] = vt.reshape(keep, d, shape[3])
+            R[k + 1] = right_env(R[k + 2], A[k + 1], W[k + 1])
+        if verbose:
+            print(f"sweep {sweep} D={Dcur} E={E:.12f}", flush=True)
+        if E_prev is not None and Dcur == D and abs(E - E_prev) < tol:
+            break
+        E_prev = E if Dcur == D else None
+    for k in range(L - 1):
+        m = A[k].reshape(-1, A[k].shape[2])
+        q, r = torch.linalg.qr(m)
+        A[k] = q.reshape(A[k].shape[0], d, -1)
+        A[k + 1] = td(r, A[k + 1], ([1], [0]))
+    A[L - 1] = A[L - 1] / torch.linalg.vector_norm(A[L - 1])
+    sites = [a.permute(1, 0, 2).cpu().numpy() for a in A]  # [sigma, Dl, Dr]
+    return MPS.from_sites(sites, d), E

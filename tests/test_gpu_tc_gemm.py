@@ -1,0 +1,88 @@
+"""The tcgen05 batched FP32 product (mpsqmc_tc_gemm) against an FP64 torch reference of the same
+op: D_z = alpha A_{z/adiv} B_{z/bdiv}^T (+ D_z), operands K-major in zero-padded tiles.
+
+Tolerances (relative to max |D|): 3 passes (TF32 head/tail split, FP32 accumulation) 2e-6;
+1 pass (TF32 operands) 4e-3.  Shapes cover the sweep's uses: a shared trial operand with walkers
+stacked along N (M = 256, K = 512), per-walker operands with M = 64 (half-datapath accumulator
+layout), padding of M, N and K to whole tiles, an operand shared by pairs of batch entries,
+row- and column-major outputs, and accumulation."""
+import numpy as np
+import pytest
+
+from mpsqmc_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+
+def _pad(n, q):
+    return (n + q - 1) // q * q
+
+
+def run_case(M, N, K, Z, adiv, bdiv, bstack, passes, alpha=1.0, beta=0, colmajor=False, seed=0):
+    import torch
+
+    g = torch.Generator().manual_seed(seed)
+    dev = "cuda"
+    tm = 64 if M <= 64 else 128
+    kp = _pad(K, 32)
+    tn = _pad(N * bstack, 16) if bstack > 1 else min(256, _pad(N, 16))
+    ar = _pad(M, tm)
+    br = N if bstack > 1 else _pad(N, tn)
+    za = 1 if adiv == 0 else (Z - 1) // adiv + 1
+    zb = 1 if bdiv == 0 else (Z - 1) // bdiv + 1
+    if bstack > 1:
+        zb = _pad(zb, bstack)
+    A = torch.zeros((za, ar, kp), dtype=torch.float32)
+    B = torch.zeros((zb, br, kp), dtype=torch.float32)
+    A[:, :M, :K] = torch.randn((za, M, K), generator=g)
+    B[:, :N, :K] = torch.randn((zb, N, K), generator=g)
+    D0 = torch.randn((Z, M, N), generator=g) if beta else torch.zeros((Z, M, N))
+    ai = torch.tensor([z // adiv if adiv else 0 for z in range(Z)])
+    bi = torch.tensor([z // bdiv if bdiv else 0 for z in range(Z)])
+    ref = alpha * torch.einsum("zmk,znk->zmn", A[ai, :M, :K].double(), B[bi, :N, :K].double())
+    if beta:
+        ref = ref + D0.double()
+    Ad, Bd = A.to(dev), B.to(dev)
+    if colmajor:  # D_z stored (n, m): element (m, n) at z*M*N + n*M + m
+        Dd = D0.transpose(1, 2).contiguous().to(dev)
+        dz, dm, dn = M * N, 1, M
+    else:
+        Dd = D0.contiguous().to(dev)
+        dz, dm, dn = M * N, N, 1
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    rc = capi.tc_gemm(D=Dd.data_ptr(), A=Ad.data_ptr(), B=Bd.data_ptr(), M=M, N=N, K=K, lda=kp, a_zstride=ar * kp,
+                      adiv=adiv, a_zcount=za, ldb=kp, b_zstride=br * kp, bdiv=bdiv, b_zcount=zb, Z=Z, bstack=bstack,
+                      alpha=alpha, beta=beta, passes=passes, dz=dz, dm=dm, dn=dn, err=err.data_ptr(),
+                      stream=torch.cuda.current_stream().cuda_stream)
+    assert rc == 0, capi.load().mpsqmc_last_error().decode()
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    out = Dd.cpu().double()
+    if colmajor:
+        out = out.transpose(1, 2)
+    scale = float(ref.abs().max())
+    return float((out - ref).abs().max()) / scale
+
+
+CASES = [
+    # M, N, K, Z, adiv, bdiv, bstack
+    (256, 64, 512, 9, 0, 1, 4),     # trial x stacked walkers (8x8: M = 256, sigma-stacked K = 512)
+    (64, 32, 64, 13, 0, 1, 8),      # chain64 trial products, 8 walkers per tile
+    (64, 64, 32, 7, 1, 1, 1),       # walker products, M = 64
+    (96, 40, 40, 3, 1, 1, 1),       # padding of M, N and K
+    (128, 48, 64, 6, 1, 2, 1),      # B shared by pairs (a walker's site for its branches)
+    (200, 256, 96, 2, 1, 1, 1),     # two M tiles, a full-width N tile
+    (128, 300, 64, 2, 1, 1, 1),     # two N tiles per batch entry
+]
+
+
+@pytest.mark.parametrize("passes,tol", [(3, 2e-6), (1, 4e-3)])
+@pytest.mark.parametrize("case", CASES, ids=[f"M{c[0]}N{c[1]}K{c[2]}Z{c[3]}a{c[4]}b{c[5]}s{c[6]}" for c in CASES])
+def test_tc_gemm_matches_fp64(case, passes, tol):
+    assert run_case(*case, passes=passes) < tol
+
+
+@pytest.mark.parametrize("colmajor", [False, True])
+def test_tc_gemm_alpha_beta_and_layouts(colmajor):
+    assert run_case(128, 64, 64, 5, 1, 1, 1, 3, alpha=0.5, beta=1, colmajor=colmajor) < 2e-6
+    assert run_case(256, 32, 256, 8, 0, 1, 8, 3, alpha=-2.0, beta=1, colmajor=colmajor) < 2e-6
