@@ -50,9 +50,10 @@ def parse():
                          "throughput (blocking error of the mixed energy; first 20%% discarded)")
     ap.add_argument("--workspace", default="auto", choices=["auto", "global"],
                     help="matrix work buffers: shared memory when they fit (auto) or global scratch")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3", "tf32"],
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3", "tf32", "tf32x3_tc", "tf32_tc"],
                     help="walker-step contractions: FP64 tensor cores, or FP32 buffers on TF32 tensor cores "
-                         "(three passes / one pass); weights, overlaps, energies stay FP64")
+                         "(three passes / one pass; *_tc: the walker-batched sweep on tcgen05); weights, "
+                         "overlaps, energies stay FP64")
     ap.add_argument("--proposal", default="grid", choices=["grid", "learned"],
                     help="auxiliary-field proposal: the exact grid PDF, or the learned network (trained online "
                          "on the grid walk for --train-steps steps first; exact-ratio reweighting)")
@@ -76,7 +77,7 @@ def parse():
     return ap.parse_args()
 
 
-PRECISIONS = {"fp64": 0, "tf32": 1, "tf32x3": 2}
+PRECISIONS = {"fp64": 0, "tf32": 1, "tf32x3": 2, "tf32x3_tc": 3, "tf32_tc": 4}
 
 
 def configure(eng, args, sweep, plain=False):

@@ -4,8 +4,10 @@ chain64   L=64 open Heisenberg chain, J=1, h=0, D_T=64 trial (compact-MPO DMRG, 
           walkers = trial compressed to D_W=32 plus i.i.d. N(0, 1e-3) noise per element, dtau=0.01,
           2048 walkers, Marsaglia(4) grid (240 points).
 chain16   L=16 chain, D_T=D_W=16 trial from the reference's DMRG, 128 walkers, dtau=0.01.
-snake6x6, snake8x8   open 6x6 / 8x8 lattices on the snake path with seeded random trials of the
-          D_T bond profile (throughput: the work per walker-step does not depend on the trial).
+snake6x6  open 6x6 lattice on the snake path with a seeded random trial of the D_T = 128 bond
+          profile (throughput: the work per walker-step does not depend on the trial).
+snake8x8  the open 8x8 lattice with its D_T = 256 DMRG ground-state trial (made on the GPU),
+          D_W = 64, 4096 walkers, dtau = 0.005; snake8x8_random the same shapes with a random trial.
 snake6x6_dmrg   the open 6x6 lattice with its ground-state trial from the compact-MPO DMRG at
           D_T = 64 (mpsqmc_b200/data, made by data/make_trials.py), walkers of D_W in {16, 32, 64}.
 snake8x8_dmrg   the open 8x8 lattice with its DMRG ground-state trial at D_T = 64, walkers of D_W
@@ -148,6 +150,10 @@ class LatticeWorkload:
     def L(self):
         return self.W * self.H
 
+    def has_trial(self):
+        """False when the workload names a stored trial that is not present."""
+        return not self.trial_file or os.path.exists(os.path.join(DATA, self.trial_file))
+
     def trial_energy(self):
         """The DMRG energy of the stored trial (a variational upper bound), or None."""
         if not self.trial_file:
@@ -164,7 +170,10 @@ class LatticeWorkload:
     def trial(self):
         if self.trial_file:
             z = np.load(os.path.join(DATA, self.trial_file))
-            return pb.MPS(z["dims"].astype(np.int32), z["data"])
+            m = pb.MPS(z["dims"].astype(np.int32), z["data"].astype(np.float64))
+            # trials stored in FP32 (26 MB instead of 52 MB at D_T = 256) are left-normalised
+            # again in FP64; their energy is stored for that FP64 state
+            return pb.left_normalize(m) if z["data"].dtype == np.float32 else m
         rng = np.random.default_rng(self.seed)
         dims = pb.virtual_dims(self.L, self.DT)
         data = rng.normal(size=int(sum(dims[k] * dims[k + 1] * 2 for k in range(self.L))))
@@ -189,5 +198,11 @@ def snake8x8_dmrg(Nw: int = 1024) -> LatticeWorkload:
 
 
 def snake8x8(Nw: int = 4096) -> LatticeWorkload:
-    """8x8 open lattice, D_T = 256, D_W = 64, dtau 0.005."""
-    return LatticeWorkload("snake8x8", 8, 8, 256, [64], Nw, 0.005)
+    """The full chosen configuration: 8x8 open lattice, D_T = 256 DMRG ground-state trial (made on
+    the GPU, data/make_trials.py snake8x8_256), D_W = 64, 4096 walkers, dtau 0.005."""
+    return LatticeWorkload("snake8x8", 8, 8, 256, [64], Nw, 0.005, trial_file="trial_snake8x8_D256.npz")
+
+
+def snake8x8_random(Nw: int = 4096) -> LatticeWorkload:
+    """The 8x8 shapes (D_T = 256, D_W = 64) with a seeded random left-normalised trial."""
+    return LatticeWorkload("snake8x8_random", 8, 8, 256, [64], Nw, 0.005)

@@ -568,6 +568,19 @@ int mode_propagate(int argc, char **argv) {
   std::vector<MPSstate *> trials(nth);
   for (int t = 0; t < nth; ++t) trials[t] = new MPSstate(&psi);
   const int G = grid.gNPoints();
+  // the non-zero couplings in the order MPSQMC2.cpp:286-299 lists them
+  std::vector<int> ci, cj;
+  for (int i = 0; i < L - 1; ++i)
+    for (int j = i + 1; j < L; ++j)
+      if (trot.gCoupling(i, j) != 0.0) {
+        ci.push_back(i);
+        cj.push_back(j);
+      }
+  const int nC = (int)ci.size();
+  // $MPSQMC_REF_MAX_COUPLINGS = k: time the first k couplings of each walker-step only (large
+  // lattices); the rate is then extrapolated to all nC couplings
+  const char *mk = getenv("MPSQMC_REF_MAX_COUPLINGS");
+  const int ntime = (mk && atoi(mk) > 0) ? std::min(nC, atoi(mk)) : nC;
   std::cout.rdbuf(old);
   const auto t0 = std::chrono::steady_clock::now();
   for (int step = 0; step < steps; ++step) {
@@ -580,11 +593,11 @@ int mode_propagate(int argc, char **argv) {
         Walker *W = walkers[w];
         W->gState()->ApplyOneSiteTrotterTermEverywhere(&trot);
         W->setOverlap(trials[tid]);
-        for (int c = 0; c < L - 1; ++c) {
+        for (int c = 0; c < ntime; ++c) {
           for (int k = 0; k < 16; ++k) {
             delete terms[k];
             terms[k] = new MPSstate(trials[tid]);
-            terms[k]->ApplyTwoSiteTrotterTerm(&trot, c, c + 1, k % 4, k / 4, true);
+            terms[k]->ApplyTwoSiteTrotterTerm(&trot, ci[c], cj[c], k % 4, k / 4, true);
             C[k] = terms[k]->InnerProduct(W->gState());
           }
           double norm = 0.0;
@@ -603,7 +616,7 @@ int mode_propagate(int argc, char **argv) {
           int count = 0;
           double cum = pdf[0];
           while (cum <= u && count < G - 1) cum += pdf[++count];
-          W->gState()->ApplyTwoSiteTrotterTerm(&trot, c, c + 1, &grid, count);
+          W->gState()->ApplyTwoSiteTrotterTerm(&trot, ci[c], cj[c], &grid, count);
           W->setOverlap(trials[tid]);
         }
         W->gState()->ApplyOneSiteTrotterTermEverywhere(&trot);
@@ -614,9 +627,11 @@ int mode_propagate(int argc, char **argv) {
   }
   const auto t1 = std::chrono::steady_clock::now();
   const double sec = std::chrono::duration<double>(t1 - t0).count();
+  const double full = sec * (double)nC / (double)ntime;  // all couplings (extrapolated when ntime < nC)
   printf("{\"walker_steps\": %lld, \"seconds\": %.6f, \"walker_steps_per_s\": %.6f, \"threads\": %d, "
+         "\"couplings_timed\": %d, \"couplings\": %d, \"measured_seconds\": %.6f, "
          "\"kind\": \"reference classes, propagation only (no energy)\"}\n",
-         (long long)Nw * steps, sec, (double)Nw * steps / sec, nth);
+         (long long)Nw * steps, full, (double)Nw * steps / full, nth, ntime, nC, sec);
   for (size_t i = 0; i < walkers.size(); ++i) delete walkers[i];
   for (int t = 0; t < nth; ++t) delete trials[t];
   return 0;

@@ -231,3 +231,20 @@ def test_stored_lattice_trial_is_the_dmrg_state(name):
         A = m.site(k)  # [sigma, Dl, Dr]
         G = sum(A[s].T @ A[s] for s in range(2))
         np.testing.assert_allclose(G, np.eye(G.shape[0]), atol=1e-10)
+
+
+def test_stored_d256_trial_is_left_normalised():
+    """The 8x8 D_T = 256 trial (grown on the GPU by dmrg.dmrg_device, stored in FP32 and
+    left-normalised again in FP64 on load): bond profile and left-canonical sites.  Its energy
+    under the compact MPO equals the stored one (checked once when it was made: the host
+    contraction at D = 256 takes minutes)."""
+    import numpy as np
+    from mpsqmc_b200 import workloads
+    wl = workloads.snake8x8()
+    m = wl.trial()
+    np.testing.assert_array_equal(m.dims, workloads.pb.virtual_dims(64, 256))
+    for k in (0, 7, 8, 31, 56, 62):
+        A = m.site(k)
+        G = sum(A[s].T @ A[s] for s in range(2))
+        np.testing.assert_allclose(G, np.eye(G.shape[0]), atol=1e-10)
+    assert -0.62 * wl.L < wl.trial_energy() < -0.61 * wl.L
