@@ -1,13 +1,17 @@
 """Walker-propagation benchmark (MPSQMC2::Walk hot path) on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference] [--workload chain64]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference] [--workload snake8x8]
 
-Workload chain64 (the L=64 chain configuration): D_T=64 trial, 2048 walkers of D_W=32 (trial
-compressed + N(0,1e-3) noise), dtau=0.01, one walker-step = propagation over all 63 couplings,
-local energy, statistics and threshold branching.  Prints one JSON line (rank 0).
+Default workload snake8x8 (the full chosen configuration): the open 8x8 Heisenberg lattice on the
+snake path, D_T = 256 DMRG ground-state trial, 4096 walkers of D_W = 64 (the trial compressed),
+dtau = 0.005, Marsaglia(4) grid.  One walker-step = propagation over all 112 couplings, local
+energy, statistics and threshold branching.  The timed arm is the walker-batched mixed-precision
+sweep on the tcgen05 tensor cores (TF32 x3, FP32-accurate products; FP64 walkers, weights,
+overlaps, energies and population control); the plain FP64 sweep on the same configuration is
+timed beside it for the ratio.  Prints one JSON line (rank 0).
 
 Timing: W untimed steps, then K steps in one engine call; device time from CUDA events recorded on
-the engine's stream around those K steps (the walker population, 1.8 GB, exceeds L2 so no flush
+the engine's stream around those K steps (the walker population, 14 GB, exceeds L2 so no flush
 is needed).  Multi-GPU: independent replicas (one population per rank), max time over ranks.
 """
 from __future__ import annotations
@@ -35,11 +39,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="chain64", choices=["chain64", "snake6x6", "snake6x6_dmrg", "snake8x8",
-                                                               "snake8x8_dmrg"],
-                    help="chain64: the L=64 chain (default line); snake6x6 / snake8x8: the 2D lattices "
-                         "(walkers compressed on the device; no CPU baseline or e2e); *_dmrg: with "
-                         "their DMRG ground-state trials")
+    ap.add_argument("--workload", default="snake8x8", choices=["chain64", "snake6x6", "snake6x6_dmrg", "snake8x8",
+                                                                "snake8x8_dmrg", "snake8x8_random"],
+                    help="snake8x8: the 8x8 lattice with its D_T = 256 DMRG trial (default line); chain64: the "
+                         "L = 64 chain; snake6x6: the 6x6 lattice with uneven walkers; *_dmrg: D_T = 64 "
+                         "DMRG trials; snake8x8_random: the 8x8 shapes with a random trial")
+    ap.add_argument("--fp64-steps", type=int, default=2,
+                    help="steps of the plain FP64 sweep timed beside a mixed-precision main arm (its "
+                         "throughput for the ratio); 0: skip")
     ap.add_argument("--walkers", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -50,10 +57,10 @@ def parse():
                          "throughput (blocking error of the mixed energy; first 20%% discarded)")
     ap.add_argument("--workspace", default="auto", choices=["auto", "global"],
                     help="matrix work buffers: shared memory when they fit (auto) or global scratch")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3", "tf32", "tf32x3_tc", "tf32_tc"],
+    ap.add_argument("--precision", default=None, choices=["fp64", "tf32x3", "tf32", "tf32x3_tc", "tf32_tc"],
                     help="walker-step contractions: FP64 tensor cores, or FP32 buffers on TF32 tensor cores "
                          "(three passes / one pass; *_tc: the walker-batched sweep on tcgen05); weights, "
-                         "overlaps, energies stay FP64")
+                         "overlaps, energies stay FP64.  Default: tf32x3_tc on snake8x8, fp64 otherwise")
     ap.add_argument("--proposal", default="grid", choices=["grid", "learned"],
                     help="auxiliary-field proposal: the exact grid PDF, or the learned network (trained online "
                          "on the grid walk for --train-steps steps first; exact-ratio reweighting)")
@@ -74,7 +81,10 @@ def parse():
                          "balancing, mpsqmc_b200.population) instead of N independent replicas")
     ap.add_argument("--vn-arms", default="tf32x3/grid,tf32x3/learned",
                     help="precision/proposal variants compared with the plain FP64 grid walk")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.precision is None:
+        a.precision = "tf32x3_tc" if a.workload == "snake8x8" else "fp64"
+    return a
 
 
 PRECISIONS = {"fp64": 0, "tf32": 1, "tf32x3": 2, "tf32x3_tc": 3, "tf32_tc": 4}
@@ -243,53 +253,48 @@ def tf32_peak_tflops():
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def reference_cpu(wl, sample_walkers=None, steps=1, threads=None):
+def reference_cpu(wl, sample_walkers=None, steps=1, threads=None, max_couplings=None):
     """The reference's own classes (oracle/_ref/ref_harness, built from the reference sources) timed on
     this host: propagation of `sample_walkers` walkers for `steps` steps, energy excluded (the
-    reference's H*Psi_T MPS does not fit at L=64, D_T=64)."""
+    reference's H*Psi_T MPS does not fit at these sizes).  max_couplings: time only the first k
+    couplings of each step and extrapolate to all of them (the reference's cost per coupling is
+    16 full-chain InnerProducts and one LeftNormalize whatever the coupling, so the rate scales)."""
     from oracle import pyoracle as po
     if not po.harness_available():
         return None
     threads = threads or os.cpu_count()
     sample_walkers = sample_walkers or threads
+    trial = wl.trial() if callable(getattr(wl, "trial", None)) else wl.trial
+    env = {"OMP_NUM_THREADS": str(threads)}
+    if hasattr(wl, "W"):
+        env["MPSQMC_REF_LATTICE"] = f"snake:{wl.W}x{wl.H}"
+    if max_couplings:
+        env["MPSQMC_REF_MAX_COUPLINGS"] = str(max_couplings)
+    DW = wl.DW if hasattr(wl, "DW") else max(wl.Ds)
     with tempfile.TemporaryDirectory() as t:
         path = os.path.join(t, "trial.mps")
-        po.write_mps(path, po.MPS(wl.trial.dims, wl.trial.data))
-        out = po.run_harness("propagate", path, wl.DW, sample_walkers, wl.dtau, steps,
-                             env_extra={"OMP_NUM_THREADS": str(threads)})
+        po.write_mps(path, po.MPS(trial.dims, trial.data))
+        out = po.run_harness("propagate", path, DW, sample_walkers, wl.dtau, steps, env_extra=env)
     r = json.loads(out.strip().splitlines()[-1])
+    part = (f", {r['couplings_timed']} of {r['couplings']} couplings timed per step and the rate "
+            f"extrapolated to all" if r.get("couplings_timed", 0) < r.get("couplings", 0) else "")
     r["sample"] = (f"{sample_walkers} walkers x {steps} step(s) of {wl.name}, propagation only "
-                   f"(reference classes, per-coupling trial terms, no energy)")
+                   f"(reference classes, per-coupling trial terms, no energy{part})")
     r["cores"] = threads
     return r
 
 
-def lattice_engine(wl, device):
-    """Engine for a 2D lattice workload.  Walkers start as copies of the trial compressed
-    (CompressState + setOverlap, as SetupWalkers does): on the device to uneven targets in one
-    population when D_T is among them, else one walker compressed on the host and replicated
-    (slots of the D_W layout)."""
-    from mpsqmc_b200 import Engine
+def lattice_population(wl):
+    """Walkers of a 2D workload as SetupWalkers makes them (MPSQMC2.cpp:404-409): copies of the trial
+    compressed to D_W (CompressState + setOverlap), on the host when D_W < D_T; with uneven targets
+    that include D_T, on the device (compress_walkers).  Returns (slot bond profile, host population
+    or None, device targets or None)."""
     from mpsqmc_b200 import problem as pb
-    ci, cj, cJ = wl.couplings()
     trial = wl.trial()
-    U, S, VT = pb.trotter_tables(1.0, wl.dtau)
-    common = dict(L=wl.L, ci=ci, cj=cj, cJ=cJ, h=0.0, dtau=wl.dtau, trial_dims=trial.dims, trial=trial.data,
-                  Jvals=[1.0], U=U, S=S, VT=VT, grid=pb.grid_marsaglia(4, 4), Ndesired=wl.Nw, device=device)
-    N = wl.Nw
     if max(wl.Ds) >= wl.DT:
-        eng = Engine(capacity=max(1000, 3 * N), walker_dims=trial.dims, **common)
-        eng.set_walkers(np.tile(trial.data, (N, 1)), np.ones(N), normalize=False)
-        eng.compress_walkers(wl.targets(), normalize=True)
-        dims = trial.dims
-    else:
-        # one walker compressed on the host (the engine's slots hold walkers up to D = 128)
-        w = pb.compress(trial, max(wl.Ds))
-        dims, w0 = w.dims, w.data
-        eng = Engine(capacity=max(1000, 3 * N), walker_dims=dims, **common)
-        eng.set_walkers(np.tile(w0, (N, 1)), np.ones(N), normalize=True)
-    inputs = dict(common, walker_dims=dims)
-    return eng, inputs
+        return trial.dims, None, wl.targets()
+    w = pb.compress(trial, max(wl.Ds))
+    return w.dims, w.data, None
 
 
 def main():
@@ -300,46 +305,38 @@ def main():
     lattice = args.workload != "chain64"
     if lattice:
         wl = getattr(workloads, args.workload)(Nw=args.walkers) if args.walkers else getattr(workloads, args.workload)()
+        te = wl.trial_energy()
         cfg = {"workload": f"{wl.name}: {wl.W}x{wl.H} open Heisenberg lattice on the snake path (L={wl.L}, "
                            f"{len(wl.couplings()[0])} couplings), D_T={wl.DT}, D_W in {wl.Ds}, {wl.Nw} walkers/GPU, "
-                           f"dtau={wl.dtau}, Marsaglia(4) grid, FP64; "
-                           + (f"trial: DMRG ground state at D_T={wl.DT} (E={wl.trial_energy():.10f})"
-                              if wl.trial_file else "seeded random left-normalised trial of the D_T shape")
-                           + ", walkers = trial compressed on the device",
+                           f"dtau={wl.dtau}, Marsaglia(4) grid; "
+                           + (f"trial: DMRG ground state at D_T={wl.DT} (E={te:.10f})" if wl.trial_file
+                              else "seeded random left-normalised trial of the D_T shape")
+                           + "; walkers = the trial compressed to D_W",
                "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.Ds, "dtau": wl.dtau,
-               "parallelism": f"{'split walk' if args.sharded else 'replicas'} x{world}", "sweep": args.sweep,
-               "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
-               "proposal_mix": args.proposal_mix if args.proposal_mix is not None else 100,
-               "canonical_interval": args.canon if args.canon is not None else 16}
+               "l2": f"population ({wl.Nw * 8 * 2 * sum(int(a) * int(b) for a, b in zip(workloads.pb.virtual_dims(wl.L, max(wl.Ds))[:-1], workloads.pb.virtual_dims(wl.L, max(wl.Ds))[1:])) / 1e9:.1f} GB) larger than L2 (126 MB); no flush"}
     else:
         wl = workloads.chain64(Nw=args.walkers or 2048)
         cfg = {"workload": f"{wl.name}: L={wl.L} Heisenberg chain, D_T={wl.DT}, D_W={wl.DW}, {wl.Nw} walkers/GPU, "
-                           f"dtau={wl.dtau}, Marsaglia(4) grid, FP64",
+                           f"dtau={wl.dtau}, Marsaglia(4) grid",
                "walkers_per_gpu": wl.Nw, "L": wl.L, "D_T": wl.DT, "D_W": wl.DW, "dtau": wl.dtau,
-               "l2": f"population ({wl.Nw * wl.walker.data.size * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
-               "parallelism": f"{'split walk' if args.sharded else 'replicas'} x{world}", "sweep": args.sweep,
-               "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
-               "proposal_mix": args.proposal_mix if args.proposal_mix is not None else 100,
-               "canonical_interval": args.canon if args.canon is not None else 16}
+               "l2": f"population ({wl.Nw * wl.walker.data.size * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush"}
+    cfg.update({"parallelism": f"{'split walk' if args.sharded else 'replicas'} x{world}", "sweep": args.sweep,
+                "workspace": args.workspace, "precision": args.precision, "proposal": args.proposal,
+                "proposal_mix": args.proposal_mix if args.proposal_mix is not None else 100,
+                "canonical_interval": args.canon if args.canon is not None else 16})
+    # the reference CPU sample: all couplings of chain64; two of the lattices' (extrapolated)
+    ref_couplings = 2 if lattice else None
+    ref_walkers = min(os.cpu_count() or 1, 16)
 
     if args.impl == "reference":
         if rank != 0:
             return
-        if lattice:
-            print(json.dumps({"impl": "reference", "unavailable": "the reference classes need nC*16 trial copies "
-                              "and H*Psi_T per thread at this size; only chain64 has a CPU arm"}))
-            return
-        r = reference_cpu(wl, steps=1)
+        r = reference_cpu(wl, sample_walkers=ref_walkers, steps=max(1, args.steps), threads=ref_walkers,
+                          max_couplings=ref_couplings)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built"}))
             return
-        total_t = 0.0
-        ws = 0
-        for _ in range(max(1, args.steps)):
-            rr = reference_cpu(wl, steps=1)
-            total_t += rr["seconds"]
-            ws += rr["walker_steps"]
-        v = ws / total_t
+        v = r["walker_steps_per_s"]
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "walker-steps/s", "n_gpus": 0,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
                 "data": "synthetic", "config": cfg,
@@ -356,31 +353,51 @@ def main():
     sweep = {"auto": 0, "nearest": 1, "general": 2}[args.sweep]
     seed = wl.seed + 7919 * rank
     if lattice:
-        eng, inputs = lattice_engine(wl, local)
-        walkers = None
+        from mpsqmc_b200 import problem as pb
+        ci, cj, cJ = wl.couplings()
+        trial = wl.trial()
+        U, S, VT = pb.trotter_tables(1.0, wl.dtau)
+        wdims, w0, targets = lattice_population(wl)
         N = wl.Nw
-        args.no_e2e = True
-        args.no_cpu_baseline = True
-
-        def make():
-            return lattice_engine(wl, local)[0]
+        inputs = dict(L=wl.L, ci=ci, cj=cj, cJ=cJ, h=0.0, dtau=wl.dtau, trial_dims=trial.dims, trial=trial.data,
+                      Jvals=[1.0], U=U, S=S, VT=VT, grid=pb.grid_marsaglia(4, 4), Ndesired=N,
+                      capacity=max(1000, 2 * N), walker_dims=wdims)
+        if w0 is not None:
+            # the population in pinned host memory (the device upload and the e2e arm read it)
+            walkers = torch.empty((N, w0.size), dtype=torch.float64, pin_memory=True).numpy()
+            walkers[:] = w0[None, :]
+        else:
+            walkers = None
+            args.no_e2e = True
     else:
         inputs = wl.inputs()
         walkers = wl.walkers()
         N = walkers.shape[0]
 
-        def make():
-            e = Engine(device=local, **inputs)
+    def make():
+        e = Engine(device=local, **inputs)
+        if walkers is not None:
             e.set_walkers(walkers, np.ones(N), None, np.zeros(N), normalize=True)
-            return e
+        else:
+            e.set_walkers(np.tile(inputs["trial"], (N, 1)), np.ones(N), normalize=False)
+            e.compress_walkers(targets, normalize=True)
+        return e
 
-        eng = make()
-    configure(eng, args, sweep)
-    eng.set_rng(seed, 0)
+    def timed_arm(precision, steps, warmup, proposal="grid", params=None):
+        """One engine walking `warmup` untimed then `steps` timed steps from the common start and
+        random stream; returns (engine, stats, timing)."""
+        a = argparse.Namespace(**vars(args))
+        a.precision, a.proposal = precision, proposal
+        e = make()
+        configure(e, a, sweep, plain=(precision == "fp64"))
+        e.set_rng(seed, 0)
+        use_proposal(e, params)
+        e.walk(warmup)
+        torch.cuda.synchronize()
+        return e, a
+
     params, training = train_proposal(make, args, sweep, seed)
-    use_proposal(eng, params)
-    eng.walk(args.warmup)
-    torch.cuda.synchronize()
+    eng, _ = timed_arm(args.precision, args.steps, args.warmup, args.proposal, params)
     if pg is not None:
         pg.barrier()
     rw = None
@@ -408,23 +425,26 @@ def main():
     t_ms, k_ms, ws_all = aggregate_ranks(pg, t_ms, k_ms, ws_done)
     value = ws_all / (t_ms * 1e-3)
 
+    # roofline of the dominant work (the walker step): canonical FP64-equivalent work / its device
+    # time, averaged over the walkers' own bond dims
+    cpl = list(zip(inputs["ci"], inputs["cj"]))
+    dims_now = eng.get_walker_dims()
+    rows, counts = np.unique(dims_now, axis=0, return_counts=True)
+    flops_ws = float(sum(c * workloads.algorithmic_flops_per_walker_step(inputs["trial_dims"], r, cpl)
+                         for r, c in zip(rows, counts)) / counts.sum())
+    achieved = flops_ws * ws_done / (k_ms * 1e-3) / 1e12
+    mixed = args.precision != "fp64"
+    tc = args.precision.endswith("_tc")
+    passes = 1 if args.precision in ("tf32", "tf32_tc") else 3
+    E_last = {"E_P_last": stats[-1]["E_P"], "E_T_last": stats[-1]["E_T"], "walkers_last": stats[-1]["n_after"],
+              "E_P_mean": float(np.mean([s["E_P"] for s in stats]))}
+
     vn = None
-    vn_compare = args.vn_compare
-    if rw is not None:
-        vn_compare = 0
-    if vn_compare is None:
-        vn_compare = 300 if (not lattice and args.precision == "fp64" and args.proposal == "grid"
-                             and args.walkers is None and args.steps >= 5) else 0
-    vn_steps = max(args.vn, vn_compare)
-    if vn_steps > 0:
+    vn_steps = max(args.vn, args.vn_compare or 0)
+    if vn_steps > 0 and rw is None:
         from mpsqmc_b200 import analysis
-        e_ref, e_src = None, None
-        if not lattice:
-            e_ref = float(np.load(os.path.join(ROOT, "mpsqmc_b200", "data", "trial_L64D64.npz"))["energy"])
-            e_src = "DMRG D=64 energy of the trial (mpsqmc_b200/data)"
-        elif wl.trial_energy() is not None:
-            e_ref = wl.trial_energy()
-            e_src = f"DMRG D={wl.DT} energy of the trial (mpsqmc_b200/data; a variational upper bound)"
+        e_ref = wl.trial_energy() if lattice else None
+        e_src = f"DMRG D={wl.DT} energy of the trial (a variational upper bound)" if e_ref is not None else None
 
         def vn_of(e, throughput):
             more = e.walk(vn_steps)
@@ -433,75 +453,78 @@ def main():
             if e_ref is not None:
                 r["E_ref"] = e_ref
                 r["E_ref_source"] = e_src
-                r["abs_err_per_site"] = abs(r["E_mean"] - e_ref) / wl.L
-            return r
-
-        def arm(precision, proposal):
-            """A variant from the same start and random stream: set-up (training for the learned
-            proposal), warm-up, timed steps for its throughput, then the VN steps."""
-            a = argparse.Namespace(**vars(args))
-            a.precision, a.proposal = precision, proposal
-            e = make()
-            configure(e, a, sweep, plain=(precision == "fp64"))
-            e.set_rng(seed, 0)
-            p_arm, tr = train_proposal(make, a, sweep, seed)
-            use_proposal(e, p_arm)
-            e.walk(args.warmup)
-            st = e.walk(args.steps)
-            t = e.last_timing()
-            thr = sum(x["n_walkers"] for x in st) / (t["total_ms"] * 1e-3)
-            r = vn_of(e, thr)
-            if tr:
-                r["proposal_training"] = tr
-            e.close()
             return r
 
         this = vn_of(eng, value / max(world, 1))
         this["arm"] = f"{args.precision}/{args.proposal}"
         vn = this
-        if vn_compare > 0:
-            plain = this if (args.precision, args.proposal) == ("fp64", "grid") else arm("fp64", "grid")
-            vn = {"plain_fp64_grid": plain, "vn_ratio_vs_plain_fp64": {}, "throughput_ratio_vs_plain_fp64": {}}
-            arms = [this["arm"]] if this is not plain else []
+        if args.vn_compare:
+            eng.close()
+            arms = {this["arm"]: this}
             named = [x if "/" in x else x + "/grid" for x in args.vn_arms.split(",") if x]
-            arms += [x for x in named if x not in arms and x != "fp64/grid"]
-            for name in arms:
-                r = this if name == this["arm"] else arm(*name.split("/"))
+            for name in ["fp64/grid"] + named:
+                if name in arms:
+                    continue
+                prec, prop = name.split("/")
+                p_arm, tr = train_proposal(make, argparse.Namespace(**{**vars(args), "precision": prec,
+                                                                          "proposal": prop}), sweep, seed)
+                e, _ = timed_arm(prec, args.steps, args.warmup, prop, p_arm)
+                st = e.walk(args.steps)
+                t = e.last_timing()
+                r = vn_of(e, sum(x["n_walkers"] for x in st) / (t["total_ms"] * 1e-3))
+                if tr:
+                    r["proposal_training"] = tr
+                e.close()
+                arms[name] = r
+            plain = arms["fp64/grid"]
+            vn = {"plain_fp64_grid": plain, "vn_ratio_vs_plain_fp64": {}, "throughput_ratio_vs_plain_fp64": {},
+                  "E_mean_diff_vs_plain_per_site": {}}
+            for name, r in arms.items():
+                if name == "fp64/grid":
+                    continue
                 vn[name] = r
                 vn["vn_ratio_vs_plain_fp64"][name] = r["vn"] / plain["vn"] if plain["vn"] else None
                 vn["throughput_ratio_vs_plain_fp64"][name] = r["throughput_per_gpu"] / plain["throughput_per_gpu"]
+                vn["E_mean_diff_vs_plain_per_site"][name] = abs(r["E_mean"] - plain["E_mean"]) / wl.L
+            eng = None
+    if eng is not None:
+        eng.close()
 
-    # roofline of the dominant kernel (the walker-step kernel): canonical FP64 work / kernel time,
-    # averaged over the walkers' own bond dims
-    cpl = list(zip(inputs["ci"], inputs["cj"]))
-    dims_now = eng.get_walker_dims()
-    rows, counts = np.unique(dims_now, axis=0, return_counts=True)
-    flops_ws = float(sum(c * workloads.algorithmic_flops_per_walker_step(inputs["trial_dims"], r, cpl)
-                         for r, c in zip(rows, counts)) / counts.sum())
-    achieved = flops_ws * ws_done / (k_ms * 1e-3) / 1e12
-    mixed = args.precision != "fp64"
-    peak = (tf32_peak_tflops() if mixed else fp64_peak_tflops()) if rank == 0 else None
+    # the plain FP64 sweep on the same configuration, timed beside a mixed-precision main arm
+    fp64_arm = None
+    if mixed and args.fp64_steps > 0 and vn is None:
+        e, _ = timed_arm("fp64", args.fp64_steps, 1)
+        st = e.walk(args.fp64_steps)
+        t = e.last_timing()
+        e.close()
+        t_f, _, ws_f = aggregate_ranks(pg, t["total_ms"], t["step_kernel_ms"], sum(x["n_walkers"] for x in st))
+        v_f = ws_f / (t_f * 1e-3)
+        fp64_arm = {"value": v_f, "unit": "walker-steps/s", "steps": args.fp64_steps, "warmup": 1,
+                    "ms_per_step": t_f / args.fp64_steps, "E_P_mean": float(np.mean([x["E_P"] for x in st])),
+                    "throughput_ratio_mixed_vs_fp64": value / v_f,
+                    "note": "same configuration, start and random stream; the mixed arm's products are "
+                            "FP32-accurate, so it follows the FP64 trajectory and the energy variance per "
+                            "walker-step is the same: the throughput ratio is the variance-normalised ratio "
+                            "(measured over long walks in profiles/)"}
+
+    peak = None
+    if rank == 0:
+        peak = tf32_peak_tflops() if mixed else fp64_peak_tflops()
 
     # end to end through the public API: host population -> device, K steps (stats read back each
     # step), population -> host; host wall clock.
     e2e = None
-    if not args.no_e2e:
-        eng2 = Engine(device=local, **inputs)
-        configure(eng2, args, sweep)
-        use_proposal(eng2, params)  # the trained network, as the timed engine walks with it
+    if not args.no_e2e and walkers is not None:
+        eng2, _ = timed_arm(args.precision, args.steps, args.warmup, args.proposal, params)
         # the population in pinned host memory (both directions), as a serving caller would keep it
-        host_w = torch.empty(walkers.shape, dtype=torch.float64, pin_memory=True).numpy()
-        host_w[:] = walkers
-        back_w = torch.empty((eng2.capacity, eng2.walker_size), dtype=torch.float64, pin_memory=True).numpy()
-        # untimed warm-up on this engine, as for the device-timed steps (step graphs captured, kernels
-        # loaded); the timed run then starts again from the host population
-        eng2.set_walkers(host_w, np.ones(N), None, np.zeros(N), normalize=True)
-        eng2.set_rng(wl.seed + 7919 * rank, 0)
-        eng2.walk(args.warmup)
+        host_w = walkers if lattice else torch.empty(walkers.shape, dtype=torch.float64, pin_memory=True).numpy()
+        if not lattice:
+            host_w[:] = walkers
+        back_w = torch.empty((max(N + N // 2, 64), eng2.walker_size), dtype=torch.float64, pin_memory=True).numpy()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         eng2.set_walkers(host_w, np.ones(N), None, np.zeros(N), normalize=True)
-        eng2.set_rng(wl.seed + 7919 * rank, 0)
+        eng2.set_rng(seed, 0)
         st2 = eng2.walk(args.steps)
         back = eng2.get_walkers(out=back_w)
         t1 = time.perf_counter()
@@ -515,7 +538,7 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        r = reference_cpu(wl, steps=1)
+        r = reference_cpu(wl, sample_walkers=ref_walkers, steps=1, threads=ref_walkers, max_couplings=ref_couplings)
         if r is not None:
             cpu = {"value": r["walker_steps_per_s"], "unit": "walker-steps/s", "cores": r["cores"],
                    "kind": "reference", "sample": r["sample"]}
@@ -523,31 +546,37 @@ def main():
     if rank == 0:
         prof_traffic = None
         kname = "walker_step_kernel" if args.sweep == "nearest" else (
-            "walker_step_mixed_kernel" if mixed else "walker_step_general_kernel")
-        tp = os.path.join(ROOT, "profiles", f"{kname}_traffic.json")
-        if os.path.exists(tp) and not lattice and N == 2048:
-            prof_traffic = json.load(open(tp)).get("bytes_per_launch")
+            "tc_gemm_kernel" if tc else ("walker_step_mixed_kernel" if mixed else "walker_step_general_kernel"))
+        tp = os.path.join(ROOT, "profiles", f"{kname}_{wl.name}_traffic.json")
+        if os.path.exists(tp):
+            prof_traffic = json.load(open(tp)).get("bytes_per_step_per_walker")
+            if prof_traffic is not None:
+                prof_traffic = prof_traffic * N  # one step processes every walker once
         line = {
             "metric": METRIC, "value": value, "unit": "walker-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if not mixed else f"{args.precision}+f64", "data": "synthetic",
             "config": cfg,
-            "energy": {"E_P_last": stats[-1]["E_P"], "E_T_last": stats[-1]["E_T"], "walkers_last": stats[-1]["n_after"]},
+            "energy": E_last,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": prof_traffic,
                          "kernel": kname, "flops_per_walker_step": flops_ws,
+                         "timed": ("the whole walker-step sweep (all its launches) on the engine's stream"
+                                   if tc else "the walker-step kernel on the engine's stream"),
+                         **({"passes": passes, "executed_frac": passes * achieved / peak if peak else None}
+                            if mixed else {}),
                          "peak_source": ("cuBLAS TF32 GEMM 8192^3 measured in this run (TF32 tensor path; the "
                                          "canonical flops count each product once)") if mixed else
                                         "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor path)"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": tim["launches"],
+            **({"fp64_arm": fp64_arm} if fp64_arm is not None else {}),
             **({"variance_normalised": vn} if vn is not None else {}),
             **({"proposal_training": training} if training else {}),
             "clocks": clk.summary(),
         }
         print(json.dumps(line))
-    eng.close()
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()

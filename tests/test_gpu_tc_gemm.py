@@ -1,7 +1,8 @@
 """The tcgen05 batched FP32 product (mpsqmc_tc_gemm) against an FP64 torch reference of the same
 op: D_z = alpha A_{z/adiv} B_{z/bdiv}^T (+ D_z), operands K-major in zero-padded tiles.
 
-Tolerances (relative to max |D|): 3 passes (TF32 head/tail split, FP32 accumulation) 2e-6;
+Tolerances (relative to max |D|): 3 passes (TF32 head/tail split, FP32 accumulation) within 4x
+the error of a plain FP32 product of the same inputs (torch, TF32 off), and at most 2e-5;
 1 pass (TF32 operands) 4e-3.  Shapes cover the sweep's uses: a shared trial operand with walkers
 stacked along N (M = 256, K = 512), per-walker operands with M = 64 (half-datapath accumulator
 layout), padding of M, N and K to whole tiles, an operand shared by pairs of batch entries,
@@ -61,7 +62,14 @@ def run_case(M, N, K, Z, adiv, bdiv, bstack, passes, alpha=1.0, beta=0, colmajor
     if colmajor:
         out = out.transpose(1, 2)
     scale = float(ref.abs().max())
-    return float((out - ref).abs().max()) / scale
+    # the same product in plain FP32 (TF32 off): the accuracy the 3-pass product should match
+    keep = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    f32 = alpha * torch.einsum("zmk,znk->zmn", A[ai, :M, :K].to(dev), B[bi, :N, :K].to(dev)).double().cpu()
+    torch.backends.cuda.matmul.allow_tf32 = keep
+    if beta:
+        f32 = f32 + D0.double()
+    return float((out - ref).abs().max()) / scale, float((f32 - ref).abs().max()) / scale
 
 
 CASES = [
@@ -76,13 +84,22 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("passes,tol", [(3, 2e-6), (1, 4e-3)])
+def fp32_accurate(err, err_f32):
+    return err <= max(4.0 * err_f32, 1e-6) and err < 2e-5
+
+
+@pytest.mark.parametrize("passes", [3, 1])
 @pytest.mark.parametrize("case", CASES, ids=[f"M{c[0]}N{c[1]}K{c[2]}Z{c[3]}a{c[4]}b{c[5]}s{c[6]}" for c in CASES])
-def test_tc_gemm_matches_fp64(case, passes, tol):
-    assert run_case(*case, passes=passes) < tol
+def test_tc_gemm_matches_fp64(case, passes):
+    err, err_f32 = run_case(*case, passes=passes)
+    print(f"{case} passes={passes}: {err:.3e} (plain FP32 {err_f32:.3e})")
+    if passes == 3:
+        assert fp32_accurate(err, err_f32), (err, err_f32)
+    else:
+        assert err < 4e-3
 
 
 @pytest.mark.parametrize("colmajor", [False, True])
 def test_tc_gemm_alpha_beta_and_layouts(colmajor):
-    assert run_case(128, 64, 64, 5, 1, 1, 1, 3, alpha=0.5, beta=1, colmajor=colmajor) < 2e-6
-    assert run_case(256, 32, 256, 8, 0, 1, 8, 3, alpha=-2.0, beta=1, colmajor=colmajor) < 2e-6
+    assert fp32_accurate(*run_case(128, 64, 64, 5, 1, 1, 1, 3, alpha=0.5, beta=1, colmajor=colmajor))
+    assert fp32_accurate(*run_case(256, 32, 256, 8, 0, 1, 8, 3, alpha=-2.0, beta=1, colmajor=colmajor))
