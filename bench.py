@@ -78,7 +78,8 @@ def parse():
                          "default chain64 run, else off)")
     ap.add_argument("--sharded", action="store_true",
                     help="N>1: one walk split over the ranks (global population control and walker "
-                         "balancing, mpsqmc_b200.population) instead of N independent replicas")
+                         "balancing, mpsqmc_b200.population; NCCL, records in device buffers) instead of N "
+                         "independent replicas")
     ap.add_argument("--vn-arms", default="tf32x3/grid,tf32x3/learned",
                     help="precision/proposal variants compared with the plain FP64 grid walk")
     a = ap.parse_args()
@@ -136,7 +137,10 @@ def use_proposal(eng, params):
         eng.set_option(OPT_PROPOSAL, PROPOSAL_LEARNED)
 
 
-def dist_setup(n):
+def dist_setup(n, nccl=False):
+    """One process per GPU.  nccl: the split walk's data plane (global sums and walker records
+    in device buffers over NCCL); otherwise gloo, which only carries the replicas' barriers and
+    timing aggregation."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -144,7 +148,12 @@ def dist_setup(n):
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("gloo", timeout=timedelta(seconds=120))
+        if nccl:
+            import torch
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=timedelta(seconds=120))
         pg = dist
     return rank, world, local, pg
 
@@ -196,12 +205,13 @@ def aggregate_ranks(pg, t_ms, k_ms, walker_steps):
     if pg is None:
         return t_ms, k_ms, float(walker_steps)
     import torch
-    tt = torch.tensor([t_ms, k_ms, float(walker_steps)], dtype=torch.float64)
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    tt = torch.tensor([t_ms, k_ms, float(walker_steps)], dtype=torch.float64, device=dev)
     mx = tt.clone()
     pg.all_reduce(mx, op=pg.ReduceOp.MAX)
     sm = tt.clone()
     pg.all_reduce(sm, op=pg.ReduceOp.SUM)
-    return float(mx[0]), float(mx[1]), float(sm[2])
+    return float(mx[0].item()), float(mx[1].item()), float(sm[2].item())
 
 
 def measured_peaks():
@@ -299,7 +309,7 @@ def lattice_population(wl):
 
 def main():
     args = parse()
-    rank, world, local, pg = dist_setup(args.gpus)
+    rank, world, local, pg = dist_setup(args.gpus, nccl=args.sharded and args.impl == "mine")
     from mpsqmc_b200 import workloads
 
     lattice = args.workload != "chain64"
@@ -403,7 +413,8 @@ def main():
     rw = None
     if args.sharded and pg is not None:
         from mpsqmc_b200.population import RankWalk
-        rw = RankWalk(eng, pg, [N] * world, device="cpu")
+        # walker records and the five sums in device buffers, moved by NCCL into the receiver's HBM
+        rw = RankWalk(eng, pg, [N] * world, device=f"cuda:{local}")
     with ClockSampler(local) as clk:
         if rw is None:
             stats = eng.walk(args.steps)

