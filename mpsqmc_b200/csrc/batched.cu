@@ -67,29 +67,45 @@ int make_operand_map(CUtensorMap *map, const float *base, long k_ext, long rows,
   return 0;
 }
 
-int configure_kernel(int *sms) {
-  static int n_sms = 0;
+// SM count and the dynamic shared memory a launch may use (the opt-in limit less the kernel's
+// static barriers), set once per process.
+int configure_kernel(int *sms, int *smem_limit) {
+  static int n_sms = 0, limit = 0;
   static std::once_flag once;
   static cudaError_t status = cudaSuccess;
   std::call_once(once, [] {
-    int dev = 0;
+    int dev = 0, optin = 0;
     status = cudaGetDevice(&dev);
     if (status == cudaSuccess) status = cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (status == cudaSuccess) status = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    limit = optin - 2048;
     if (status == cudaSuccess)
-      status = cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes(128, 256));
+      status = cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
   });
   if (status != cudaSuccess) return fail(MPSQMC_E_CUDA, std::string("tcgen05 GEMM set-up: ") + cudaGetErrorString(status));
   *sms = n_sms;
+  if (smem_limit) *smem_limit = limit;
+  return 0;
+}
+
+// The load ring's depth for this tile shape (as deep as shared memory allows).
+int pick_stages(GemmParams &p) {
+  int sms = 0, limit = 0;
+  const int rc = configure_kernel(&sms, &limit);
+  if (rc) return rc;
+  p.stages = stages_for(p.tm, p.tn, p.passes, limit);
+  if (smem_bytes(p.tm, p.tn, p.passes, p.stages) > limit)
+    return fail(MPSQMC_E_UNSUPPORTED, "tcgen05 GEMM tile does not fit in shared memory");
   return 0;
 }
 
 // Launch one batched product; max_tiles bounds the grid (the persistent CTAs loop over tiles).
 int launch(const GemmParams &p, long max_tiles, cudaStream_t stream) {
   int sms = 0;
-  int rc = configure_kernel(&sms);
+  int rc = configure_kernel(&sms, nullptr);
   if (rc) return rc;
   const int grid = (int)std::max(1L, std::min((long)sms, max_tiles));
-  tc_gemm_kernel<<<grid, kThreads, smem_bytes(p.tm, p.tn), stream>>>(p);
+  tc_gemm_kernel<<<grid, kThreads, smem_bytes(p.tm, p.tn, p.passes, p.stages), stream>>>(p);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(MPSQMC_E_CUDA, std::string("tcgen05 GEMM launch: ") + cudaGetErrorString(e));
   return 0;
@@ -141,7 +157,8 @@ extern "C" int mpsqmc_tc_gemm(float *D, const float *A, const float *B, int M, i
   // B to a multiple of the tile rows when bstack == 1)
   const long arows = ((M + p.tm - 1) / p.tm) * p.tm;
   const long brows = bstack > 1 ? N : ((N + p.tn - 1) / p.tn) * p.tn;
-  int rc = make_operand_map(&p.tmA, A, kpad, arows, std::max(1L, a_zcount), lda, a_zstride, p.tm, 1);
+  int rc = pick_stages(p);
+  if (!rc) rc = make_operand_map(&p.tmA, A, kpad, arows, std::max(1L, a_zcount), lda, a_zstride, p.tm, 1);
   if (!rc) rc = make_operand_map(&p.tmB, B, kpad, brows, std::max(1L, b_zcount), ldb, b_zstride, p.brows, bstack);
   if (rc) return rc;
   const long mt = (M + p.tm - 1) / p.tm;
@@ -618,7 +635,8 @@ int add_gemm(Plan *p, const Opnd &A, const Opnd &B, int M, int N, int K, int zpe
     g.dstride = 16;
     g.doff = doff;
   }
-  int rc = make_operand_map(&g.tmA, A.base, K, A.rows, std::max(1L, A.zn), A.ld, A.zs, g.tm, 1);
+  int rc = pick_stages(g);
+  if (!rc) rc = make_operand_map(&g.tmA, A.base, K, A.rows, std::max(1L, A.zn), A.ld, A.zs, g.tm, 1);
   if (!rc) rc = make_operand_map(&g.tmB, B.base, K, bstack > 1 ? N : B.rows, std::max(1L, B.zn), B.ld, B.zs, g.brows,
                                  bstack);
   if (rc) return rc;

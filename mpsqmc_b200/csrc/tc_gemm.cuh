@@ -16,11 +16,12 @@
 // with FP32 accumulation in TMEM.  passes = 1 runs A_hi B_hi only (TF32).
 //
 // Roles (384 threads, one CTA per SM, persistent over tiles):
-//   warp 0      TMA producer (one lane), ring of kStages shared-memory stages;
+//   warp 0      TMA producer (one lane), ring of 2-4 shared-memory stages (as many as fit);
 //   warp 1      TMEM owner and MMA issuer (one lane); two accumulators of tn columns;
 //   warps 2-7   head/tail split of each landed stage (passes = 3);
 //   warps 8-11  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM lanes 32 (w % 4)...),
-//               alpha/beta and the store to D.
+//               alpha/beta and the store to D; row-major outputs are transposed through shared
+//               memory so that every store instruction writes consecutive elements.
 // Every mbarrier wait is bounded: on expiry the kernel sets bit kTcErrTimeout in *err, every role
 // leaves its loop, the CTA waits (bounded) for its loads in flight, frees TMEM and returns.
 #pragma once
@@ -33,7 +34,7 @@ namespace mq {
 namespace tc {
 
 constexpr int kThreads = 384;
-constexpr int kStages = 2;
+constexpr int kMaxStages = 4;        // shared-memory stages of the load ring (2 .. 4 by tile size)
 constexpr int kKC = 32;                 // k-values per stage (128 bytes of FP32: one swizzle row)
 constexpr int kMaxTN = 256;
 constexpr int kErrTimeout = 4;          // bit in the device error word (batched.h: bs::kErrTimeout)
@@ -54,6 +55,7 @@ struct alignas(64) GemmParams {
   float alpha;
   int beta;          // 1: accumulate into D
   int passes;        // 1 or 3
+  int stages;        // shared-memory stages of the load ring (2 .. kMaxStages)
   float *D;
   long dz, dm, dn;   // D_z[m, n] = D[z dz + m dm + n dn]
   int epi;           // kStore, or kDot4: out[z] += sum_mn D_z[m,n] * E_{z,q}[m,n] for q < 4 (no store)
@@ -211,28 +213,65 @@ __device__ __forceinline__ void tile_coords(const GemmParams &p, const Tiling &t
   }
 }
 
+// tile column j -> batch entry z and row n of B (z < 0: past the stacked box)
+__device__ __forceinline__ void col_of(const GemmParams &p, int j, int z0, int n0, int &z, int &n) {
+  if (p.bstack > 1) {
+    if (j >= p.N * p.bstack) {  // rows past the stacked box: stale shared memory
+      z = -1;
+      n = 0;
+      return;
+    }
+    z = z0 + j / p.N;
+    n = j % p.N;
+  } else {
+    z = z0;
+    n = n0 + j;
+  }
+}
+
+// x rounded to the nearest TF32 value (10 explicit mantissa bits), as an FP32 bit pattern
+__device__ __forceinline__ float to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// closures: the warp's four partial sums of batch entry z into dot (one atomic per sum)
+__device__ __forceinline__ void flush_dot(const GemmParams &p, int z, double *dsum, int lane) {
+#pragma unroll
+  for (int qq = 0; qq < 4; ++qq) {
+    double v = dsum[qq];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) atomicAdd(p.dot + (long)z * p.dstride + p.doff + qq, v);
+    dsum[qq] = 0.0;
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // The kernel
 // ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ GemmParams p) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  __shared__ uint64_t bar_full[kStages], bar_conv[kStages], bar_empty[kStages];
+  __shared__ uint64_t bar_full[kMaxStages], bar_conv[kMaxStages], bar_empty[kMaxStages];
   __shared__ uint64_t bar_tfull[2], bar_tempty[2], bar_drain;
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
-  __shared__ int issued[kStages];  // loads issued per stage (for the drain at exit)
+  __shared__ int issued[kMaxStages];  // loads issued per stage (for the drain at exit)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int NS = p.stages;
   uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const uint32_t a_bytes = (uint32_t)p.tm * 128, b_bytes = (uint32_t)p.tn * 128;
-  const uint32_t stage_bytes = 2 * (a_bytes + b_bytes);
+  const uint32_t lo_mult = (p.passes == 3) ? 2u : 1u;  // head (+ tail) tiles per operand
+  const uint32_t stage_bytes = lo_mult * (a_bytes + b_bytes);
   const uint32_t b_load = (uint32_t)p.brows * p.bstack * 128;  // bytes one B box brings
+  float *stagebuf = reinterpret_cast<float *>(base + NS * stage_bytes);  // epilogue transposes
   const Tiling t = tiling(p);
   const int nk = (p.K + kKC - 1) / kKC;
   const int tcols = p.tn <= 16 ? 32 : (p.tn <= 32 ? 64 : (p.tn <= 64 ? 128 : (p.tn <= 128 ? 256 : 512)));
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < NS; ++s) {
       mbar_init(&bar_full[s], 1);
       mbar_init(&bar_conv[s], 6);
       mbar_init(&bar_empty[s], 1);
@@ -275,9 +314,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           uint8_t *st = base + s * stage_bytes;
           mbar_expect_tx(&bar_full[s], a_bytes + b_load);
           tma_load_3d(st, &p.tmA, &bar_full[s], kc * kKC, m0, za);
-          tma_load_3d(st + 2 * a_bytes, &p.tmB, &bar_full[s], kc * kKC, n0, zb);
+          tma_load_3d(st + lo_mult * a_bytes, &p.tmB, &bar_full[s], kc * kKC, n0, zb);
           issued[s] += 1;
-          if (++s == kStages) {
+          if (++s == NS) {
             s = 0;
             ph ^= 1;
           }
@@ -305,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           }
           tc_fence_after();
           uint8_t *st = base + s * stage_bytes;
-          const uint32_t ahi = smem_u32(st), alo = ahi + a_bytes, bhi = ahi + 2 * a_bytes, blo = bhi + b_bytes;
+          const uint32_t ahi = smem_u32(st), alo = ahi + a_bytes, bhi = ahi + lo_mult * a_bytes, blo = bhi + b_bytes;
 #pragma unroll
           for (int kk = 0; kk < kKC / 8; ++kk) {
             const uint32_t off = kk * 32;  // 8 TF32 values = 32 bytes inside the swizzle row
@@ -317,7 +356,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             }
           }
           mma_commit(&bar_empty[s]);  // frees the stage once these products are done
-          if (++s == kStages) {
+          if (++s == NS) {
             s = 0;
             ph ^= 1;
           }
@@ -330,6 +369,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     }
   } else if (warp < 8) {
     // ---------------- head/tail split ----------------
+    // head = x rounded to TF32 (cvt.rna), tail = x - head rounded to TF32: the three products
+    // then miss only tail x tail and the tail's rounding (about 2^-22 relative per term)
     if (p.passes == 3) {
       const int ct = threadIdx.x - 64;  // 0 .. 191
       int s = 0;
@@ -347,23 +388,23 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           for (int v = ct; v < na + nb; v += 192) {
             uint8_t *hp = (v < na) ? st + 16 * v : st + 2 * a_bytes + 16 * (v - na);
             uint8_t *lp = hp + ((v < na) ? a_bytes : b_bytes);
-            float4 x = *reinterpret_cast<float4 *>(hp);
+            const float4 x = *reinterpret_cast<float4 *>(hp);
             float4 h, l;
-            h.x = __uint_as_float(__float_as_uint(x.x) & 0xFFFFE000u);
-            h.y = __uint_as_float(__float_as_uint(x.y) & 0xFFFFE000u);
-            h.z = __uint_as_float(__float_as_uint(x.z) & 0xFFFFE000u);
-            h.w = __uint_as_float(__float_as_uint(x.w) & 0xFFFFE000u);
-            l.x = x.x - h.x;
-            l.y = x.y - h.y;
-            l.z = x.z - h.z;
-            l.w = x.w - h.w;
+            h.x = to_tf32(x.x);
+            h.y = to_tf32(x.y);
+            h.z = to_tf32(x.z);
+            h.w = to_tf32(x.w);
+            l.x = to_tf32(x.x - h.x);
+            l.y = to_tf32(x.y - h.y);
+            l.z = to_tf32(x.z - h.z);
+            l.w = to_tf32(x.w - h.w);
             *reinterpret_cast<float4 *>(hp) = h;
             *reinterpret_cast<float4 *>(lp) = l;
           }
           fence_proxy_async();
           __syncwarp();
           if (lane == 0) mbar_arrive(&bar_conv[s]);
-          if (++s == kStages) {
+          if (++s == NS) {
             s = 0;
             ph ^= 1;
           }
@@ -373,58 +414,80 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
   } else {
     // ---------------- epilogue ----------------
     const int q = warp & 3;  // TMEM lane quarter of this warp
+    float *stg = stagebuf + (warp - 8) * 32 * 33;
+    const bool staged = p.epi == kStore && p.dn == 1 && p.dm != 1;  // row-major output: transpose first
+    const int nrow = (p.tm == 128) ? 32 : 16;  // accumulator rows this warp holds (lanes 0 .. nrow-1)
     int acc = 0;
     uint32_t aph[2] = {0, 0};
     for (int tile = blockIdx.x; tile < t.total; tile += gridDim.x) {
       int m0, z0, n0;
       tile_coords(p, t, tile, m0, z0, n0);
       if (!mbar_wait(&bar_tfull[acc], aph[acc], &abort_flag, p.err)) break;
+      __syncwarp();
       tc_fence_after();
-      // accumulator row of this thread: M = 128 -> lane 32q + l; M = 64 -> lanes 16 per quarter
-      const int row = (p.tm == 128) ? (32 * q + lane) : (lane < 16 ? 16 * q + lane : -1);
-      const int m = m0 + row;
-      const bool mrow = row >= 0 && m < p.M;
+      const int mq0 = m0 + (p.tm == 128 ? 32 * q : 16 * q);  // first row of this warp
+      const int m = mq0 + lane;
+      const bool mrow = lane < nrow && m < p.M;
       double dsum[4] = {0.0, 0.0, 0.0, 0.0};
       int zlast = -1;
       for (int c0 = 0; c0 < p.tn; c0 += 16) {
         float v[16];
         __syncwarp();  // tcgen05.ld is warp-collective
         tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * p.tn + c0), v);
-        if (!mrow) continue;
+        if (staged) {
+          // this lane's row segment into shared memory, then lanes take the columns: each store
+          // instruction writes 16 consecutive elements of one row (coalesced)
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const int j = c0 + i;
+          for (int i = 0; i < 16; ++i) stg[lane * 33 + i] = v[i];
+          __syncwarp();
+          const int cl = lane & 15, rh = lane >> 4;  // column in the chunk, row parity
+          const int j = c0 + cl;
           int z, n;
-          if (p.bstack > 1) {
-            if (j >= p.N * p.bstack) continue;  // rows past the stacked box: stale shared memory
-            z = z0 + j / p.N;
-            n = j % p.N;
-          } else {
-            z = z0;
-            n = n0 + j;
+          col_of(p, j, z0, n0, z, n);
+          const bool cok = z >= 0 && z < t.Zt && n < p.N;
+          for (int r = rh; r < nrow; r += 2) {
+            const int mm = mq0 + r;
+            if (cok && mm < p.M) {
+              float *d = p.D + (long)z * p.dz + (long)mm * p.dm + n;
+              const float x = p.alpha * stg[r * 33 + cl];
+              *d = p.beta ? *d + x : x;
+            }
           }
-          if (z >= t.Zt || n >= p.N) continue;
-          const float x = p.alpha * v[i];
-          if (p.epi == kStore) {
-            float *d = p.D + (long)z * p.dz + (long)m * p.dm + (long)n * p.dn;
-            *d = p.beta ? *d + x : x;
-          } else {
-            if (z != zlast) {
-              if (zlast >= 0)
+          __syncwarp();
+        } else if (p.epi == kStore) {
+          if (mrow) {
 #pragma unroll
-                for (int qq = 0; qq < 4; ++qq) atomicAdd(p.dot + (long)zlast * p.dstride + p.doff + qq, dsum[qq]);
-              dsum[0] = dsum[1] = dsum[2] = dsum[3] = 0.0;
+            for (int i = 0; i < 16; ++i) {
+              int z, n;
+              col_of(p, c0 + i, z0, n0, z, n);
+              if (z < 0 || z >= t.Zt || n >= p.N) continue;
+              float *d = p.D + (long)z * p.dz + (long)m * p.dm + (long)n * p.dn;
+              const float x = p.alpha * v[i];
+              *d = p.beta ? *d + x : x;
+            }
+          }
+        } else {
+          // closures: per-thread sums over this row, reduced over the warp when the batch entry
+          // changes (the column -> entry map is the same for every lane), one atomic per entry
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            int z, n;
+            col_of(p, c0 + i, z0, n0, z, n);
+            if (z < 0 || z >= t.Zt || n >= p.N) continue;
+            if (z != zlast) {
+              if (zlast >= 0) flush_dot(p, zlast, dsum, lane);
               zlast = z;
             }
-            const float *e = p.E + (long)z * p.ez + (long)m * p.em + (long)n * p.en;
+            if (mrow) {
+              const float x = p.alpha * v[i];
+              const float *e = p.E + (long)z * p.ez + (long)m * p.em + (long)n * p.en;
 #pragma unroll
-            for (int qq = 0; qq < 4; ++qq) dsum[qq] += (double)x * (double)e[qq * p.eq];
+              for (int qq = 0; qq < 4; ++qq) dsum[qq] += (double)x * (double)e[qq * p.eq];
+            }
           }
         }
       }
-      if (p.epi == kDot4 && zlast >= 0)
-#pragma unroll
-        for (int qq = 0; qq < 4; ++qq) atomicAdd(p.dot + (long)zlast * p.dstride + p.doff + qq, dsum[qq]);
+      if (p.epi == kDot4 && zlast >= 0) flush_dot(p, zlast, dsum, lane);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&bar_tempty[acc]);
@@ -438,7 +501,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
   if (threadIdx.x == 0 && abort_flag) {
     // the loads issued into each stage complete its full barrier in order: wait (bounded) for
     // the last one, so that no copy lands in shared memory after the CTA has gone
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < NS; ++s) {
       if (issued[s] == 0) continue;
       mbar_wait_bounded(&bar_full[s], (uint32_t)((issued[s] - 1) & 1));
     }
@@ -457,7 +520,21 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
   }
 }
 
-__host__ __device__ constexpr int smem_bytes(int tm, int tn) { return kStages * 2 * (tm + tn) * 128 + 1024; }
+// Shared memory of one launch: the stage ring (head and, with 3 passes, tail tiles), the
+// epilogue's transpose buffers and the 1024-byte alignment slack.
+__host__ __device__ constexpr int stage_bytes_of(int tm, int tn, int passes) {
+  return (passes == 3 ? 2 : 1) * (tm + tn) * 128;
+}
+__host__ __device__ constexpr int smem_bytes(int tm, int tn, int passes, int stages) {
+  return stages * stage_bytes_of(tm, tn, passes) + 4 * 32 * 33 * 4 + 1024;
+}
+// As many stages (2 .. kMaxStages) as fit in the opt-in shared memory.
+inline int stages_for(int tm, int tn, int passes, int smem_limit) {
+  int s = kMaxStages;
+  while (s > 2 && smem_bytes(tm, tn, passes, s) > smem_limit) --s;
+  return s;
+}
+
 
 }  // namespace tc
 }  // namespace mq
