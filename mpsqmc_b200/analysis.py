@@ -45,3 +45,20 @@ def variance_normalised(walker_steps_per_s: float, energies, walkers_per_step, e
     return {"steps_used": int(len(e)), "equil_steps": k0, "E_mean": float(e.mean()), "E_err": err,
             "walker_steps": n_ws, "sigma2_ws": sigma2_ws,
             "vn": walker_steps_per_s / sigma2_ws if sigma2_ws > 0 else float("nan")}
+
+
+def proposal_gain_bound(weights_per_step):
+    """The largest factor by which any auxiliary-field proposal could lower the variance of the
+    weighted mean energy, from the walkers' weights after propagation.
+
+    With the grid PDF every coupling multiplies a weight by sum P whatever x is drawn, so the
+    weights of a step differ only through the product of those sums along each walker's path.  A
+    proposal that made all weights equal (the best case, zero weight variance) would turn the
+    weighted mean's variance Var(E) / N_eff into Var(E) / N, N_eff = (sum w)^2 / sum w^2: a gain of
+    N / N_eff = N sum w^2 / (sum w)^2 at most.  Returns its mean over the steps."""
+    g = []
+    for w in weights_per_step:
+        w = np.asarray(w, dtype=np.float64)
+        if w.size and w.sum() > 0:
+            g.append(w.size * float(np.sum(w * w)) / float(w.sum()) ** 2)
+    return float(np.mean(g)) if g else float("nan")

@@ -200,7 +200,9 @@ struct SiteForms {          // device tables, one entry per site
   const long *sl_ld, *sr_ld;    // their row strides
 };
 
-// FP64 walker sites -> the two FP32 forms: SL_k[(s br + c) ldl + r], SR_k[(s bl + r) ldr + c].
+// FP64 walker sites -> the two FP32 forms: SL_k[(2c + s) ldl + r] (rows (c, sigma), k = the left
+// bond) and SR_k[(2r + s) ldr + c] (rows (r, sigma), k = the right bond).  Interleaving sigma in the
+// rows lets the sums over sigma of the trial products run as one product with sigma stacked along K.
 __global__ void convert_kernel(SiteForms f, const double *walkers, long wstride, const int *slot_of, const int *n_cur,
                                int cap, float *SL, float *SR) {
   const int k = blockIdx.y;
@@ -213,8 +215,8 @@ __global__ void convert_kernel(SiteForms f, const double *walkers, long wstride,
     const long q = e % per;
     const int r = (int)(q % bl), c = (int)((q / bl) % br), s = (int)(q / ((long)bl * br));
     const double x = walkers[(long)slot_of[w] * wstride + f.woff[k] + q];
-    SL[f.sl_off[k] + (long)w * f.sl_sz[k] + ((long)s * br + c) * ldl + r] = (float)x;
-    SR[f.sr_off[k] + (long)w * f.sr_sz[k] + ((long)s * bl + r) * ldr + c] = (float)x;
+    SL[f.sl_off[k] + (long)w * f.sl_sz[k] + (2L * c + s) * ldl + r] = (float)x;
+    SR[f.sr_off[k] + (long)w * f.sr_sz[k] + (2L * r + s) * ldr + c] = (float)x;
   }
 }
 
@@ -353,10 +355,10 @@ __global__ void site_op_kernel(SiteForms f, int si, int sj, const double *ob, do
     X[blk + q] = y1;
     float *sl = SL + f.sl_off[k] + (long)w * f.sl_sz[k];
     float *sr = SR + f.sr_off[k] + (long)w * f.sr_sz[k];
-    sl[(long)c * ldl + r] = (float)y0;
-    sl[((long)br + c) * ldl + r] = (float)y1;
-    sr[(long)r * ldr + c] = (float)y0;
-    sr[((long)bl + r) * ldr + c] = (float)y1;
+    sl[2L * c * ldl + r] = (float)y0;
+    sl[(2L * c + 1) * ldl + r] = (float)y1;
+    sr[2L * r * ldr + c] = (float)y0;
+    sr[(2L * r + 1) * ldr + c] = (float)y1;
   }
 }
 
@@ -385,8 +387,8 @@ __global__ void rescale_kernel(SiteForms f, int k, double *walkers, long wstride
     const double y = X[q] * inv;
     X[q] = y;
     const int r = (int)(q % bl), c = (int)((q / bl) % br), s = (int)(q / ((long)bl * br));
-    sl[((long)s * br + c) * ldl + r] = (float)y;
-    sr[((long)s * bl + r) * ldr + c] = (float)y;
+    sl[(2L * c + s) * ldl + r] = (float)y;
+    sr[(2L * r + s) * ldr + c] = (float)y;
   }
   if (threadIdx.x == 0) {
     ovb[w] *= inv;
@@ -441,10 +443,10 @@ __global__ void env_init_kernel(const float *P, long psz, long pld, int a, int b
 }
 
 // G[t](r, c) = delta_st Fd + sum_e J_e (Sx(s,t) F_x - iSy(s,t) F_y + Sz(s,t) F_z) for the channels
-// e closing on site k (a_k x b_k), sigma = s.
+// e closing on site k (a_k x b_k), sigma = s; stored Gb[r (2 gld) + t gld + c] (t stacked along K).
 __global__ void gbuild_kernel(int s, const float *Fd, long fsz, long fld, const float *Fch, long csz, int nslots,
                               const int *eslot, const float *eJ, int ne, int a, int b, EnvOps ops, float *Gb,
-                              long gsz, const int *n_cur, int cap) {
+                              long gsz, long gld, const int *n_cur, int cap) {
   const int N = min(*n_cur, cap);
   const long blk = (long)a * b;
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < blk * N; e += (long)gridDim.x * blockDim.x) {
@@ -459,11 +461,11 @@ __global__ void gbuild_kernel(int s, const float *Fd, long fsz, long fld, const 
       gy += eJ[i] * F[csz];
       gz += eJ[i] * F[2 * csz];
     }
-    float *Gw = Gb + (long)w * 2 * gsz + off;
+    float *Gw = Gb + (long)w * gsz + (q / b) * 2 * gld + q % b;
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
       const int o = s + 2 * t;
-      Gw[t * gsz] = ((s == t) ? fd : 0.f) + (float)ops.opSx[o] * gx - (float)ops.opISy[o] * gy + (float)ops.opSz[o] * gz;
+      Gw[t * gld] = ((s == t) ? fd : 0.f) + (float)ops.opSx[o] * gx - (float)ops.opISy[o] * gy + (float)ops.opSz[o] * gz;
     }
   }
 }
@@ -546,6 +548,10 @@ struct Plan {
   // FP32 trial copies: TO_k[s] rows c < a_{k+1}, k = r (ld pad4(a_k)); TT_k[s] rows r < a_k, k = c
   std::vector<long> to_off, tt_off;  // per (k, s): k * 2 + s
   float *TO = nullptr, *TT = nullptr;
+  // the same with sigma stacked along K (blocks of ldA): TOs_k[c][s ldA + r] = B_k[s](r, c),
+  // TTs_k[r][s ldA + c] = B_k[s](r, c); zero beyond the site's bond
+  std::vector<long> tos_off, tts_off;  // per k
+  float *TOs = nullptr, *TTs = nullptr;
   // walker forms and right environments
   std::vector<long> sl_off, sr_off, sl_sz, sr_sz, sl_ld, sr_ld, r_off, r_sz, r_ld;
   float *SL = nullptr, *SR = nullptr, *R = nullptr;
@@ -667,7 +673,7 @@ size_t bytes_needed(const Problem &pr) {
   }
   const long szBl = pad64(maxA * ldB), szX = pad64(2 * maxB * ldA), szN = pad64(maxB * ldB), szW = pad64(2 * maxB * ldB);
   const int ns = std::max(1, pr.nslots);
-  per += szBl * (1 + 4 + 2 + 2 + 3L * ns) + szX * (1 + 4 + 1 + 3L * ns) + 2 * szN + szW + pad64(maxB * ldA);
+  per += szBl * (1 + 4 + 2 + 2 + 3L * ns) + szX * (1 + 4 + 1 + 3L * ns) + 2 * szN + szW + pad64(2 * maxB * ldA);
   return (size_t)per * pr.capacity * sizeof(float) + (size_t)pr.capacity * 48 * sizeof(double);
 }
 
@@ -706,7 +712,16 @@ int build(const Problem &pr, Plan **out) {
       p->tt_off[2 * k + s] = ntt;
       ntt += pad64((long)a[k] * pad4(a[k + 1]));
     }
-  int rc = palloc(p, &p->TO, nto) | palloc(p, &p->TT, ntt);
+  p->tos_off.resize(L);
+  p->tts_off.resize(L);
+  long ntos = 0, ntts = 0;
+  for (int k = 0; k < L; ++k) {
+    p->tos_off[k] = ntos;
+    ntos += pad64((long)a[k + 1] * 2 * p->ldA);
+    p->tts_off[k] = ntts;
+    ntts += pad64((long)a[k] * 2 * p->ldA);
+  }
+  int rc = palloc(p, &p->TO, nto) | palloc(p, &p->TT, ntt) | palloc(p, &p->TOs, ntos) | palloc(p, &p->TTs, ntts);
   if (rc) return bail(MPSQMC_E_CUDA);
   {
     std::vector<double> tr;
@@ -715,7 +730,8 @@ int build(const Problem &pr, Plan **out) {
     tr.resize(tot);
     if (cudaMemcpy(tr.data(), pr.trial, sizeof(double) * tot, cudaMemcpyDeviceToHost) != cudaSuccess)
       return bail(fail(MPSQMC_E_CUDA, "batched sweep: trial download failed"));
-    std::vector<float> to(nto, 0.f), tt(ntt, 0.f);
+    std::vector<float> to(nto, 0.f), tt(ntt, 0.f), tos(ntos, 0.f), tts(ntts, 0.f);
+    const long l2 = 2 * p->ldA;
     for (int k = 0; k < L; ++k)
       for (int s = 0; s < 2; ++s) {
         const long lo = pad4(a[k]), lt = pad4(a[k + 1]);
@@ -724,10 +740,14 @@ int build(const Problem &pr, Plan **out) {
             const float x = (float)tr[pr.toff[k] + r + (long)a[k] * (c + (long)a[k + 1] * s)];
             to[p->to_off[2 * k + s] + c * lo + r] = x;
             tt[p->tt_off[2 * k + s] + (long)r * lt + c] = x;
+            tos[p->tos_off[k] + c * l2 + s * p->ldA + r] = x;
+            tts[p->tts_off[k] + (long)r * l2 + s * p->ldA + c] = x;
           }
       }
     if (cudaMemcpy(p->TO, to.data(), sizeof(float) * nto, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(p->TT, tt.data(), sizeof(float) * ntt, cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaMemcpy(p->TT, tt.data(), sizeof(float) * ntt, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->TOs, tos.data(), sizeof(float) * ntos, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->TTs, tts.data(), sizeof(float) * ntts, cudaMemcpyHostToDevice) != cudaSuccess)
       return bail(fail(MPSQMC_E_CUDA, "batched sweep: trial upload failed"));
   }
   // ---- walker forms and right environments (site k: per walker sizes, arrays of cap walkers)
@@ -762,7 +782,7 @@ int build(const Problem &pr, Plan **out) {
         palloc(p, &p->X4, 4 * p->szX * cap) | palloc(p, &p->Y, p->szX * cap) | palloc(p, &p->Nl[0], p->szN * cap) |
         palloc(p, &p->Nl[1], p->szN * cap) | palloc(p, &p->Wn, p->szW * cap) | palloc(p, &p->Fd[0], p->szBl * cap) |
         palloc(p, &p->Fd[1], p->szBl * cap) | palloc(p, &p->Gb, 2 * p->szBl * cap) |
-        palloc(p, &p->Q, pad64(maxB * p->ldA) * cap) | palloc(p, &p->Fch, 3L * ns * p->szBl * cap) |
+        palloc(p, &p->Q, pad64(2 * maxB * p->ldA) * cap) | palloc(p, &p->Fch, 3L * ns * p->szBl * cap) |
         palloc(p, &p->Xch, 3L * ns * p->szX * cap);
   rc |= palloc(p, &p->ovb, cap) | palloc(p, &p->wtb, cap) | palloc(p, &p->scl, cap) | palloc(p, &p->ob, 8 * cap) |
         palloc(p, &p->dot, 16 * cap) | palloc(p, &p->err_tc, 1) | palloc(p, &p->nb, 1);
@@ -809,12 +829,16 @@ int build(const Problem &pr, Plan **out) {
   auto TTo = [P](int k, int s) {
     return Opnd{P->TT + P->tt_off[2 * k + s], pad4(P->pr.aT[k + 1]), P->pr.aT[k], 0, 1, 0};
   };
-  // right environment R_k from R_{k+1}: Y = R_{k+1} SR_k^T, then R_k = sum_s TT_k[s] Y_s
+  auto TOso = [P](int k) { return Opnd{P->TOs + P->tos_off[k], 2 * P->ldA, P->pr.aT[k + 1], 0, 1, 0}; };
+  auto TTso = [P](int k) { return Opnd{P->TTs + P->tts_off[k], 2 * P->ldA, P->pr.aT[k], 0, 1, 0}; };
+  const long l2 = 2 * p->ldA;  // K of the sigma-stacked trial products
+  // right environment R_k from R_{k+1}: Y = R_{k+1} SR_k^T (rows (r, s)), then
+  // R_k = sum_s TT_k[s] Y_s as one product with s stacked along K
   auto right_env = [&](int k) -> int {
     int r = add_gemm(p, Ro(k + 1), SRo(k), a[k + 1], 2 * b[k], b[k + 1], 1, p->Y, p->szX, 1, p->ldA, 0);
-    for (int s = 0; s < 2 && !r; ++s) {
-      Opnd Yb{p->Y + (long)s * b[k] * p->ldA, p->ldA, b[k], p->szX, cap, 1};
-      r = add_gemm(p, TTo(k, s), Yb, a[k], b[k], a[k + 1], 1, p->R + p->r_off[k], p->r_sz[k], p->r_ld[k], 1, s);
+    if (!r) {
+      Opnd Yr{p->Y, l2, b[k], p->szX, cap, 1};
+      r = add_gemm(p, TTso(k), Yr, a[k], b[k], (int)l2, 1, p->R + p->r_off[k], p->r_sz[k], p->r_ld[k], 1, 0);
     }
     return r;
   };
@@ -824,7 +848,7 @@ int build(const Problem &pr, Plan **out) {
     int r = add_gemm(p, Le, SLo(i), a[i], 2 * b[i + 1], b[i], 1, p->X, p->szX, 1, p->ldA, 0);
     for (int s = 0; s < 2 && !r; ++s)
       for (int t = 0; t < 2 && !r; ++t) {
-        Opnd Xb{p->X + (long)t * b[i + 1] * p->ldA, p->ldA, b[i + 1], p->szX, cap, 1};
+        Opnd Xb{p->X + (long)t * p->ldA, l2, b[i + 1], p->szX, cap, 1};
         r = add_gemm(p, TOo(i, s), Xb, a[i + 1], b[i + 1], a[i], 1, p->P + (long)(s + 2 * t) * p->szBl, 4 * p->szBl,
                      p->ldB, 1, 0);
       }
@@ -836,9 +860,9 @@ int build(const Problem &pr, Plan **out) {
     Opnd S = SLo(m);
     S.div = 4;
     int r = add_gemm(p, Pq, S, a[m], 2 * b[m + 1], b[m], 4, p->X4, p->szX, 1, p->ldA, 0);
-    for (int s = 0; s < 2 && !r; ++s) {
-      Opnd Xb{p->X4 + (long)s * b[m + 1] * p->ldA, p->ldA, b[m + 1], p->szX, 4L * cap, 1};
-      r = add_gemm(p, TOo(m, s), Xb, a[m + 1], b[m + 1], a[m], 4, p->P, p->szBl, p->ldB, 1, s);
+    if (!r) {
+      Opnd Xr{p->X4, l2, b[m + 1], p->szX, 4L * cap, 1};
+      r = add_gemm(p, TOso(m), Xr, a[m + 1], b[m + 1], (int)l2, 4, p->P, p->szBl, p->ldB, 1, 0);
     }
     return r;
   };
@@ -852,7 +876,7 @@ int build(const Problem &pr, Plan **out) {
     int r = add_gemm(p, Ro(j + 1), SRo(j), a[j + 1], 2 * b[j], b[j + 1], 1, p->Y, p->szX, 1, p->ldA, 0);
     for (int s = 0; s < 2 && !r; ++s)
       for (int t = 0; t < 2 && !r; ++t) {
-        Opnd Yb{p->Y + (long)t * b[j] * p->ldA, p->ldA, b[j], p->szX, cap, 1};
+        Opnd Yb{p->Y + (long)t * p->ldA, l2, b[j], p->szX, cap, 1};
         r = add_gemm(p, TTo(j, s), Yb, a[j], b[j], a[j + 1], 1, p->X, 0, 0, 0, 0, 1.f, p->P, 4 * p->szBl, p->szBl,
                      p->ldB, 1, 4 * (s + 2 * t));
       }
@@ -927,12 +951,15 @@ int build(const Problem &pr, Plan **out) {
       if (!kept && (rc = left_branches(i))) return bail(rc);
       // left norm environment: Nl' = sum_s C[s]^T Nl C[s]
       {
+        // W = Nl SL_i (rows (c, s), ld of site i's left bond); Nl' = sum_s C[s]^T W_s in one
+        // product with s stacked along K (A = site i's left form read as rows c, K = (s, m))
+        const long ldl = p->sl_ld[i];
         Opnd Nlo{p->Nl[nl], p->ldB, b[i], p->szN, cap, 1};
-        rc = add_gemm(p, Nlo, SLo(i), b[i], 2 * bi1, b[i], 1, p->Wn, p->szW, 1, p->ldB, 0);
-        for (int s = 0; s < 2 && !rc; ++s) {
-          Opnd Ct{p->SL + p->sl_off[i] + (long)s * bi1 * p->sl_ld[i], p->sl_ld[i], bi1, p->sl_sz[i], cap, 1};
-          Opnd Wb{p->Wn + (long)s * bi1 * p->ldB, p->ldB, bi1, p->szW, cap, 1};
-          rc = add_gemm(p, Ct, Wb, bi1, bi1, b[i], 1, p->Nl[1 - nl], p->szN, p->ldB, 1, s);
+        rc = add_gemm(p, Nlo, SLo(i), b[i], 2 * bi1, b[i], 1, p->Wn, p->szW, 1, ldl, 0);
+        if (!rc) {
+          Opnd Ct{p->SL + p->sl_off[i], 2 * ldl, bi1, p->sl_sz[i], cap, 1};
+          Opnd Wr{p->Wn, 2 * ldl, bi1, p->szW, cap, 1};
+          rc = add_gemm(p, Ct, Wr, bi1, bi1, (int)(2 * ldl), 1, p->Nl[1 - nl], p->szN, p->ldB, 1, 0);
         }
         if (rc) return bail(rc);
         nl = 1 - nl;
@@ -970,25 +997,26 @@ int build(const Problem &pr, Plan **out) {
           return bail(fail(MPSQMC_E_CUDA, "batched sweep: channel upload failed"));
         const int ai = a[i], bi = b[i];
         const int nsl = ns;
+        const long ldl = p->sl_ld[i];
+        const long szQ = pad64(2 * maxB * p->ldA);
+        // per sigma: G_s[t] (rows r, K = (t, c)), Q_s = sum_t G_st C[t] in one product (t along K),
+        // stored Q[c (2 ldA) + s ldA + m]; then done' += sum_s TO_i[s] Q_s in one product
         for (int s = 0; s < 2; ++s) {
           p->ops.push_back([=](cudaStream_t st, double *) {
             gbuild_kernel<<<grid_elems(P, (long)ai * bi), 256, 0, st>>>(s, Fdc, P->szBl, P->ldB, P->Fch, P->szBl, nsl,
-                                                                        es_d, ej_d, ne, ai, bi, eo, P->Gb, P->szBl,
-                                                                        ncur, icap);
+                                                                        es_d, ej_d, ne, ai, bi, eo, P->Gb, 2 * P->szBl,
+                                                                        ldl, ncur, icap);
             return cudaGetLastError() == cudaSuccess ? 0 : fail(MPSQMC_E_CUDA, "batched sweep: energy");
           });
           p->launches += 1;
-          for (int t = 0; t < 2 && !rc; ++t) {
-            Opnd Gt{p->Gb + (long)t * p->szBl, p->ldB, ai, 2 * p->szBl, cap, 1};
-            Opnd Ct{p->SL + p->sl_off[i] + (long)t * bi1 * p->sl_ld[i], p->sl_ld[i], bi1, p->sl_sz[i], cap, 1};
-            rc = add_gemm(p, Gt, Ct, ai, bi1, bi, 1, p->Q, pad64(maxB * p->ldA), 1, p->ldA, t);
-          }
-          if (!rc) {
-            Opnd Qo{p->Q, p->ldA, bi1, pad64(maxB * p->ldA), cap, 1};
-            rc = add_gemm(p, TOo(i, s), Qo, ai1, bi1, ai, 1, Fdn, p->szBl, p->ldB, 1, 1);
-          }
+          Opnd Gr{p->Gb, 2 * ldl, ai, 2 * p->szBl, cap, 1};
+          Opnd Cr{p->SL + p->sl_off[i], 2 * ldl, bi1, p->sl_sz[i], cap, 1};
+          rc = add_gemm(p, Gr, Cr, ai, bi1, (int)(2 * ldl), 1, p->Q + (long)s * p->ldA, szQ, 1, l2, 0);
           if (rc) return bail(rc);
         }
+        Opnd Qr{p->Q, l2, bi1, szQ, cap, 1};
+        rc = add_gemm(p, TOso(i), Qr, ai1, bi1, (int)l2, 1, Fdn, p->szBl, p->ldB, 1, 1);
+        if (rc) return bail(rc);
       }
       bool cont = false;
       for (int e = e0; e < e1; ++e) cont |= q.ech_cont[e] != 0;
@@ -997,9 +1025,9 @@ int build(const Problem &pr, Plan **out) {
         Opnd S = SLo(i);
         S.div = 3 * ns;
         rc = add_gemm(p, Fo, S, a[i], 2 * bi1, b[i], 3 * ns, p->Xch, p->szX, 1, p->ldA, 0);
-        for (int s = 0; s < 2 && !rc; ++s) {
-          Opnd Xb{p->Xch + (long)s * bi1 * p->ldA, p->ldA, bi1, p->szX, 3L * ns * cap, 1};
-          rc = add_gemm(p, TOo(i, s), Xb, ai1, bi1, a[i], 3 * ns, p->Fch, p->szBl, p->ldB, 1, s);
+        if (!rc) {
+          Opnd Xr{p->Xch, l2, bi1, p->szX, 3L * ns * cap, 1};
+          rc = add_gemm(p, TOso(i), Xr, ai1, bi1, (int)l2, 3 * ns, p->Fch, p->szBl, p->ldB, 1, 0);
         }
         if (rc) return bail(rc);
       }

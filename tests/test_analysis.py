@@ -35,3 +35,10 @@ def test_variance_normalised_scales_with_throughput():
     b = analysis.variance_normalised(2000.0, e, np.full(500, 2048))
     assert b["vn"] == pytest.approx(2 * a["vn"])
     assert a["steps_used"] == 400 and a["equil_steps"] == 100
+
+
+def test_proposal_gain_bound():
+    from mpsqmc_b200 import analysis
+    assert analysis.proposal_gain_bound([np.ones(10)]) == pytest.approx(1.0)
+    w = np.array([1.0, 1.0, 2.0, 4.0])
+    assert analysis.proposal_gain_bound([w, w]) == pytest.approx(4 * 22 / 64)
