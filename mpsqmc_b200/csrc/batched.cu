@@ -425,9 +425,10 @@ struct EnvOps {
   double opSx[4], opISy[4], opSz[4];
 };
 
-// done' = -h sum_e Sz[e] P_e (the field closes on the site) over a_{k+1} x b_{k+1}.
+// done' (+)= -h sum_e Sz[e] P_e (the field closes on the site) over a_{k+1} x b_{k+1}; add: the
+// products of the closing channels are already in Fdn.
 __global__ void env_init_kernel(const float *P, long psz, long pld, int a, int b, float *Fdn, long fsz, long fld,
-                                double h, EnvOps ops, const int *n_cur, int cap) {
+                                double h, EnvOps ops, int add, const int *n_cur, int cap) {
   const int N = min(*n_cur, cap);
   const long blk = (long)a * b;
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < blk * N; e += (long)gridDim.x * blockDim.x) {
@@ -438,7 +439,8 @@ __global__ void env_init_kernel(const float *P, long psz, long pld, int a, int b
     float fz = 0.f;
 #pragma unroll
     for (int k = 0; k < 4; ++k) fz += (float)ops.opSz[k] * Pw[k * psz];
-    Fdn[(long)w * fsz + r * fld + c] = (float)(-h) * fz;
+    float *f = Fdn + (long)w * fsz + r * fld + c;
+    *f = add ? *f + (float)(-h) * fz : (float)(-h) * fz;
   }
 }
 
@@ -561,6 +563,7 @@ struct Plan {
   long szX = 0;                    // 2 maxB x ldA (a column-major block with sigma-stacked rows)
   long szN = 0;                    // maxB x ldB
   long szW = 0;                    // 2 maxB x ldB
+  float *Fdn_ptr(int fd) { return Fd[1 - fd]; }
   float *Lenv = nullptr, *P = nullptr, *X = nullptr, *X4 = nullptr, *Y = nullptr, *Nl[2] = {nullptr, nullptr},
         *Wn = nullptr, *Fd[2] = {nullptr, nullptr}, *Gb = nullptr, *Q = nullptr, *Fch = nullptr, *Xch = nullptr;
   double *ovb = nullptr, *wtb = nullptr, *scl = nullptr, *ob = nullptr, *dot = nullptr;
@@ -969,13 +972,18 @@ int build(const Problem &pr, Plan **out) {
     }
     // energy channels and the trial-walker left environment through site i
     {
-      float *Fdn = p->Fd[1 - fd], *Fdc = p->Fd[fd];
-      p->ops.push_back([=](cudaStream_t s, double *) {
-        env_init_kernel<<<grid_elems(P, (long)ai1 * bi1), 256, 0, s>>>(P->P, P->szBl, P->ldB, ai1, bi1, Fdn, P->szBl,
-                                                                       P->ldB, q.h, eo, ncur, icap);
-        return cudaGetLastError() == cudaSuccess ? 0 : fail(MPSQMC_E_CUDA, "batched sweep: energy");
-      });
-      p->launches += 1;
+      float *Fdn = p->Fdn_ptr(fd), *Fdc = p->Fd[fd];
+      // the field term -h sum Sz P: written alone on site 0, added after the channel products on
+      // later sites (h != 0)
+      auto field_term = [=](int add) {
+        P->ops.push_back([=](cudaStream_t s, double *) {
+          env_init_kernel<<<grid_elems(P, (long)ai1 * bi1), 256, 0, s>>>(P->P, P->szBl, P->ldB, ai1, bi1, Fdn,
+                                                                         P->szBl, P->ldB, q.h, eo, add, ncur, icap);
+          return cudaGetLastError() == cudaSuccess ? 0 : fail(MPSQMC_E_CUDA, "batched sweep: energy");
+        });
+        P->launches += 1;
+      };
+      if (i == 0) field_term(0);
       const int e0 = q.ech_off[i], e1 = q.ech_off[i + 1];
       int ne = 0;
       for (int e = e0; e < e1; ++e) ne += (q.ech_J[e] != 0.0) ? 1 : 0;
@@ -1015,8 +1023,9 @@ int build(const Problem &pr, Plan **out) {
           if (rc) return bail(rc);
         }
         Opnd Qr{p->Q, l2, bi1, szQ, cap, 1};
-        rc = add_gemm(p, TOso(i), Qr, ai1, bi1, (int)l2, 1, Fdn, p->szBl, p->ldB, 1, 1);
+        rc = add_gemm(p, TOso(i), Qr, ai1, bi1, (int)l2, 1, Fdn, p->szBl, p->ldB, 1, 0);
         if (rc) return bail(rc);
+        if (q.h != 0.0) field_term(1);
       }
       bool cont = false;
       for (int e = e0; e < e1; ++e) cont |= q.ech_cont[e] != 0;
