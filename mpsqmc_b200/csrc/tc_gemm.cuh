@@ -38,7 +38,7 @@ constexpr int kMaxStages = 4;        // shared-memory stages of the load ring (2
 constexpr int kKC = 32;                 // k-values per stage (128 bytes of FP32: one swizzle row)
 constexpr int kMaxTN = 256;
 constexpr int kErrTimeout = 4;          // bit in the device error word (batched.h: bs::kErrTimeout)
-constexpr unsigned long long kWaitNs = 2000000000ull;  // a pipeline wait gives up after 2 s
+constexpr long long kWaitCycles = 4000000000LL;  // a pipeline wait gives up after ~2 s of SM cycles
 
 enum Epilogue : int { kStore = 0, kDot4 = 1 };
 
@@ -98,22 +98,19 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-__device__ __forceinline__ unsigned long long now_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
 // Bounded wait for the phase of `parity` to complete.  Returns false (and flags the error) when
-// kWaitNs pass or another role already gave up.
+// about kWaitCycles SM cycles pass or another role already gave up.  The cycle counter is read
+// only after the first 64 polls, so a wait that completes soon costs nothing beyond the polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = now_ns();
   unsigned n = 0;
+  long long t0 = 0;
   while (!mbar_try(bar, parity)) {
     if (((++n) & 63) == 0) {
       if (*abort_flag) return false;
-      if (now_ns() - t0 > kWaitNs) {
+      const long long now = clock64();
+      if (t0 == 0) {
+        t0 = now;
+      } else if (now - t0 > kWaitCycles) {
         *abort_flag = 1;
         atomicOr(err, kErrTimeout);
         return false;
@@ -125,8 +122,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
 
 // Bounded wait used at teardown (no abort flag).
 __device__ __forceinline__ void mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-  const unsigned long long t0 = now_ns();
-  while (!mbar_try(bar, parity) && now_ns() - t0 < kWaitNs) {
+  const long long t0 = clock64();
+  while (!mbar_try(bar, parity) && clock64() - t0 < kWaitCycles) {
   }
 }
 
@@ -213,38 +210,11 @@ __device__ __forceinline__ void tile_coords(const GemmParams &p, const Tiling &t
   }
 }
 
-// tile column j -> batch entry z and row n of B (z < 0: past the stacked box)
-__device__ __forceinline__ void col_of(const GemmParams &p, int j, int z0, int n0, int &z, int &n) {
-  if (p.bstack > 1) {
-    if (j >= p.N * p.bstack) {  // rows past the stacked box: stale shared memory
-      z = -1;
-      n = 0;
-      return;
-    }
-    z = z0 + j / p.N;
-    n = j % p.N;
-  } else {
-    z = z0;
-    n = n0 + j;
-  }
-}
-
 // x rounded to the nearest TF32 value (10 explicit mantissa bits), as an FP32 bit pattern
 __device__ __forceinline__ float to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
-}
-
-// closures: the warp's four partial sums of batch entry z into dot (one atomic per sum)
-__device__ __forceinline__ void flush_dot(const GemmParams &p, int z, double *dsum, int lane) {
-#pragma unroll
-  for (int qq = 0; qq < 4; ++qq) {
-    double v = dsum[qq];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) atomicAdd(p.dot + (long)z * p.dstride + p.doff + qq, v);
-    dsum[qq] = 0.0;
-  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -413,10 +383,45 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     }
   } else {
     // ---------------- epilogue ----------------
+    // every launch parameter the loops below use, copied to registers once: a store through D
+    // may alias the parameter block as far as the compiler can tell, so reading the parameters
+    // in place would repeat those loads after every store
+    const int M = p.M, N = p.N, tm = p.tm, tn = p.tn, bstack = p.bstack, beta = p.beta, Zt = t.Zt;
+    const int dot4 = p.epi == kDot4;
+    const float alpha = p.alpha;
+    float *const D = p.D;
+    const long dz = p.dz, dm = p.dm, dn = p.dn;
+    const float *const E = p.E;
+    const long ez = p.ez, eq = p.eq, em = p.em, en = p.en;
+    double *const dot = p.dot;
+    const long dstride = p.dstride, doff = p.doff;
+    const int NB = N * bstack;
+    // every 16-column chunk lies in one batch entry (unstacked tiles, or N a multiple of 16)
+    const bool chunk_uniform = bstack == 1 || (N & 15) == 0;
     const int q = warp & 3;  // TMEM lane quarter of this warp
     float *stg = stagebuf + (warp - 8) * 32 * 33;
-    const bool staged = p.epi == kStore && p.dn == 1 && p.dm != 1;  // row-major output: transpose first
-    const int nrow = (p.tm == 128) ? 32 : 16;  // accumulator rows this warp holds (lanes 0 .. nrow-1)
+    const bool staged = !dot4 && dn == 1 && dm != 1;  // row-major output: transpose first
+    const int nrow = (tm == 128) ? 32 : 16;            // accumulator rows this warp holds (lanes 0 .. nrow-1)
+    // tile column j -> batch entry z (-1: past the stacked box, stale shared memory) and row n of B
+    auto col = [&](int j, int z0, int n0, int &z, int &n) {
+      if (bstack > 1) {
+        z = (j < NB) ? z0 + j / N : -1;
+        n = j % N;
+      } else {
+        z = z0;
+        n = n0 + j;
+      }
+    };
+    // closures: the warp's four partial sums of entry z (one atomic per sum)
+    auto flush = [&](int z, double *ds) {
+#pragma unroll
+      for (int qq = 0; qq < 4; ++qq) {
+        double v = ds[qq];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) atomicAdd(dot + (long)z * dstride + doff + qq, v);
+        ds[qq] = 0.0;
+      }
+    };
     int acc = 0;
     uint32_t aph[2] = {0, 0};
     for (int tile = blockIdx.x; tile < t.total; tile += gridDim.x) {
@@ -425,69 +430,117 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       if (!mbar_wait(&bar_tfull[acc], aph[acc], &abort_flag, p.err)) break;
       __syncwarp();
       tc_fence_after();
-      const int mq0 = m0 + (p.tm == 128 ? 32 * q : 16 * q);  // first row of this warp
+      const int mq0 = m0 + (tm == 128 ? 32 * q : 16 * q);  // first row of this warp
       const int m = mq0 + lane;
-      const bool mrow = lane < nrow && m < p.M;
+      const bool mrow = lane < nrow && m < M;
       double dsum[4] = {0.0, 0.0, 0.0, 0.0};
       int zlast = -1;
-      for (int c0 = 0; c0 < p.tn; c0 += 16) {
+      for (int c0 = 0; c0 < tn; c0 += 16) {
         float v[16];
         __syncwarp();  // tcgen05.ld is warp-collective
-        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * p.tn + c0), v);
-        if (staged) {
-          // this lane's row segment into shared memory, then lanes take the columns: each store
-          // instruction writes 16 consecutive elements of one row (coalesced)
+        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * tn + c0), v);
+        int z, n;
+        col(c0, z0, n0, z, n);  // the chunk's first column
+        if (z < 0 || z >= Zt || n >= N) continue;  // the same for every lane
+        if (chunk_uniform) {
+          // all 16 columns belong to entry z, rows n .. n + nv - 1 of B: one base pointer per chunk
+          const int nv = min(16, N - n);
+          if (staged) {
+            // this lane's row segment into shared memory, then lanes take the columns: each
+            // store instruction writes 16 consecutive elements of each of two rows (coalesced)
 #pragma unroll
-          for (int i = 0; i < 16; ++i) stg[lane * 33 + i] = v[i];
-          __syncwarp();
-          const int cl = lane & 15, rh = lane >> 4;  // column in the chunk, row parity
-          const int j = c0 + cl;
-          int z, n;
-          col_of(p, j, z0, n0, z, n);
-          const bool cok = z >= 0 && z < t.Zt && n < p.N;
-          for (int r = rh; r < nrow; r += 2) {
-            const int mm = mq0 + r;
-            if (cok && mm < p.M) {
-              float *d = p.D + (long)z * p.dz + (long)mm * p.dm + n;
-              const float x = p.alpha * stg[r * 33 + cl];
-              *d = p.beta ? *d + x : x;
+            for (int i = 0; i < 16; ++i) stg[lane * 33 + i] = v[i];
+            __syncwarp();
+            const int cl = lane & 15, rh = lane >> 4;  // column in the chunk, row parity
+            if (cl < nv) {
+              float *d = D + (long)z * dz + (long)(mq0 + rh) * dm + (n + cl);
+              const int rows = min(nrow, M - mq0);
+              for (int r = rh; r < rows; r += 2, d += 2 * dm) {
+                const float x = alpha * stg[r * 33 + cl];
+                *d = beta ? *d + x : x;
+              }
             }
-          }
-          __syncwarp();
-        } else if (p.epi == kStore) {
-          if (mrow) {
+            __syncwarp();
+          } else if (!dot4) {
+            if (mrow) {
+              float *d = D + (long)z * dz + (long)m * dm + (long)n * dn;
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              int z, n;
-              col_of(p, c0 + i, z0, n0, z, n);
-              if (z < 0 || z >= t.Zt || n >= p.N) continue;
-              float *d = p.D + (long)z * p.dz + (long)m * p.dm + (long)n * p.dn;
-              const float x = p.alpha * v[i];
-              *d = p.beta ? *d + x : x;
+              for (int i = 0; i < 16; ++i)
+                if (i < nv) {
+                  const float x = alpha * v[i];
+                  d[i * dn] = beta ? d[i * dn] + x : x;
+                }
             }
-          }
-        } else {
-          // closures: per-thread sums over this row, reduced over the warp when the batch entry
-          // changes (the column -> entry map is the same for every lane), one atomic per entry
-#pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            int z, n;
-            col_of(p, c0 + i, z0, n0, z, n);
-            if (z < 0 || z >= t.Zt || n >= p.N) continue;
+          } else {
             if (z != zlast) {
-              if (zlast >= 0) flush_dot(p, zlast, dsum, lane);
+              if (zlast >= 0) flush(zlast, dsum);
               zlast = z;
             }
             if (mrow) {
-              const float x = p.alpha * v[i];
-              const float *e = p.E + (long)z * p.ez + (long)m * p.em + (long)n * p.en;
+              const float *e = E + (long)z * ez + (long)m * em + (long)n * en;
 #pragma unroll
-              for (int qq = 0; qq < 4; ++qq) dsum[qq] += (double)x * (double)e[qq * p.eq];
+              for (int i = 0; i < 16; ++i)
+                if (i < nv) {
+                  const double x = (double)(alpha * v[i]);
+#pragma unroll
+                  for (int qq = 0; qq < 4; ++qq) dsum[qq] += x * (double)e[i * en + qq * eq];
+                }
+            }
+          }
+          continue;
+        }
+        // a chunk that spans two batch entries (stacked tiles with N not a multiple of 16): per element
+        if (staged) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) stg[lane * 33 + i] = v[i];
+          __syncwarp();
+          const int cl = lane & 15, rh = lane >> 4;
+          int zc, nc;
+          col(c0 + cl, z0, n0, zc, nc);
+          if (zc >= 0 && zc < Zt && nc < N) {
+            float *dcol = D + (long)zc * dz + nc;
+            for (int r = rh; r < nrow; r += 2) {
+              const int mm = mq0 + r;
+              if (mm < M) {
+                float *d = dcol + (long)mm * dm;
+                const float x = alpha * stg[r * 33 + cl];
+                *d = beta ? *d + x : x;
+              }
+            }
+          }
+          __syncwarp();
+        } else if (!dot4) {
+          if (mrow) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              int zi, ni;
+              col(c0 + i, z0, n0, zi, ni);
+              if (zi < 0 || zi >= Zt || ni >= N) continue;
+              float *d = D + (long)zi * dz + (long)m * dm + (long)ni * dn;
+              const float x = alpha * v[i];
+              *d = beta ? *d + x : x;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            int zi, ni;
+            col(c0 + i, z0, n0, zi, ni);
+            if (zi < 0 || zi >= Zt || ni >= N) continue;
+            if (zi != zlast) {
+              if (zlast >= 0) flush(zlast, dsum);
+              zlast = zi;
+            }
+            if (mrow) {
+              const float x = alpha * v[i];
+              const float *e = E + (long)zi * ez + (long)m * em + (long)ni * en;
+#pragma unroll
+              for (int qq = 0; qq < 4; ++qq) dsum[qq] += (double)x * (double)e[qq * eq];
             }
           }
         }
       }
-      if (p.epi == kDot4 && zlast >= 0) flush_dot(p, zlast, dsum, lane);
+      if (dot4 && zlast >= 0) flush(zlast, dsum);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&bar_tempty[acc]);
