@@ -17,7 +17,7 @@
 //
 // Roles (384 threads, one CTA per SM, persistent over tiles):
 //   warp 0      TMA producer (one lane), ring of 2-4 shared-memory stages (as many as fit);
-//   warp 1      TMEM owner and MMA issuer (one lane); two accumulators of tn columns;
+//   warp 1      TMEM owner and MMA issuer (one lane); two or four accumulators of tn columns;
 //   warps 2-7   head/tail split of each landed stage (passes = 3);
 //   warps 8-11  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM lanes 32 (w % 4)...),
 //               alpha/beta and the store to D; row-major outputs are transposed through shared
@@ -223,7 +223,7 @@ __device__ __forceinline__ float to_tf32(float x) {
 __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ GemmParams p) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ uint64_t bar_full[kMaxStages], bar_conv[kMaxStages], bar_empty[kMaxStages];
-  __shared__ uint64_t bar_tfull[2], bar_tempty[2], bar_drain;
+  __shared__ uint64_t bar_tfull[4], bar_tempty[4], bar_drain;
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
   __shared__ int issued[kMaxStages];  // loads issued per stage (for the drain at exit)
@@ -238,7 +238,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
   float *stagebuf = reinterpret_cast<float *>(base + NS * stage_bytes);  // epilogue transposes
   const Tiling t = tiling(p);
   const int nk = (p.K + kKC - 1) / kKC;
-  const int tcols = p.tn <= 16 ? 32 : (p.tn <= 32 ? 64 : (p.tn <= 64 ? 128 : (p.tn <= 128 ? 256 : 512)));
+  // accumulators in TMEM: four when they fit in its 512 columns (more slack between the products
+  // of one tile and the epilogue of an earlier one), else two
+  const int nacc = p.tn <= 128 ? 4 : 2;
+  const int need = nacc * p.tn;
+  const int tcols = need <= 32 ? 32 : (need <= 64 ? 64 : (need <= 128 ? 128 : (need <= 256 ? 256 : 512)));
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NS; ++s) {
@@ -247,7 +251,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       mbar_init(&bar_empty[s], 1);
       issued[s] = 0;
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < 4; ++b) {
       mbar_init(&bar_tfull[b], 1);
       mbar_init(&bar_tempty[b], 4);
     }
@@ -299,7 +303,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       int s = 0;
       uint32_t ph = 0;
       int acc = 0;
-      uint32_t aph[2] = {0, 0};
+      uint32_t aph[4] = {0, 0, 0, 0};
       const uint32_t idesc = instr_desc(p.tm, p.tn);
       bool ok = true;
       for (int tile = blockIdx.x; tile < t.total && ok; tile += gridDim.x) {
@@ -334,7 +338,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         if (!ok) break;
         mma_commit(&bar_tfull[acc]);
         aph[acc] ^= 1;
-        acc ^= 1;
+        acc = (acc + 1 == nacc) ? 0 : acc + 1;
       }
     }
   } else if (warp < 8) {
@@ -423,7 +427,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       }
     };
     int acc = 0;
-    uint32_t aph[2] = {0, 0};
+    uint32_t aph[4] = {0, 0, 0, 0};
     for (int tile = blockIdx.x; tile < t.total; tile += gridDim.x) {
       int m0, z0, n0;
       tile_coords(p, t, tile, m0, z0, n0);
@@ -545,7 +549,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       __syncwarp();
       if (lane == 0) mbar_arrive(&bar_tempty[acc]);
       aph[acc] ^= 1;
-      acc ^= 1;
+      acc = (acc + 1 == nacc) ? 0 : acc + 1;
     }
   }
 
