@@ -243,6 +243,14 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
                                       * 37 (1995) 185), so the weight factor P(x) / q_mix(x) is at
                                       * most sum P / alpha and a poorly trained network cannot
                                       * give heavy-tailed weights.  1000 samples the grid PDF. */
+#define MPSQMC_OPT_TC_STACK_TN 11     /* tile choices of the tcgen05 sweep's products (defaults
+                                      * 256, 256, 4; mpsqmc_autotune picks them per bond profile):
+                                      * widest N tile (64, 128, 256) of the products whose left
+                                      * factor is a trial tensor, walkers stacked along N up to it */
+#define MPSQMC_OPT_TC_WIDE_TN 12      /*   widest N tile (64, 128, 256) of the walker-by-walker
+                                      *   products */
+#define MPSQMC_OPT_TC_STAGES 13       /*   load-ring depth cap, 2..4 (fewer when shared memory is
+                                      *   short) */
 int mpsqmc_set_option(mpsqmc_ctx *ctx, int option, long value);
 int mpsqmc_get_option(mpsqmc_ctx *ctx, int option, long *value);
 
@@ -288,9 +296,12 @@ int mpsqmc_proposal_stats(mpsqmc_ctx *ctx, double *last_loss, int *updates);
 /* Autotuner (no counterpart in the reference): times `steps` steps of every applicable
  * (MPSQMC_OPT_SWEEP, MPSQMC_OPT_WORKSPACE) choice on the first walkers of the current population
  * (two waves of one CTA per SM), restores the population, random stream and step count after
- * each trial, and keeps the fastest.  The choice is remembered per problem shape (L, trial and
- * walker bond dims, couplings, projector) for later contexts of this process, which then skip the
- * measurement.  best_* (may be NULL) receive the chosen option values. */
+ * each trial, and keeps the fastest.  Under the tcgen05 sweep (MPSQMC_PRECISION_TF32X3_TC,
+ * TF32_TC) it instead tunes that sweep's tile choices (MPSQMC_OPT_TC_STACK_TN, _WIDE_TN, _STAGES)
+ * by a coordinate search from the defaults, each timed on up to 1024 walkers (its tile counts
+ * grow with the population).  The choice is remembered per problem shape (L, trial and walker
+ * bond dims, couplings, projector, sweep family) for later contexts of this process, which then
+ * skip the measurement.  best_* (may be NULL) receive the chosen sweep and workspace values. */
 int mpsqmc_autotune(mpsqmc_ctx *ctx, int steps, int *best_sweep, int *best_workspace);
 
 /* ---------------------------------------------------------------------------------------------

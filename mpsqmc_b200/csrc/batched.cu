@@ -67,6 +67,29 @@ int make_operand_map(CUtensorMap *map, const float *base, long k_ext, long rows,
   return 0;
 }
 
+// Column-major D (element (m, n, z) at D[m + n dn + z dz]) as the epilogue's store map: box
+// (box_rows, 16, 1), no swizzle; extents M x N x zs clip what a box holds past them.  Used when
+// dn and dz are multiples of 4 and D is 16-byte aligned (else the epilogue stores directly).
+bool make_store_map(CUtensorMap *map, float *D, long M, long N, long zs, long dn, long dz, int box_rows) {
+  EncodeTiled enc = encoder();
+  if (!enc || (reinterpret_cast<uintptr_t>(D) & 15) || (dn & 3) || (dz & 3) || dn < M || (zs > 1 && dz < N * dn))
+    return false;
+  cuuint64_t dims[3] = {(cuuint64_t)M, (cuuint64_t)N, (cuuint64_t)std::max(1L, zs)};
+  cuuint64_t strides[2] = {(cuuint64_t)dn * 4, (cuuint64_t)std::max(dz, N * dn) * 4};
+  cuuint32_t box[3] = {(cuuint32_t)box_rows, 16, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, D, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+// The epilogue's store route: TMA boxes for column-major outputs without accumulation.
+void pick_store(GemmParams &p, long zs) {
+  p.dtma = 0;
+  if (p.epi == kStore && p.dm == 1 && !p.beta && p.dn > 1)
+    p.dtma = make_store_map(&p.tmD, p.D, p.M, p.N, zs, p.dn, p.dz, p.tm == 128 ? 32 : 16) ? 1 : 0;
+}
+
 // SM count and the dynamic shared memory a launch may use (the opt-in limit less the kernel's
 // static barriers), set once per process.
 int configure_kernel(int *sms, int *smem_limit) {
@@ -88,12 +111,12 @@ int configure_kernel(int *sms, int *smem_limit) {
   return 0;
 }
 
-// The load ring's depth for this tile shape (as deep as shared memory allows).
-int pick_stages(GemmParams &p) {
+// The load ring's depth for this tile shape (as deep as shared memory allows, at most max_stages).
+int pick_stages(GemmParams &p, int max_stages = kMaxStages) {
   int sms = 0, limit = 0;
   const int rc = configure_kernel(&sms, &limit);
   if (rc) return rc;
-  p.stages = stages_for(p.tm, p.tn, p.passes, limit);
+  p.stages = std::max(2, std::min(max_stages, stages_for(p.tm, p.tn, p.passes, limit)));
   if (smem_bytes(p.tm, p.tn, p.passes, p.stages) > limit)
     return fail(MPSQMC_E_UNSUPPORTED, "tcgen05 GEMM tile does not fit in shared memory");
   return 0;
@@ -158,6 +181,7 @@ extern "C" int mpsqmc_tc_gemm(float *D, const float *A, const float *B, int M, i
   const long arows = ((M + p.tm - 1) / p.tm) * p.tm;
   const long brows = bstack > 1 ? N : ((N + p.tn - 1) / p.tn) * p.tn;
   int rc = pick_stages(p);
+  pick_store(p, Z);
   if (!rc) rc = make_operand_map(&p.tmA, A, kpad, arows, std::max(1L, a_zcount), lda, a_zstride, p.tm, 1);
   if (!rc) rc = make_operand_map(&p.tmB, B, kpad, brows, std::max(1L, b_zcount), ldb, b_zstride, p.brows, bstack);
   if (rc) return rc;
@@ -611,13 +635,14 @@ int add_gemm(Plan *p, const Opnd &A, const Opnd &B, int M, int N, int K, int zpe
   g.N = N;
   g.K = K;
   g.tm = tm_for(M);
+  const Tiles &t = p->pr.tiles;
   int bstack = 1;
-  if (A.div == 0 && (N & 7) == 0 && N <= 128) bstack = kMaxTN / N;
+  if (A.div == 0 && (N & 7) == 0 && 2 * N <= t.stack_tn) bstack = t.stack_tn / N;
   if (bstack > 1) {
-    g.tn = N * bstack;
+    g.tn = (N * bstack + 15) & ~15;  // the MMA's N: a multiple of 16 (columns past N bstack unused)
     g.brows = N;
   } else {
-    g.tn = std::min(kMaxTN, (N + 15) & ~15);
+    g.tn = std::min(A.div == 0 ? t.stack_tn : t.wide_tn, (N + 15) & ~15);
     g.brows = g.tn;
   }
   g.bstack = bstack;
@@ -644,7 +669,8 @@ int add_gemm(Plan *p, const Opnd &A, const Opnd &B, int M, int N, int K, int zpe
     g.dstride = 16;
     g.doff = doff;
   }
-  int rc = pick_stages(g);
+  int rc = pick_stages(g, t.max_stages);
+  pick_store(g, (long)zper * p->cap);
   if (!rc) rc = make_operand_map(&g.tmA, A.base, K, A.rows, std::max(1L, A.zn), A.ld, A.zs, g.tm, 1);
   if (!rc) rc = make_operand_map(&g.tmB, B.base, K, bstack > 1 ? N : B.rows, std::max(1L, B.zn), B.ld, B.zs, g.brows,
                                  bstack);

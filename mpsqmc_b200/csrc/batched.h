@@ -13,6 +13,19 @@
 namespace mq {
 namespace bs {
 
+// Tile choices of the plan's products (what the autotuner varies per bond-profile bucket).
+struct Tiles {
+  int stack_tn = 256;   // widest N tile of products whose A (a trial tensor) is shared: walkers are
+                        // stacked along N up to this width (64, 128 or 256; 64 with N = 64 means
+                        // one walker per tile)
+  int wide_tn = 256;    // widest N tile of the walker-by-walker products (64, 128 or 256)
+  int max_stages = 4;   // load-ring depth cap (2 .. 4; fewer when shared memory is short)
+  bool operator==(const Tiles &o) const {
+    return stack_tn == o.stack_tn && wide_tn == o.wide_tn && max_stages == o.max_stages;
+  }
+  bool operator!=(const Tiles &o) const { return !(*this == o); }
+};
+
 // What one walk needs (filled by the engine).  The population must share one bond profile bW.
 struct Problem {
   int L = 0, nC = 0, G = 0;
@@ -35,6 +48,7 @@ struct Problem {
   int *err = nullptr;
   int capacity = 0;                // walkers the batched buffers hold
   int passes = 3;                  // 3: FP32-accurate products, 1: TF32
+  Tiles tiles;
 };
 
 struct Plan;

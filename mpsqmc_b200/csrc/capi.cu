@@ -189,6 +189,8 @@ struct mpsqmc_ctx {
   mq::bs::Plan *bplan = nullptr;
   int bplan_passes = 0;
   int bcap = 0;
+  mq::bs::Tiles tc_tiles;     // tile choices for the next plan (options, autotuner)
+  mq::bs::Tiles bplan_tiles;  // those the current plan was built with
 };
 
 namespace {
@@ -1122,7 +1124,7 @@ static int ensure_batched(mpsqmc_ctx *c) {
       if (all[(size_t)slots[w] * (L + 1) + k] != c->bW[k])
         return fail(MPSQMC_E_UNSUPPORTED, "the tcgen05 sweep needs every walker in the slot layout's bond profile");
   const int passes = c->precision == MPSQMC_PRECISION_TF32_TC ? 1 : 3;
-  if (c->bplan && c->bplan_passes == passes) return 0;
+  if (c->bplan && c->bplan_passes == passes && c->bplan_tiles == c->tc_tiles) return 0;
   if (c->bplan) {
     mq::bs::destroy(c->bplan);
     c->bplan = nullptr;
@@ -1167,6 +1169,7 @@ static int ensure_batched(mpsqmc_ctx *c) {
   pr.grid = c->d_grid;
   pr.err = c->d_err;
   pr.passes = passes;
+  pr.tiles = c->tc_tiles;
   // buffers for the whole slot capacity when they fit in half the free memory, else for 1.5x the
   // target population (a step with more walkers then stops with MPSQMC_E_CAPACITY)
   size_t free_b = 0, total_b = 0;
@@ -1179,6 +1182,7 @@ static int ensure_batched(mpsqmc_ctx *c) {
   const int rc = mq::bs::build(pr, &c->bplan);
   if (rc) return rc;
   c->bplan_passes = passes;
+  c->bplan_tiles = pr.tiles;
   c->bcap = pr.capacity;
   drop_graphs(c);
   return 0;
@@ -1384,10 +1388,15 @@ int mpsqmc_walk(mpsqmc_ctx *c, int nsteps, mpsqmc_step_stats *stats) {
 }
 
 // Autotuning: choices measured once per problem shape (L, trial and walker bond dims, coupling
-// structure, projector) and remembered for every later context of the same shape in this process.
+// structure, projector, sweep family) and remembered for every later context of the same shape in
+// this process.
 namespace {
+struct Tuned {
+  int sweep, workspace;
+  mq::bs::Tiles tiles;
+};
 std::mutex g_tune_mutex;
-std::map<std::string, std::pair<int, int>> g_tuned;  // shape -> (sweep, workspace)
+std::map<std::string, Tuned> g_tuned;  // shape -> choice
 
 std::string tune_key(const mpsqmc_ctx *c) {
   std::ostringstream k;
@@ -1395,7 +1404,17 @@ std::string tune_key(const mpsqmc_ctx *c) {
   for (int v : c->aT) k << v << ',';
   k << '|';
   for (int v : c->bW) k << v << ',';
+  k << '|' << (tc_sweep(c) ? (c->precision == MPSQMC_PRECISION_TF32_TC ? "tc1" : "tc3") : "cta");
   return k.str();
+}
+
+int apply_tuned(mpsqmc_ctx *c, const Tuned &t) {
+  int rc = mpsqmc_set_option(c, MPSQMC_OPT_SWEEP, t.sweep);
+  if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_WORKSPACE, t.workspace);
+  if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_TC_STACK_TN, t.tiles.stack_tn);
+  if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_TC_WIDE_TN, t.tiles.wide_tn);
+  if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_TC_STAGES, t.tiles.max_stages);
+  return rc;
 }
 }  // namespace
 
@@ -1404,29 +1423,21 @@ int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspa
   if (c->n_cur < 1) return fail(MPSQMC_E_ARG, "no walkers");
   CK(cudaSetDevice(c->device));
   const std::string key = tune_key(c);
+  const bool tc = tc_sweep(c);
   {
     std::lock_guard<std::mutex> lk(g_tune_mutex);
     auto it = g_tuned.find(key);
     if (it != g_tuned.end()) {
-      int rc = mpsqmc_set_option(c, MPSQMC_OPT_SWEEP, it->second.first);
-      if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_WORKSPACE, it->second.second);
-      if (best_sweep) *best_sweep = it->second.first;
-      if (best_workspace) *best_workspace = it->second.second;
+      const int rc = apply_tuned(c, it->second);
+      if (best_sweep) *best_sweep = it->second.sweep;
+      if (best_workspace) *best_workspace = it->second.workspace;
       return rc;
     }
   }
-  // candidates: every sweep that takes these couplings, both work-buffer placements (one when the
-  // buffers do not fit on chip)
-  std::vector<std::pair<int, int>> cands;
-  const bool fits = sizeof(double) * (size_t)c->all_doubles <= c->smem_optin;
-  for (int sw : {MPSQMC_SWEEP_GENERAL, MPSQMC_SWEEP_NEAREST}) {
-    if (sw == MPSQMC_SWEEP_NEAREST && (!c->nn || c->projector != MPSQMC_PROJECTOR_TROTTER)) continue;
-    cands.push_back({sw, MPSQMC_WORKSPACE_AUTO});
-    if (fits) cands.push_back({sw, MPSQMC_WORKSPACE_GLOBAL});
-  }
-  // measure on the first k walkers (two waves of one CTA per SM), with the population state saved
-  // and restored around every trial
-  const int N = c->n_cur, k = std::min(N, 2 * c->sm_count), cap = c->capacity, L = c->L;
+  // measure on the first k walkers, with the population state saved and restored around every
+  // trial: two waves of one CTA per SM for the per-walker sweeps; for the tcgen05 sweep, whose
+  // tile counts grow with the population, up to 1024 walkers
+  const int N = c->n_cur, k = std::min(N, tc ? 1024 : 2 * c->sm_count), cap = c->capacity, L = c->L;
   std::vector<int> slots(N), h_free(cap), wd((size_t)cap * (L + 1));
   std::vector<long> wf((size_t)cap * L);
   std::vector<double> wt(cap), ov(cap), eh(cap);
@@ -1447,7 +1458,7 @@ int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspa
     CK(cudaMemcpyAsync(snap + (size_t)w * c->wstride, c->d_walkers + (size_t)slots[w] * c->wstride,
                        sizeof(double) * c->wstride, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  const int keep_sweep = c->sweep, keep_ws = c->global_work ? MPSQMC_WORKSPACE_GLOBAL : MPSQMC_WORKSPACE_AUTO;
+  const Tuned keep = {c->sweep, c->global_work ? MPSQMC_WORKSPACE_GLOBAL : MPSQMC_WORKSPACE_AUTO, c->tc_tiles};
   const int keep_nd = c->Ndesired, keep_step = c->step_count;
   const unsigned long long keep_draws = c->draws;
   const bool keep_trace = c->trace_on;
@@ -1477,21 +1488,49 @@ int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspa
   };
   c->trace_on = false;
   c->Ndesired = k;  // population control sized for the measured subset
-  double best = 1e300;
-  std::pair<int, int> choice = {keep_sweep, keep_ws};
-  int rc = 0;
-  for (const auto &cd : cands) {
-    rc = mpsqmc_set_option(c, MPSQMC_OPT_SWEEP, cd.first);
-    if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_WORKSPACE, cd.second);
+  // one trial: the candidate's options, a warm-up step (graph capture, plan rebuild), `steps`
+  // timed steps; returns the device time per walker-step
+  auto trial = [&](const Tuned &cd, double *per) -> int {
+    int rc = apply_tuned(c, cd);
     if (!rc) rc = restore(k);
-    if (!rc) rc = mpsqmc_walk(c, 1, nullptr);  // warm-up (graph capture)
+    if (!rc) rc = mpsqmc_walk(c, 1, nullptr);
     if (!rc) rc = restore(k);
     if (!rc) rc = mpsqmc_walk(c, steps, nullptr);
-    if (rc) break;
-    const double per = c->last_kernel_ms / ((double)k * steps);
-    if (per < best) {
-      best = per;
-      choice = cd;
+    if (!rc) *per = c->last_kernel_ms / ((double)k * steps);
+    return rc;
+  };
+  double best = 1e300;
+  Tuned choice = keep;
+  int rc = 0;
+  if (!tc) {
+    // every sweep that takes these couplings, both work-buffer placements (one when the buffers
+    // do not fit on chip)
+    const bool fits = sizeof(double) * (size_t)c->all_doubles <= c->smem_optin;
+    for (int sw : {MPSQMC_SWEEP_GENERAL, MPSQMC_SWEEP_NEAREST}) {
+      if (sw == MPSQMC_SWEEP_NEAREST && (!c->nn || c->projector != MPSQMC_PROJECTOR_TROTTER)) continue;
+      for (int ws : {MPSQMC_WORKSPACE_AUTO, MPSQMC_WORKSPACE_GLOBAL}) {
+        if (ws == MPSQMC_WORKSPACE_GLOBAL && !fits) continue;
+        const Tuned cd = {sw, ws, keep.tiles};
+        double per = 0.0;
+        if ((rc = trial(cd, &per))) break;
+        if (per < best) best = per, choice = cd;
+      }
+      if (rc) break;
+    }
+  } else {
+    // tcgen05 sweep: coordinate search over the tile choices, one at a time from the defaults
+    // (stacked tile width, then the walker products' tile width, then the ring depth)
+    Tuned cur = {keep.sweep, keep.workspace, mq::bs::Tiles()};
+    if (!(rc = trial(cur, &best))) choice = cur;
+    for (int axis = 0; axis < 3 && !rc; ++axis) {
+      const std::vector<int> vals = axis == 2 ? std::vector<int>{3, 2} : std::vector<int>{128, 64};
+      for (int v : vals) {
+        Tuned cd = choice;
+        (axis == 0 ? cd.tiles.stack_tn : axis == 1 ? cd.tiles.wide_tn : cd.tiles.max_stages) = v;
+        double per = 0.0;
+        if ((rc = trial(cd, &per))) break;
+        if (per < best) best = per, choice = cd;
+      }
     }
   }
   c->Ndesired = keep_nd;
@@ -1499,18 +1538,20 @@ int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspa
   const int rr = restore(N);
   c->gauge_dirty = keep_dirty;
   cudaFree(snap);
-  if (rc) return rc;
+  if (rc) {
+    apply_tuned(c, keep);
+    return rc;
+  }
   if (rr) return rr;
   drop_graphs(c);  // captured with the subset's population size
-  rc = mpsqmc_set_option(c, MPSQMC_OPT_SWEEP, choice.first);
-  if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_WORKSPACE, choice.second);
+  rc = apply_tuned(c, choice);
   if (rc) return rc;
   {
     std::lock_guard<std::mutex> lk(g_tune_mutex);
     g_tuned[key] = choice;
   }
-  if (best_sweep) *best_sweep = choice.first;
-  if (best_workspace) *best_workspace = choice.second;
+  if (best_sweep) *best_sweep = choice.sweep;
+  if (best_workspace) *best_workspace = choice.workspace;
   return 0;
 }
 
@@ -1635,6 +1676,15 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
       if (value < 0 || value > 1000) return fail(MPSQMC_E_ARG, "proposal mixture is 0..1000 thousandths");
       c->prop_mix = (int)value;
       break;
+    case MPSQMC_OPT_TC_STACK_TN:
+    case MPSQMC_OPT_TC_WIDE_TN:
+      if (value != 64 && value != 128 && value != 256) return fail(MPSQMC_E_ARG, "tile width is 64, 128 or 256");
+      (option == MPSQMC_OPT_TC_STACK_TN ? c->tc_tiles.stack_tn : c->tc_tiles.wide_tn) = (int)value;
+      break;
+    case MPSQMC_OPT_TC_STAGES:
+      if (value < 2 || value > 4) return fail(MPSQMC_E_ARG, "load-ring stages are 2..4");
+      c->tc_tiles.max_stages = (int)value;
+      break;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");
   }
@@ -1674,6 +1724,15 @@ int mpsqmc_get_option(mpsqmc_ctx *c, int option, long *value) {
       return 0;
     case MPSQMC_OPT_PROPOSAL_MIX:
       *value = c->prop_mix;
+      return 0;
+    case MPSQMC_OPT_TC_STACK_TN:
+      *value = c->tc_tiles.stack_tn;
+      return 0;
+    case MPSQMC_OPT_TC_WIDE_TN:
+      *value = c->tc_tiles.wide_tn;
+      return 0;
+    case MPSQMC_OPT_TC_STAGES:
+      *value = c->tc_tiles.max_stages;
       return 0;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");

@@ -45,6 +45,9 @@ enum Epilogue : int { kStore = 0, kDot4 = 1 };
 struct alignas(64) GemmParams {
   CUtensorMap tmA;   // 3D (k, row, z): FP32, box (32, tm, 1), SWIZZLE_128B
   CUtensorMap tmB;   // 3D (k, row, z): FP32, box (32, brows, bstack), SWIZZLE_128B
+  CUtensorMap tmD;   // dtma: D as 3D (m, n, z) with m contiguous, box (rows per epilogue warp, 16, 1)
+  int dtma;          // 1: column-major D (dm = 1), no accumulation: the epilogue writes through
+                     // shared memory and TMA bulk tensor stores
   int M, N, K;       // per batch entry
   int tm, tn;        // MMA M (64 or 128) and tile N (multiple of 16, <= 256)
   int adiv, bdiv;    // operand batch coordinate = z / div; 0: shared (coordinate 0)
@@ -133,6 +136,19 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
       ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
       : "memory");
 }
+
+// Bulk tensor store of one shared-memory box to D at (x, y, z) (x: the contiguous coordinate;
+// a multiple of 4 elements and never negative); completion tracked by the issuing thread's bulk
+// groups.
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void *src, int x, int y, int z) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];"
+               ::"l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// wait until at most one committed group of this thread still reads shared memory
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -303,11 +319,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       int s = 0;
       uint32_t ph = 0;
       int acc = 0;
-      uint32_t aph[4] = {0, 0, 0, 0};
+      uint32_t aph = 0;  // phase bit per accumulator (a register, not an indexed array)
       const uint32_t idesc = instr_desc(p.tm, p.tn);
       bool ok = true;
       for (int tile = blockIdx.x; tile < t.total && ok; tile += gridDim.x) {
-        if (!mbar_wait(&bar_tempty[acc], aph[acc] ^ 1, &abort_flag, p.err)) break;
+        if (!mbar_wait(&bar_tempty[acc], ((aph >> acc) & 1u) ^ 1u, &abort_flag, p.err)) break;
         tc_fence_after();
         const uint32_t dt = tmem + (uint32_t)(acc * p.tn);
         for (int kc = 0; kc < nk; ++kc) {
@@ -337,7 +353,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         }
         if (!ok) break;
         mma_commit(&bar_tfull[acc]);
-        aph[acc] ^= 1;
+        aph ^= 1u << acc;
         acc = (acc + 1 == nacc) ? 0 : acc + 1;
       }
     }
@@ -404,7 +420,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     const bool chunk_uniform = bstack == 1 || (N & 15) == 0;
     const int q = warp & 3;  // TMEM lane quarter of this warp
     float *stg = stagebuf + (warp - 8) * 32 * 33;
-    const bool staged = !dot4 && dn == 1 && dm != 1;  // row-major output: transpose first
+    const bool dtma = p.dtma != 0;
+    const bool staged = !dtma && !dot4 && dn == 1 && dm != 1;  // row-major output: transpose first
+    // dtma: two 32 x 16 boxes per warp (column-major: 16 columns of nrow contiguous rows), used in
+    // turn, so that filling one overlaps the bulk store of the other
+    float *dbox = stagebuf + (warp - 8) * 1024;
+    int nbox = 0;
     const int nrow = (tm == 128) ? 32 : 16;            // accumulator rows this warp holds (lanes 0 .. nrow-1)
     // tile column j -> batch entry z (-1: past the stacked box, stale shared memory) and row n of B
     auto col = [&](int j, int z0, int n0, int &z, int &n) {
@@ -416,28 +437,45 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         n = n0 + j;
       }
     };
-    // closures: the warp's four partial sums of entry z (one atomic per sum)
-    auto flush = [&](int z, double *ds) {
-#pragma unroll
-      for (int qq = 0; qq < 4; ++qq) {
-        double v = ds[qq];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) atomicAdd(dot + (long)z * dstride + doff + qq, v);
-        ds[qq] = 0.0;
+    // closures: the lane's four partial sums (scalars, so that they stay in registers) and their
+    // warp sum into entry z (one atomic per sum)
+    double ds0 = 0.0, ds1 = 0.0, ds2 = 0.0, ds3 = 0.0;
+    auto flush = [&](int z) {
+      for (int o = 16; o > 0; o >>= 1) {
+        ds0 += __shfl_xor_sync(0xffffffffu, ds0, o);
+        ds1 += __shfl_xor_sync(0xffffffffu, ds1, o);
+        ds2 += __shfl_xor_sync(0xffffffffu, ds2, o);
+        ds3 += __shfl_xor_sync(0xffffffffu, ds3, o);
       }
+      if (lane == 0) {
+        double *d = dot + (long)z * dstride + doff;
+        atomicAdd(d, ds0);
+        atomicAdd(d + 1, ds1);
+        atomicAdd(d + 2, ds2);
+        atomicAdd(d + 3, ds3);
+      }
+      ds0 = ds1 = ds2 = ds3 = 0.0;
     };
+    auto accum = [&](double x, const float *e) {
+      ds0 += x * (double)e[0];
+      ds1 += x * (double)e[eq];
+      ds2 += x * (double)e[2 * eq];
+      ds3 += x * (double)e[3 * eq];
+    };
+    // E rows read as 16-byte vectors when they are contiguous and aligned (chunks start at
+    // columns that are multiples of 16)
+    const bool e_vec = dot4 && en == 1 && ((ez | eq | em) & 3) == 0 && (reinterpret_cast<uintptr_t>(E) & 15) == 0;
     int acc = 0;
-    uint32_t aph[4] = {0, 0, 0, 0};
+    uint32_t aph = 0;
     for (int tile = blockIdx.x; tile < t.total; tile += gridDim.x) {
       int m0, z0, n0;
       tile_coords(p, t, tile, m0, z0, n0);
-      if (!mbar_wait(&bar_tfull[acc], aph[acc], &abort_flag, p.err)) break;
+      if (!mbar_wait(&bar_tfull[acc], (aph >> acc) & 1u, &abort_flag, p.err)) break;
       __syncwarp();
       tc_fence_after();
       const int mq0 = m0 + (tm == 128 ? 32 * q : 16 * q);  // first row of this warp
       const int m = mq0 + lane;
       const bool mrow = lane < nrow && m < M;
-      double dsum[4] = {0.0, 0.0, 0.0, 0.0};
       int zlast = -1;
       for (int c0 = 0; c0 < tn; c0 += 16) {
         float v[16];
@@ -449,6 +487,24 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         if (chunk_uniform) {
           // all 16 columns belong to entry z, rows n .. n + nv - 1 of B: one base pointer per chunk
           const int nv = min(16, N - n);
+          if (dtma) {
+            // rows past M and columns past N are clipped by the tensor map's extents
+            float *bx = dbox + (nbox & 1) * 512;
+            if (lane == 0) bulk_wait_read1();  // the store issued two boxes ago has read bx
+            __syncwarp();
+            if (lane < nrow) {
+#pragma unroll
+              for (int i = 0; i < 16; ++i) bx[i * nrow + lane] = alpha * v[i];
+            }
+            fence_proxy_async();
+            __syncwarp();
+            if (lane == 0) {
+              tma_store_3d(&p.tmD, bx, mq0, n, z);
+              bulk_commit();
+            }
+            ++nbox;
+            continue;
+          }
           if (staged) {
             // this lane's row segment into shared memory, then lanes take the columns: each
             // store instruction writes 16 consecutive elements of each of two rows (coalesced)
@@ -477,18 +533,29 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             }
           } else {
             if (z != zlast) {
-              if (zlast >= 0) flush(zlast, dsum);
+              if (zlast >= 0) flush(zlast);
               zlast = z;
             }
             if (mrow) {
               const float *e = E + (long)z * ez + (long)m * em + (long)n * en;
+              if (e_vec && nv == 16) {
 #pragma unroll
-              for (int i = 0; i < 16; ++i)
-                if (i < nv) {
-                  const double x = (double)(alpha * v[i]);
+                for (int i4 = 0; i4 < 4; ++i4) {
+                  float4 ev[4];
 #pragma unroll
-                  for (int qq = 0; qq < 4; ++qq) dsum[qq] += x * (double)e[i * en + qq * eq];
+                  for (int qq = 0; qq < 4; ++qq) ev[qq] = __ldg(reinterpret_cast<const float4 *>(e + qq * eq) + i4);
+                  const double x0 = (double)(alpha * v[4 * i4]), x1 = (double)(alpha * v[4 * i4 + 1]),
+                               x2 = (double)(alpha * v[4 * i4 + 2]), x3 = (double)(alpha * v[4 * i4 + 3]);
+                  ds0 += x0 * (double)ev[0].x + x1 * (double)ev[0].y + x2 * (double)ev[0].z + x3 * (double)ev[0].w;
+                  ds1 += x0 * (double)ev[1].x + x1 * (double)ev[1].y + x2 * (double)ev[1].z + x3 * (double)ev[1].w;
+                  ds2 += x0 * (double)ev[2].x + x1 * (double)ev[2].y + x2 * (double)ev[2].z + x3 * (double)ev[2].w;
+                  ds3 += x0 * (double)ev[3].x + x1 * (double)ev[3].y + x2 * (double)ev[3].z + x3 * (double)ev[3].w;
                 }
+              } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                  if (i < nv) accum((double)(alpha * v[i]), e + i * en);
+              }
             }
           }
           continue;
@@ -532,25 +599,22 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             col(c0 + i, z0, n0, zi, ni);
             if (zi < 0 || zi >= Zt || ni >= N) continue;
             if (zi != zlast) {
-              if (zlast >= 0) flush(zlast, dsum);
+              if (zlast >= 0) flush(zlast);
               zlast = zi;
             }
-            if (mrow) {
-              const float x = alpha * v[i];
-              const float *e = E + (long)zi * ez + (long)m * em + (long)ni * en;
-#pragma unroll
-              for (int qq = 0; qq < 4; ++qq) dsum[qq] += (double)x * (double)e[qq * eq];
-            }
+            if (mrow) accum((double)(alpha * v[i]), E + (long)zi * ez + (long)m * em + (long)ni * en);
           }
         }
       }
-      if (dot4 && zlast >= 0) flush(zlast, dsum);
+      if (dot4 && zlast >= 0) flush(zlast);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&bar_tempty[acc]);
-      aph[acc] ^= 1;
+      aph ^= 1u << acc;
       acc = (acc + 1 == nacc) ? 0 : acc + 1;
     }
+    // the bulk stores this warp issued have completed (they read its boxes until then)
+    if (dtma && lane == 0) bulk_wait_all();
   }
 
   // ---------------- teardown ----------------
