@@ -80,6 +80,11 @@ def parse():
                     help="N>1: one walk split over the ranks (global population control and walker "
                          "balancing, mpsqmc_b200.population; NCCL, records in device buffers) instead of N "
                          "independent replicas")
+    ap.add_argument("--gain-steps", type=int, default=3, metavar="STEPS",
+                    help="untimed grid steps after the timed ones that measure the proposal gain bound")
+    ap.add_argument("--tiles", default="autotune", choices=["autotune", "default"],
+                    help="tcgen05 sweep: tile choices picked by mpsqmc_autotune for this bond profile (untimed "
+                         "set-up, remembered for the process) or the built-in defaults")
     ap.add_argument("--vn-arms", default="tf32x3/grid,tf32x3/learned",
                     help="precision/proposal variants compared with the plain FP64 grid walk")
     a = ap.parse_args()
@@ -402,12 +407,20 @@ def main():
         configure(e, a, sweep, plain=(precision == "fp64"))
         e.set_rng(seed, 0)
         use_proposal(e, params)
+        if precision.endswith("_tc") and args.tiles == "autotune":
+            e.autotune(steps=1)  # restores population, random stream and step count
         e.walk(warmup)
         torch.cuda.synchronize()
         return e, a
 
     params, training = train_proposal(make, args, sweep, seed)
     eng, _ = timed_arm(args.precision, args.steps, args.warmup, args.proposal, params)
+    if args.precision.endswith("_tc"):
+        from mpsqmc_b200.capi import OPT_TC_SPLIT_OUT, OPT_TC_STACK_TN, OPT_TC_STAGES, OPT_TC_WIDE_TN
+        cfg["tiles"] = {"split_out": eng.get_option(OPT_TC_SPLIT_OUT), "stack_tn": eng.get_option(OPT_TC_STACK_TN),
+                        "wide_tn": eng.get_option(OPT_TC_WIDE_TN), "max_stages": eng.get_option(OPT_TC_STAGES),
+                        "chosen_by": ("mpsqmc_autotune: coordinate search over the tile choices on up to 1024 "
+                                      "walkers of this bond profile" if args.tiles == "autotune" else "defaults")}
     if pg is not None:
         pg.barrier()
     rw = None
@@ -449,6 +462,20 @@ def main():
     passes = 1 if args.precision in ("tf32", "tf32_tc") else 3
     E_last = {"E_P_last": stats[-1]["E_P"], "E_T_last": stats[-1]["E_T"], "walkers_last": stats[-1]["n_after"],
               "E_P_mean": float(np.mean([s["E_P"] for s in stats]))}
+
+    # what any auxiliary-field proposal could gain over the grid PDF on this walk (untimed steps
+    # after the timed ones): N sum w^2 / (sum w)^2 of the propagated weights
+    gain = None
+    if args.gain_steps > 0 and rw is None and args.proposal == "grid" and not (args.vn or args.vn_compare):
+        from mpsqmc_b200 import analysis
+        ws_g = []
+        for _ in range(args.gain_steps):
+            eng.walk(1)
+            ws_g.append(eng.last_step_walkers()["weight"])
+        gain = {"value": analysis.proposal_gain_bound(ws_g), "steps": args.gain_steps,
+                "definition": "mean over steps of N sum w^2 / (sum w)^2 of the walkers' weights after "
+                              "propagation: the largest factor by which any proposal (learned or look-ahead) "
+                              "could lower the variance of the weighted mean energy"}
 
     vn = None
     vn_steps = max(args.vn, args.vn_compare or 0)
@@ -585,6 +612,7 @@ def main():
             **({"fp64_arm": fp64_arm} if fp64_arm is not None else {}),
             **({"variance_normalised": vn} if vn is not None else {}),
             **({"proposal_training": training} if training else {}),
+            **({"proposal_gain_bound": gain} if gain is not None else {}),
             "clocks": clk.summary(),
         }
         print(json.dumps(line))

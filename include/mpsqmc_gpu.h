@@ -251,6 +251,10 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
                                       *   products */
 #define MPSQMC_OPT_TC_STAGES 13       /*   load-ring depth cap, 2..4 (fewer when shared memory is
                                       *   short) */
+#define MPSQMC_OPT_TC_SPLIT_OUT 14    /*   0 (default) / 1: with three passes, the walker-side right
+                                      *   factors of the trial products are written as TF32 head
+                                      *   and tail arrays and loaded split (the trial itself always
+                                      *   is), instead of being split in shared memory */
 int mpsqmc_set_option(mpsqmc_ctx *ctx, int option, long value);
 int mpsqmc_get_option(mpsqmc_ctx *ctx, int option, long *value);
 
@@ -297,8 +301,8 @@ int mpsqmc_proposal_stats(mpsqmc_ctx *ctx, double *last_loss, int *updates);
  * (MPSQMC_OPT_SWEEP, MPSQMC_OPT_WORKSPACE) choice on the first walkers of the current population
  * (two waves of one CTA per SM), restores the population, random stream and step count after
  * each trial, and keeps the fastest.  Under the tcgen05 sweep (MPSQMC_PRECISION_TF32X3_TC,
- * TF32_TC) it instead tunes that sweep's tile choices (MPSQMC_OPT_TC_STACK_TN, _WIDE_TN, _STAGES)
- * by a coordinate search from the defaults, each timed on up to 1024 walkers (its tile counts
+ * TF32_TC) it instead tunes that sweep's choices (MPSQMC_OPT_TC_SPLIT_OUT, _STACK_TN, _WIDE_TN,
+ * _STAGES) by a coordinate search from the defaults, each timed on up to 1024 walkers (its tile counts
  * grow with the population).  The choice is remembered per problem shape (L, trial and walker
  * bond dims, couplings, projector, sweep family) for later contexts of this process, which then
  * skip the measurement.  best_* (may be NULL) receive the chosen sweep and workspace values. */

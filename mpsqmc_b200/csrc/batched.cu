@@ -116,8 +116,8 @@ int pick_stages(GemmParams &p, int max_stages = kMaxStages) {
   int sms = 0, limit = 0;
   const int rc = configure_kernel(&sms, &limit);
   if (rc) return rc;
-  p.stages = std::max(2, std::min(max_stages, stages_for(p.tm, p.tn, p.passes, limit)));
-  if (smem_bytes(p.tm, p.tn, p.passes, p.stages) > limit)
+  p.stages = std::max(2, std::min(max_stages, stages_for(p.tm, p.tn, p.passes, limit, p.dsplit)));
+  if (smem_bytes(p.tm, p.tn, p.passes, p.stages, p.dsplit) > limit)
     return fail(MPSQMC_E_UNSUPPORTED, "tcgen05 GEMM tile does not fit in shared memory");
   return 0;
 }
@@ -128,7 +128,7 @@ int launch(const GemmParams &p, long max_tiles, cudaStream_t stream) {
   int rc = configure_kernel(&sms, nullptr);
   if (rc) return rc;
   const int grid = (int)std::max(1L, std::min((long)sms, max_tiles));
-  tc_gemm_kernel<<<grid, kThreads, smem_bytes(p.tm, p.tn, p.passes, p.stages), stream>>>(p);
+  tc_gemm_kernel<<<grid, kThreads, smem_bytes(p.tm, p.tn, p.passes, p.stages, p.dsplit), stream>>>(p);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(MPSQMC_E_CUDA, std::string("tcgen05 GEMM launch: ") + cudaGetErrorString(e));
   return 0;
@@ -211,6 +211,18 @@ constexpr int kErrNumeric = 1, kErrCapacity = 2;
 inline long pad4(long x) { return (x + 3) & ~3L; }
 inline long pad64(long x) { return (x + 63) & ~63L; }
 inline int tm_for(int M) { return M <= 64 ? 64 : 128; }
+
+// x rounded to the nearest TF32 value, ties away from zero (the device's cvt.rna.tf32.f32): the
+// 13 low mantissa bits are rounded off the magnitude
+inline float tf32_round(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return x;
+  u = (u + 0x1000u) & ~0x1fffu;
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
 
 // ---------------------------------------------------------------------------------------------
 // Small kernels (FP64 bookkeeping and elementwise steps).  w: logical walker index; every kernel
@@ -590,6 +602,11 @@ struct Plan {
   float *Fdn_ptr(int fd) { return Fd[1 - fd]; }
   float *Lenv = nullptr, *P = nullptr, *X = nullptr, *X4 = nullptr, *Y = nullptr, *Nl[2] = {nullptr, nullptr},
         *Wn = nullptr, *Fd[2] = {nullptr, nullptr}, *Gb = nullptr, *Q = nullptr, *Fch = nullptr, *Xch = nullptr;
+  // three passes: the trial copies hold [values | TF32 heads | TF32 tails] (sections of nto,
+  // ntt, ntos, ntts floats), and the right factors of the trial products (X, X4, Y, Q, Xch) are
+  // written as heads, with their tails in these arrays
+  long nto = 0, ntt = 0, ntos = 0, ntts = 0;
+  float *Xl = nullptr, *X4l = nullptr, *Yl = nullptr, *Ql = nullptr, *Xchl = nullptr;
   double *ovb = nullptr, *wtb = nullptr, *scl = nullptr, *ob = nullptr, *dot = nullptr;
   int *nb = nullptr;               // min(n_cur, cap), written at the step start: the products' walker count
   SiteForms sf;
@@ -622,12 +639,15 @@ struct Opnd {
   const float *base;
   long ld, rows, zs, zn;  // row stride, rows, z stride, z count (allocated)
   int div;                // z -> operand index divisor (0: shared)
+  const float *hi = nullptr, *lo = nullptr;  // the same operand as TF32 head and tail arrays
 };
 
 // One batched product over zper * n_cur batch entries (per walker: zper consecutive entries).
+// With three passes, operands that carry head and tail arrays are loaded split (both must), and
+// Dlo asks for D as head (D) and tail (Dlo) arrays.
 int add_gemm(Plan *p, const Opnd &A, const Opnd &B, int M, int N, int K, int zper, float *D, long dz, long dm, long dn,
              int beta, float alpha = 1.f, const float *E = nullptr, long ez = 0, long eq = 0, long em = 0, long en = 0,
-             int doff = 0) {
+             int doff = 0, float *Dlo = nullptr) {
   if (M < 1 || N < 1 || K < 1) return 0;
   GemmParams g;
   std::memset(&g, 0, sizeof g);
@@ -669,11 +689,24 @@ int add_gemm(Plan *p, const Opnd &A, const Opnd &B, int M, int N, int K, int zpe
     g.dstride = 16;
     g.doff = doff;
   }
-  int rc = pick_stages(g, t.max_stages);
   pick_store(g, (long)zper * p->cap);
-  if (!rc) rc = make_operand_map(&g.tmA, A.base, K, A.rows, std::max(1L, A.zn), A.ld, A.zs, g.tm, 1);
-  if (!rc) rc = make_operand_map(&g.tmB, B.base, K, bstack > 1 ? N : B.rows, std::max(1L, B.zn), B.ld, B.zs, g.brows,
-                                 bstack);
+  const bool three = p->pr.passes == 3;
+  if (three && Dlo) {
+    // the consumer loads this output split: only the TMA store route writes the two arrays
+    if (!g.dtma || !make_store_map(&g.tmD2, Dlo, M, N, (long)zper * p->cap, dn, dz, g.tm == 128 ? 32 : 16))
+      return fail(MPSQMC_E_UNSUPPORTED, "batched sweep: a split output needs the TMA store route");
+    g.dsplit = 1;
+  }
+  g.presplit = three ? ((A.lo ? 1 : 0) | (B.lo ? 2 : 0)) : 0;
+  const float *ah = (g.presplit & 1) ? A.hi : A.base, *bh = (g.presplit & 2) ? B.hi : B.base;
+  const long brows_map = bstack > 1 ? N : B.rows;
+  int rc = pick_stages(g, t.max_stages);
+  if (!rc) rc = make_operand_map(&g.tmA, ah, K, A.rows, std::max(1L, A.zn), A.ld, A.zs, g.tm, 1);
+  if (!rc) rc = make_operand_map(&g.tmB, bh, K, brows_map, std::max(1L, B.zn), B.ld, B.zs, g.brows, bstack);
+  if (!rc && (g.presplit & 1))
+    rc = make_operand_map(&g.tmA2, A.lo, K, A.rows, std::max(1L, A.zn), A.ld, A.zs, g.tm, 1);
+  if (!rc && (g.presplit & 2))
+    rc = make_operand_map(&g.tmB2, B.lo, K, brows_map, std::max(1L, B.zn), B.ld, B.zs, g.brows, bstack);
   if (rc) return rc;
   const long zt = (long)zper * p->cap;
   const long mt = (M + g.tm - 1) / g.tm;
@@ -703,6 +736,8 @@ size_t bytes_needed(const Problem &pr) {
   const long szBl = pad64(maxA * ldB), szX = pad64(2 * maxB * ldA), szN = pad64(maxB * ldB), szW = pad64(2 * maxB * ldB);
   const int ns = std::max(1, pr.nslots);
   per += szBl * (1 + 4 + 2 + 2 + 3L * ns) + szX * (1 + 4 + 1 + 3L * ns) + 2 * szN + szW + pad64(2 * maxB * ldA);
+  if (pr.passes == 3 && pr.tiles.split_out)
+    per += szX * (1 + 4 + 1 + 3L * ns) + pad64(2 * maxB * ldA);  // tails of the right factors
   return (size_t)per * pr.capacity * sizeof(float) + (size_t)pr.capacity * 48 * sizeof(double);
 }
 
@@ -731,6 +766,8 @@ int build(const Problem &pr, Plan **out) {
   const long cap = p->cap;
   const int ns = std::max(1, pr.nslots);
   // ---- trial copies (FP32), K-major for both product directions
+  const bool split = pr.passes == 3;  // also the TF32 head and tail of each copy
+  const int nsec = split ? 3 : 1;
   p->to_off.resize(2 * L);
   p->tt_off.resize(2 * L);
   long nto = 0, ntt = 0;
@@ -750,7 +787,12 @@ int build(const Problem &pr, Plan **out) {
     p->tts_off[k] = ntts;
     ntts += pad64((long)a[k] * 2 * p->ldA);
   }
-  int rc = palloc(p, &p->TO, nto) | palloc(p, &p->TT, ntt) | palloc(p, &p->TOs, ntos) | palloc(p, &p->TTs, ntts);
+  p->nto = nto;
+  p->ntt = ntt;
+  p->ntos = ntos;
+  p->ntts = ntts;
+  int rc = palloc(p, &p->TO, nsec * nto) | palloc(p, &p->TT, nsec * ntt) | palloc(p, &p->TOs, nsec * ntos) |
+           palloc(p, &p->TTs, nsec * ntts);
   if (rc) return bail(MPSQMC_E_CUDA);
   {
     std::vector<double> tr;
@@ -773,10 +815,25 @@ int build(const Problem &pr, Plan **out) {
             tts[p->tts_off[k] + (long)r * l2 + s * p->ldA + c] = x;
           }
       }
-    if (cudaMemcpy(p->TO, to.data(), sizeof(float) * nto, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(p->TT, tt.data(), sizeof(float) * ntt, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(p->TOs, tos.data(), sizeof(float) * ntos, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(p->TTs, tts.data(), sizeof(float) * ntts, cudaMemcpyHostToDevice) != cudaSuccess)
+    // sections: values, then (three passes) heads x rounded to TF32 and tails (x - head) rounded
+    auto sections = [&](std::vector<float> &v) {
+      const size_t n = v.size();
+      if (!split) return;
+      v.resize(3 * n);
+      for (size_t i = 0; i < n; ++i) {
+        const float h = tf32_round(v[i]);
+        v[n + i] = h;
+        v[2 * n + i] = tf32_round(v[i] - h);
+      }
+    };
+    sections(to);
+    sections(tt);
+    sections(tos);
+    sections(tts);
+    if (cudaMemcpy(p->TO, to.data(), sizeof(float) * to.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->TT, tt.data(), sizeof(float) * tt.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->TOs, tos.data(), sizeof(float) * tos.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->TTs, tts.data(), sizeof(float) * tts.size(), cudaMemcpyHostToDevice) != cudaSuccess)
       return bail(fail(MPSQMC_E_CUDA, "batched sweep: trial upload failed"));
   }
   // ---- walker forms and right environments (site k: per walker sizes, arrays of cap walkers)
@@ -813,6 +870,10 @@ int build(const Problem &pr, Plan **out) {
         palloc(p, &p->Fd[1], p->szBl * cap) | palloc(p, &p->Gb, 2 * p->szBl * cap) |
         palloc(p, &p->Q, pad64(2 * maxB * p->ldA) * cap) | palloc(p, &p->Fch, 3L * ns * p->szBl * cap) |
         palloc(p, &p->Xch, 3L * ns * p->szX * cap);
+  const bool split_b = split && pr.tiles.split_out;  // right factors written split
+  if (split_b)
+    rc |= palloc(p, &p->Xl, p->szX * cap) | palloc(p, &p->X4l, 4 * p->szX * cap) | palloc(p, &p->Yl, p->szX * cap) |
+          palloc(p, &p->Ql, pad64(2 * maxB * p->ldA) * cap) | palloc(p, &p->Xchl, 3L * ns * p->szX * cap);
   rc |= palloc(p, &p->ovb, cap) | palloc(p, &p->wtb, cap) | palloc(p, &p->scl, cap) | palloc(p, &p->ob, 8 * cap) |
         palloc(p, &p->dot, 16 * cap) | palloc(p, &p->err_tc, 1) | palloc(p, &p->nb, 1);
   if (rc) return bail(MPSQMC_E_CUDA);
@@ -852,21 +913,35 @@ int build(const Problem &pr, Plan **out) {
   auto SLo = [P](int k) { return Opnd{P->SL + P->sl_off[k], P->sl_ld[k], 2L * P->pr.bW[k + 1], P->sl_sz[k], P->cap, 1}; };
   auto SRo = [P](int k) { return Opnd{P->SR + P->sr_off[k], P->sr_ld[k], 2L * P->pr.bW[k], P->sr_sz[k], P->cap, 1}; };
   auto Ro = [P](int k) { return Opnd{P->R + P->r_off[k], P->r_ld[k], P->pr.aT[k], P->r_sz[k], P->cap, 1}; };
-  auto TOo = [P](int k, int s) {
-    return Opnd{P->TO + P->to_off[2 * k + s], pad4(P->pr.aT[k]), P->pr.aT[k + 1], 0, 1, 0};
+  // a trial copy, with its head and tail sections when they exist
+  auto Tr = [P, split](const float *arr, long n, long off, long ld, long rows) {
+    Opnd o{arr + off, ld, rows, 0, 1, 0};
+    if (split) {
+      o.hi = arr + n + off;
+      o.lo = arr + 2 * n + off;
+    }
+    return o;
   };
-  auto TTo = [P](int k, int s) {
-    return Opnd{P->TT + P->tt_off[2 * k + s], pad4(P->pr.aT[k + 1]), P->pr.aT[k], 0, 1, 0};
+  auto TOo = [P, Tr](int k, int s) { return Tr(P->TO, P->nto, P->to_off[2 * k + s], pad4(P->pr.aT[k]), P->pr.aT[k + 1]); };
+  auto TTo = [P, Tr](int k, int s) { return Tr(P->TT, P->ntt, P->tt_off[2 * k + s], pad4(P->pr.aT[k + 1]), P->pr.aT[k]); };
+  auto TOso = [P, Tr](int k) { return Tr(P->TOs, P->ntos, P->tos_off[k], 2 * P->ldA, P->pr.aT[k + 1]); };
+  auto TTso = [P, Tr](int k) { return Tr(P->TTs, P->ntts, P->tts_off[k], 2 * P->ldA, P->pr.aT[k]); };
+  // a right factor written as heads (base) with its tails at the same offset of `tails`
+  auto Sp = [split_b](Opnd o, const float *heads, const float *tails) {
+    if (split_b) {
+      o.hi = o.base;
+      o.lo = tails + (o.base - heads);
+    }
+    return o;
   };
-  auto TOso = [P](int k) { return Opnd{P->TOs + P->tos_off[k], 2 * P->ldA, P->pr.aT[k + 1], 0, 1, 0}; };
-  auto TTso = [P](int k) { return Opnd{P->TTs + P->tts_off[k], 2 * P->ldA, P->pr.aT[k], 0, 1, 0}; };
   const long l2 = 2 * p->ldA;  // K of the sigma-stacked trial products
   // right environment R_k from R_{k+1}: Y = R_{k+1} SR_k^T (rows (r, s)), then
   // R_k = sum_s TT_k[s] Y_s as one product with s stacked along K
   auto right_env = [&](int k) -> int {
-    int r = add_gemm(p, Ro(k + 1), SRo(k), a[k + 1], 2 * b[k], b[k + 1], 1, p->Y, p->szX, 1, p->ldA, 0);
+    int r = add_gemm(p, Ro(k + 1), SRo(k), a[k + 1], 2 * b[k], b[k + 1], 1, p->Y, p->szX, 1, p->ldA, 0, 1.f, nullptr, 0,
+                     0, 0, 0, 0, p->Yl);
     if (!r) {
-      Opnd Yr{p->Y, l2, b[k], p->szX, cap, 1};
+      const Opnd Yr = Sp(Opnd{p->Y, l2, b[k], p->szX, cap, 1}, p->Y, p->Yl);
       r = add_gemm(p, TTso(k), Yr, a[k], b[k], (int)l2, 1, p->R + p->r_off[k], p->r_sz[k], p->r_ld[k], 1, 0);
     }
     return r;
@@ -874,10 +949,11 @@ int build(const Problem &pr, Plan **out) {
   // left branches at cut i+1: X = Lenv SL_i (rows (t, c)), P[s + 2t] = TO_i[s] X_t
   auto left_branches = [&](int i) -> int {
     Opnd Le{p->Lenv, p->ldB, a[i], p->szBl, cap, 1};
-    int r = add_gemm(p, Le, SLo(i), a[i], 2 * b[i + 1], b[i], 1, p->X, p->szX, 1, p->ldA, 0);
+    int r = add_gemm(p, Le, SLo(i), a[i], 2 * b[i + 1], b[i], 1, p->X, p->szX, 1, p->ldA, 0, 1.f, nullptr, 0, 0, 0, 0,
+                     0, p->Xl);
     for (int s = 0; s < 2 && !r; ++s)
       for (int t = 0; t < 2 && !r; ++t) {
-        Opnd Xb{p->X + (long)t * p->ldA, l2, b[i + 1], p->szX, cap, 1};
+        const Opnd Xb = Sp(Opnd{p->X + (long)t * p->ldA, l2, b[i + 1], p->szX, cap, 1}, p->X, p->Xl);
         r = add_gemm(p, TOo(i, s), Xb, a[i + 1], b[i + 1], a[i], 1, p->P + (long)(s + 2 * t) * p->szBl, 4 * p->szBl,
                      p->ldB, 1, 0);
       }
@@ -888,9 +964,10 @@ int build(const Problem &pr, Plan **out) {
     Opnd Pq{p->P, p->ldB, a[m], p->szBl, 4L * cap, 1};
     Opnd S = SLo(m);
     S.div = 4;
-    int r = add_gemm(p, Pq, S, a[m], 2 * b[m + 1], b[m], 4, p->X4, p->szX, 1, p->ldA, 0);
+    int r = add_gemm(p, Pq, S, a[m], 2 * b[m + 1], b[m], 4, p->X4, p->szX, 1, p->ldA, 0, 1.f, nullptr, 0, 0, 0, 0, 0,
+                     p->X4l);
     if (!r) {
-      Opnd Xr{p->X4, l2, b[m + 1], p->szX, 4L * cap, 1};
+      const Opnd Xr = Sp(Opnd{p->X4, l2, b[m + 1], p->szX, 4L * cap, 1}, p->X4, p->X4l);
       r = add_gemm(p, TOso(m), Xr, a[m + 1], b[m + 1], (int)l2, 4, p->P, p->szBl, p->ldB, 1, 0);
     }
     return r;
@@ -902,10 +979,11 @@ int build(const Problem &pr, Plan **out) {
     p->ops.push_back([dd, dbytes](cudaStream_t s, double *) {
       return cudaMemsetAsync(dd, 0, dbytes, s) == cudaSuccess ? 0 : fail(MPSQMC_E_CUDA, "memset");
     });
-    int r = add_gemm(p, Ro(j + 1), SRo(j), a[j + 1], 2 * b[j], b[j + 1], 1, p->Y, p->szX, 1, p->ldA, 0);
+    int r = add_gemm(p, Ro(j + 1), SRo(j), a[j + 1], 2 * b[j], b[j + 1], 1, p->Y, p->szX, 1, p->ldA, 0, 1.f, nullptr, 0,
+                     0, 0, 0, 0, p->Yl);
     for (int s = 0; s < 2 && !r; ++s)
       for (int t = 0; t < 2 && !r; ++t) {
-        Opnd Yb{p->Y + (long)t * p->ldA, l2, b[j], p->szX, cap, 1};
+        const Opnd Yb = Sp(Opnd{p->Y + (long)t * p->ldA, l2, b[j], p->szX, cap, 1}, p->Y, p->Yl);
         r = add_gemm(p, TTo(j, s), Yb, a[j], b[j], a[j + 1], 1, p->X, 0, 0, 0, 0, 1.f, p->P, 4 * p->szBl, p->szBl,
                      p->ldB, 1, 4 * (s + 2 * t));
       }
@@ -1045,10 +1123,11 @@ int build(const Problem &pr, Plan **out) {
           p->launches += 1;
           Opnd Gr{p->Gb, 2 * ldl, ai, 2 * p->szBl, cap, 1};
           Opnd Cr{p->SL + p->sl_off[i], 2 * ldl, bi1, p->sl_sz[i], cap, 1};
-          rc = add_gemm(p, Gr, Cr, ai, bi1, (int)(2 * ldl), 1, p->Q + (long)s * p->ldA, szQ, 1, l2, 0);
+          rc = add_gemm(p, Gr, Cr, ai, bi1, (int)(2 * ldl), 1, p->Q + (long)s * p->ldA, szQ, 1, l2, 0, 1.f, nullptr, 0,
+                        0, 0, 0, 0, p->Ql ? p->Ql + (long)s * p->ldA : nullptr);
           if (rc) return bail(rc);
         }
-        Opnd Qr{p->Q, l2, bi1, szQ, cap, 1};
+        const Opnd Qr = Sp(Opnd{p->Q, l2, bi1, szQ, cap, 1}, p->Q, p->Ql);
         rc = add_gemm(p, TOso(i), Qr, ai1, bi1, (int)l2, 1, Fdn, p->szBl, p->ldB, 1, 0);
         if (rc) return bail(rc);
         if (q.h != 0.0) field_term(1);
@@ -1059,9 +1138,10 @@ int build(const Problem &pr, Plan **out) {
         Opnd Fo{p->Fch, p->ldB, a[i], p->szBl, 3L * ns * cap, 1};
         Opnd S = SLo(i);
         S.div = 3 * ns;
-        rc = add_gemm(p, Fo, S, a[i], 2 * bi1, b[i], 3 * ns, p->Xch, p->szX, 1, p->ldA, 0);
+        rc = add_gemm(p, Fo, S, a[i], 2 * bi1, b[i], 3 * ns, p->Xch, p->szX, 1, p->ldA, 0, 1.f, nullptr, 0, 0, 0, 0, 0,
+                      p->Xchl);
         if (!rc) {
-          Opnd Xr{p->Xch, l2, bi1, p->szX, 3L * ns * cap, 1};
+          const Opnd Xr = Sp(Opnd{p->Xch, l2, bi1, p->szX, 3L * ns * cap, 1}, p->Xch, p->Xchl);
           rc = add_gemm(p, TOso(i), Xr, ai1, bi1, (int)l2, 3 * ns, p->Fch, p->szBl, p->ldB, 1, 0);
         }
         if (rc) return bail(rc);

@@ -20,8 +20,11 @@ struct Tiles {
                         // one walker per tile)
   int wide_tn = 256;    // widest N tile of the walker-by-walker products (64, 128 or 256)
   int max_stages = 4;   // load-ring depth cap (2 .. 4; fewer when shared memory is short)
+  int split_out = 0;    // three passes: 1 = the right factors of the trial products are written as
+                        // TF32 head and tail arrays and loaded split (no conversion in the trial
+                        // products, twice the bytes written by their producers)
   bool operator==(const Tiles &o) const {
-    return stack_tn == o.stack_tn && wide_tn == o.wide_tn && max_stages == o.max_stages;
+    return stack_tn == o.stack_tn && wide_tn == o.wide_tn && max_stages == o.max_stages && split_out == o.split_out;
   }
   bool operator!=(const Tiles &o) const { return !(*this == o); }
 };

@@ -1414,6 +1414,7 @@ int apply_tuned(mpsqmc_ctx *c, const Tuned &t) {
   if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_TC_STACK_TN, t.tiles.stack_tn);
   if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_TC_WIDE_TN, t.tiles.wide_tn);
   if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_TC_STAGES, t.tiles.max_stages);
+  if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_TC_SPLIT_OUT, t.tiles.split_out);
   return rc;
 }
 }  // namespace
@@ -1519,14 +1520,21 @@ int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspa
     }
   } else {
     // tcgen05 sweep: coordinate search over the tile choices, one at a time from the defaults
-    // (stacked tile width, then the walker products' tile width, then the ring depth)
+    // (split right factors, stacked tile width, the walker products' tile width, ring depth)
     Tuned cur = {keep.sweep, keep.workspace, mq::bs::Tiles()};
     if (!(rc = trial(cur, &best))) choice = cur;
-    for (int axis = 0; axis < 3 && !rc; ++axis) {
-      const std::vector<int> vals = axis == 2 ? std::vector<int>{3, 2} : std::vector<int>{128, 64};
+    const int axes = c->precision == MPSQMC_PRECISION_TF32_TC ? 3 : 4;  // one pass: nothing to split
+    for (int ax = 0; ax < axes && !rc; ++ax) {
+      const int axis = axes == 4 ? ax : ax + 1;
+      const std::vector<int> vals = axis == 0   ? std::vector<int>{1}
+                                    : axis == 3 ? std::vector<int>{3, 2}
+                                                : std::vector<int>{128, 64};
       for (int v : vals) {
         Tuned cd = choice;
-        (axis == 0 ? cd.tiles.stack_tn : axis == 1 ? cd.tiles.wide_tn : cd.tiles.max_stages) = v;
+        (axis == 0   ? cd.tiles.split_out
+         : axis == 1 ? cd.tiles.stack_tn
+         : axis == 2 ? cd.tiles.wide_tn
+                     : cd.tiles.max_stages) = v;
         double per = 0.0;
         if ((rc = trial(cd, &per))) break;
         if (per < best) best = per, choice = cd;
@@ -1685,6 +1693,10 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
       if (value < 2 || value > 4) return fail(MPSQMC_E_ARG, "load-ring stages are 2..4");
       c->tc_tiles.max_stages = (int)value;
       break;
+    case MPSQMC_OPT_TC_SPLIT_OUT:
+      if (value != 0 && value != 1) return fail(MPSQMC_E_ARG, "split outputs are 0 or 1");
+      c->tc_tiles.split_out = (int)value;
+      break;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");
   }
@@ -1733,6 +1745,9 @@ int mpsqmc_get_option(mpsqmc_ctx *c, int option, long *value) {
       return 0;
     case MPSQMC_OPT_TC_STAGES:
       *value = c->tc_tiles.max_stages;
+      return 0;
+    case MPSQMC_OPT_TC_SPLIT_OUT:
+      *value = c->tc_tiles.split_out;
       return 0;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");

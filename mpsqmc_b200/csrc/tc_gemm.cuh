@@ -11,17 +11,22 @@
 // wide GEMM (M = trial bond, N = walkers x walker bond).
 //
 // Precision: with passes = 3 every tile is split in shared memory into an exactly-TF32 head
-// (low 13 mantissa bits cleared) and a tail (x - head), and the accumulator takes
-// A_hi B_hi + A_hi B_lo + A_lo B_hi: about FP32 accuracy (relative error ~2^-21 per product term)
-// with FP32 accumulation in TMEM.  passes = 1 runs A_hi B_hi only (TF32).
+// (x rounded to TF32) and a tail ((x - head) rounded to TF32), and the accumulator takes
+// A_hi B_hi + A_hi B_lo + A_lo B_hi: about FP32 accuracy (relative error ~2^-22 per product term)
+// with FP32 accumulation in TMEM.  passes = 1 runs A_hi B_hi only (TF32).  Operands kept in
+// memory as separate head and tail arrays (the trial tensors, and outputs a product writes
+// split for the next one) are loaded split: four TMA boxes per stage and no conversion, which
+// takes the split's shared-memory reads and writes off the stage.
 //
 // Roles (384 threads, one CTA per SM, persistent over tiles):
 //   warp 0      TMA producer (one lane), ring of 2-4 shared-memory stages (as many as fit);
 //   warp 1      TMEM owner and MMA issuer (one lane); two or four accumulators of tn columns;
-//   warps 2-7   head/tail split of each landed stage (passes = 3);
+//   warps 2-7   head/tail split of each landed stage (passes = 3, operands not stored split);
 //   warps 8-11  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM lanes 32 (w % 4)...),
-//               alpha/beta and the store to D; row-major outputs are transposed through shared
-//               memory so that every store instruction writes consecutive elements.
+//               alpha/beta and the store to D; column-major outputs go through shared-memory
+//               boxes and TMA bulk tensor stores (as head and tail arrays when the consumer
+//               loads them split), row-major ones are transposed through shared memory so that
+//               every store instruction writes consecutive elements.
 // Every mbarrier wait is bounded: on expiry the kernel sets bit kTcErrTimeout in *err, every role
 // leaves its loop, the CTA waits (bounded) for its loads in flight, frees TMEM and returns.
 #pragma once
@@ -46,8 +51,15 @@ struct alignas(64) GemmParams {
   CUtensorMap tmA;   // 3D (k, row, z): FP32, box (32, tm, 1), SWIZZLE_128B
   CUtensorMap tmB;   // 3D (k, row, z): FP32, box (32, brows, bstack), SWIZZLE_128B
   CUtensorMap tmD;   // dtma: D as 3D (m, n, z) with m contiguous, box (rows per epilogue warp, 16, 1)
+  CUtensorMap tmA2;  // presplit: the tails of A and/or B (tmA, tmB then map the heads)
+  CUtensorMap tmB2;
+  CUtensorMap tmD2;  // dsplit: where the tails of D go (tmD takes the heads)
   int dtma;          // 1: column-major D (dm = 1), no accumulation: the epilogue writes through
                      // shared memory and TMA bulk tensor stores
+  int presplit;      // passes = 3: bit 0 (A), bit 1 (B): the operand is stored as TF32 head and
+                     // tail arrays and loaded split (no conversion of its tiles)
+  int dsplit;        // dtma and passes = 3: D is written as head and tail arrays for a consumer
+                     // that loads it split
   int M, N, K;       // per batch entry
   int tm, tn;        // MMA M (64 or 128) and tile N (multiple of 16, <= 256)
   int adiv, bdiv;    // operand batch coordinate = z / div; 0: shared (coordinate 0)
@@ -251,6 +263,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
   const uint32_t lo_mult = (p.passes == 3) ? 2u : 1u;  // head (+ tail) tiles per operand
   const uint32_t stage_bytes = lo_mult * (a_bytes + b_bytes);
   const uint32_t b_load = (uint32_t)p.brows * p.bstack * 128;  // bytes one B box brings
+  const int split = p.passes == 3 ? (p.presplit & 3) : 0;
+  const bool conv = p.passes == 3 && split != 3;  // a landed stage still needs splitting
   float *stagebuf = reinterpret_cast<float *>(base + NS * stage_bytes);  // epilogue transposes
   const Tiling t = tiling(p);
   const int nk = (p.K + kKC - 1) / kKC;
@@ -302,9 +316,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             break;
           }
           uint8_t *st = base + s * stage_bytes;
-          mbar_expect_tx(&bar_full[s], a_bytes + b_load);
+          mbar_expect_tx(&bar_full[s], ((split & 1) ? 2 : 1) * a_bytes + ((split & 2) ? 2 : 1) * b_load);
           tma_load_3d(st, &p.tmA, &bar_full[s], kc * kKC, m0, za);
           tma_load_3d(st + lo_mult * a_bytes, &p.tmB, &bar_full[s], kc * kKC, n0, zb);
+          // tails of operands stored split, into the slots the conversion would fill
+          if (split & 1) tma_load_3d(st + a_bytes, &p.tmA2, &bar_full[s], kc * kKC, m0, za);
+          if (split & 2) tma_load_3d(st + 2 * a_bytes + b_bytes, &p.tmB2, &bar_full[s], kc * kKC, n0, zb);
           issued[s] += 1;
           if (++s == NS) {
             s = 0;
@@ -327,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         tc_fence_after();
         const uint32_t dt = tmem + (uint32_t)(acc * p.tn);
         for (int kc = 0; kc < nk; ++kc) {
-          uint64_t *wb = (p.passes == 3) ? &bar_conv[s] : &bar_full[s];
+          uint64_t *wb = conv ? &bar_conv[s] : &bar_full[s];
           if (!mbar_wait(wb, ph, &abort_flag, p.err)) {
             ok = false;
             break;
@@ -361,7 +378,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     // ---------------- head/tail split ----------------
     // head = x rounded to TF32 (cvt.rna), tail = x - head rounded to TF32: the three products
     // then miss only tail x tail and the tail's rounding (about 2^-22 relative per term)
-    if (p.passes == 3) {
+    if (conv) {
       const int ct = threadIdx.x - 64;  // 0 .. 191
       int s = 0;
       uint32_t ph = 0;
@@ -373,9 +390,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             break;
           }
           uint8_t *st = base + s * stage_bytes;
-          // A: [hi | lo] then B: [hi | lo]; 16-byte vectors
+          // A: [hi | lo] then B: [hi | lo]; 16-byte vectors; operands loaded split are skipped
           const int na = (int)(a_bytes / 16), nb = (int)(b_bytes / 16);
-          for (int v = ct; v < na + nb; v += 192) {
+          const int v0 = (split & 1) ? na : 0, v1 = (split & 2) ? na : na + nb;
+          for (int v = v0 + ct; v < v1; v += 192) {
             uint8_t *hp = (v < na) ? st + 16 * v : st + 2 * a_bytes + 16 * (v - na);
             uint8_t *lp = hp + ((v < na) ? a_bytes : b_bytes);
             const float4 x = *reinterpret_cast<float4 *>(hp);
@@ -423,8 +441,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     const bool dtma = p.dtma != 0;
     const bool staged = !dtma && !dot4 && dn == 1 && dm != 1;  // row-major output: transpose first
     // dtma: two 32 x 16 boxes per warp (column-major: 16 columns of nrow contiguous rows), used in
-    // turn, so that filling one overlaps the bulk store of the other
-    float *dbox = stagebuf + (warp - 8) * 1024;
+    // turn, so that filling one overlaps the bulk store of the other; dsplit: two such pairs
+    // (head and tail boxes)
+    const bool dsplit = dtma && p.dsplit;
+    float *dbox = stagebuf + (warp - 8) * (dsplit ? 2048 : 1024);
     int nbox = 0;
     const int nrow = (tm == 128) ? 32 : 16;            // accumulator rows this warp holds (lanes 0 .. nrow-1)
     // tile column j -> batch entry z (-1: past the stacked box, stale shared memory) and row n of B
@@ -489,17 +509,27 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           const int nv = min(16, N - n);
           if (dtma) {
             // rows past M and columns past N are clipped by the tensor map's extents
-            float *bx = dbox + (nbox & 1) * 512;
-            if (lane == 0) bulk_wait_read1();  // the store issued two boxes ago has read bx
+            float *bx = dbox + (nbox & 1) * (dsplit ? 1024 : 512);
+            if (lane == 0) bulk_wait_read1();  // the stores issued two chunks ago have read bx
             __syncwarp();
             if (lane < nrow) {
+              if (dsplit) {  // head = x rounded to TF32, tail = (x - head) rounded to TF32
 #pragma unroll
-              for (int i = 0; i < 16; ++i) bx[i * nrow + lane] = alpha * v[i];
+                for (int i = 0; i < 16; ++i) {
+                  const float x = alpha * v[i], h = to_tf32(x);
+                  bx[i * nrow + lane] = h;
+                  bx[512 + i * nrow + lane] = to_tf32(x - h);
+                }
+              } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) bx[i * nrow + lane] = alpha * v[i];
+              }
             }
             fence_proxy_async();
             __syncwarp();
             if (lane == 0) {
               tma_store_3d(&p.tmD, bx, mq0, n, z);
+              if (dsplit) tma_store_3d(&p.tmD2, bx + 512, mq0, n, z);
               bulk_commit();
             }
             ++nbox;
@@ -646,13 +676,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
 __host__ __device__ constexpr int stage_bytes_of(int tm, int tn, int passes) {
   return (passes == 3 ? 2 : 1) * (tm + tn) * 128;
 }
-__host__ __device__ constexpr int smem_bytes(int tm, int tn, int passes, int stages) {
-  return stages * stage_bytes_of(tm, tn, passes) + 4 * 32 * 33 * 4 + 1024;
+// The epilogue's staging area: transposes (4 warps x 32 x 33 floats) or store boxes (4 warps x
+// 2 boxes of 32 x 16 floats, twice that with head and tail boxes).
+__host__ __device__ constexpr int staging_bytes(int dsplit) { return dsplit ? 4 * 2048 * 4 : 4 * 32 * 33 * 4; }
+__host__ __device__ constexpr int smem_bytes(int tm, int tn, int passes, int stages, int dsplit = 0) {
+  return stages * stage_bytes_of(tm, tn, passes) + staging_bytes(dsplit) + 1024;
 }
 // As many stages (2 .. kMaxStages) as fit in the opt-in shared memory.
-inline int stages_for(int tm, int tn, int passes, int smem_limit) {
+inline int stages_for(int tm, int tn, int passes, int smem_limit, int dsplit = 0) {
   int s = kMaxStages;
-  while (s > 2 && smem_bytes(tm, tn, passes, s) > smem_limit) --s;
+  while (s > 2 && smem_bytes(tm, tn, passes, s, dsplit) > smem_limit) --s;
   return s;
 }
 
