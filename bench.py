@@ -416,8 +416,9 @@ def main():
     params, training = train_proposal(make, args, sweep, seed)
     eng, _ = timed_arm(args.precision, args.steps, args.warmup, args.proposal, params)
     if args.precision.endswith("_tc"):
-        from mpsqmc_b200.capi import OPT_TC_SPLIT_OUT, OPT_TC_STACK_TN, OPT_TC_STAGES, OPT_TC_WIDE_TN
-        cfg["tiles"] = {"split_out": eng.get_option(OPT_TC_SPLIT_OUT), "stack_tn": eng.get_option(OPT_TC_STACK_TN),
+        from mpsqmc_b200.capi import OPT_TC_KC, OPT_TC_SPLIT_OUT, OPT_TC_STACK_TN, OPT_TC_STAGES, OPT_TC_WIDE_TN
+        cfg["tiles"] = {"split_out": eng.get_option(OPT_TC_SPLIT_OUT), "kc_trial": eng.get_option(OPT_TC_KC),
+                        "stack_tn": eng.get_option(OPT_TC_STACK_TN),
                         "wide_tn": eng.get_option(OPT_TC_WIDE_TN), "max_stages": eng.get_option(OPT_TC_STAGES),
                         "chosen_by": ("mpsqmc_autotune: coordinate search over the tile choices on up to 1024 "
                                       "walkers of this bond profile" if args.tiles == "autotune" else "defaults")}

@@ -244,17 +244,20 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
                                       * most sum P / alpha and a poorly trained network cannot
                                       * give heavy-tailed weights.  1000 samples the grid PDF. */
 #define MPSQMC_OPT_TC_STACK_TN 11     /* tile choices of the tcgen05 sweep's products (defaults
-                                      * 256, 256, 4; mpsqmc_autotune picks them per bond profile):
+                                      * 256, 256, 8; mpsqmc_autotune picks them per bond profile):
                                       * widest N tile (64, 128, 256) of the products whose left
                                       * factor is a trial tensor, walkers stacked along N up to it */
 #define MPSQMC_OPT_TC_WIDE_TN 12      /*   widest N tile (64, 128, 256) of the walker-by-walker
                                       *   products */
-#define MPSQMC_OPT_TC_STAGES 13       /*   load-ring depth cap, 2..4 (fewer when shared memory is
-                                      *   short) */
+#define MPSQMC_OPT_TC_STAGES 13       /*   load-ring depth cap, 2..8 (fewer when shared memory is
+                                      *   short; default 8) */
 #define MPSQMC_OPT_TC_SPLIT_OUT 14    /*   0 (default) / 1: with three passes, the walker-side right
                                       *   factors of the trial products are written as TF32 head
                                       *   and tail arrays and loaded split (the trial itself always
                                       *   is), instead of being split in shared memory */
+#define MPSQMC_OPT_TC_KC 15           /*   k-values per load stage of the trial products: 32
+                                      *   (default, 128-byte swizzled rows) or 16 (64-byte rows:
+                                      *   half the stage, twice the ring depth) */
 int mpsqmc_set_option(mpsqmc_ctx *ctx, int option, long value);
 int mpsqmc_get_option(mpsqmc_ctx *ctx, int option, long *value);
 
@@ -301,8 +304,8 @@ int mpsqmc_proposal_stats(mpsqmc_ctx *ctx, double *last_loss, int *updates);
  * (MPSQMC_OPT_SWEEP, MPSQMC_OPT_WORKSPACE) choice on the first walkers of the current population
  * (two waves of one CTA per SM), restores the population, random stream and step count after
  * each trial, and keeps the fastest.  Under the tcgen05 sweep (MPSQMC_PRECISION_TF32X3_TC,
- * TF32_TC) it instead tunes that sweep's choices (MPSQMC_OPT_TC_SPLIT_OUT, _STACK_TN, _WIDE_TN,
- * _STAGES) by a coordinate search from the defaults, each timed on up to 1024 walkers (its tile counts
+ * TF32_TC) it instead tunes that sweep's choices (MPSQMC_OPT_TC_SPLIT_OUT, _KC, _STACK_TN,
+ * _WIDE_TN, _STAGES) by a coordinate search from the defaults, each timed on up to 1024 walkers (its tile counts
  * grow with the population).  The choice is remembered per problem shape (L, trial and walker
  * bond dims, couplings, projector, sweep family) for later contexts of this process, which then
  * skip the measurement.  best_* (may be NULL) receive the chosen sweep and workspace values. */

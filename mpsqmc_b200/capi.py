@@ -31,7 +31,7 @@ OPT_PROPOSAL = 8
 PROPOSAL_GRID, PROPOSAL_LEARNED = 0, 1
 OPT_PROPOSAL_TRAINING = 9
 OPT_PROPOSAL_MIX = 10  # thousandths of the exact PDF in the learned proposal's defensive mixture
-OPT_TC_STACK_TN, OPT_TC_WIDE_TN, OPT_TC_STAGES, OPT_TC_SPLIT_OUT = 11, 12, 13, 14  # tcgen05 sweep choices
+OPT_TC_STACK_TN, OPT_TC_WIDE_TN, OPT_TC_STAGES, OPT_TC_SPLIT_OUT, OPT_TC_KC = 11, 12, 13, 14, 15  # tcgen05 choices
 
 # Every symbol include/mpsqmc_gpu.h declares.
 EXPORTED = [

@@ -45,11 +45,12 @@ int fail(int code, const std::string &m) {
 }  // namespace
 
 // A K-major FP32 operand as a 3D tensor map (k, row, z): element (k, r, z) at
-// base[k + r * row_stride + z * z_stride]; box (32, box_rows, box_z), 128-byte swizzle.
+// base[k + r * row_stride + z * z_stride]; box (kc, box_rows, box_z), 128-byte swizzle for kc = 32
+// and 64-byte swizzle for kc = 16.
 // k_ext, rows, zs: extents the loads may touch (allocated memory; padding must be zero where a
 // product would read it).  Strides are in elements and must be multiples of 4 (16 bytes).
 int make_operand_map(CUtensorMap *map, const float *base, long k_ext, long rows, long zs, long row_stride,
-                     long z_stride, int box_rows, int box_z) {
+                     long z_stride, int box_rows, int box_z, int kc = kKC) {
   EncodeTiled enc = encoder();
   if (!enc) return fail(MPSQMC_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
   if ((reinterpret_cast<uintptr_t>(base) & 15) || (row_stride & 3) || (z_stride & 3))
@@ -58,11 +59,12 @@ int make_operand_map(CUtensorMap *map, const float *base, long k_ext, long rows,
     return fail(MPSQMC_E_ARG, "tcgen05 operand: box outside [1, 256]");
   cuuint64_t dims[3] = {(cuuint64_t)k_ext, (cuuint64_t)rows, (cuuint64_t)zs};
   cuuint64_t strides[2] = {(cuuint64_t)row_stride * 4, (cuuint64_t)std::max(z_stride, row_stride * rows) * 4};
-  cuuint32_t box[3] = {(cuuint32_t)kKC, (cuuint32_t)box_rows, (cuuint32_t)box_z};
+  if (kc != 32 && kc != 16) return fail(MPSQMC_E_ARG, "tcgen05 operand: 16 or 32 k-values per stage");
+  cuuint32_t box[3] = {(cuuint32_t)kc, (cuuint32_t)box_rows, (cuuint32_t)box_z};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, kc == 32 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(MPSQMC_E_ARG, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return 0;
 }
@@ -116,8 +118,8 @@ int pick_stages(GemmParams &p, int max_stages = kMaxStages) {
   int sms = 0, limit = 0;
   const int rc = configure_kernel(&sms, &limit);
   if (rc) return rc;
-  p.stages = std::max(2, std::min(max_stages, stages_for(p.tm, p.tn, p.passes, limit, p.dsplit)));
-  if (smem_bytes(p.tm, p.tn, p.passes, p.stages, p.dsplit) > limit)
+  p.stages = std::max(2, std::min(max_stages, stages_for(p.tm, p.tn, p.passes, limit, p.dsplit, p.kc)));
+  if (smem_bytes(p.tm, p.tn, p.passes, p.stages, p.dsplit, p.kc) > limit)
     return fail(MPSQMC_E_UNSUPPORTED, "tcgen05 GEMM tile does not fit in shared memory");
   return 0;
 }
@@ -128,7 +130,7 @@ int launch(const GemmParams &p, long max_tiles, cudaStream_t stream) {
   int rc = configure_kernel(&sms, nullptr);
   if (rc) return rc;
   const int grid = (int)std::max(1L, std::min((long)sms, max_tiles));
-  tc_gemm_kernel<<<grid, kThreads, smem_bytes(p.tm, p.tn, p.passes, p.stages, p.dsplit), stream>>>(p);
+  tc_gemm_kernel<<<grid, kThreads, smem_bytes(p.tm, p.tn, p.passes, p.stages, p.dsplit, p.kc), stream>>>(p);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(MPSQMC_E_CUDA, std::string("tcgen05 GEMM launch: ") + cudaGetErrorString(e));
   return 0;
@@ -175,6 +177,7 @@ extern "C" int mpsqmc_tc_gemm(float *D, const float *A, const float *B, int M, i
   p.dn = dn;
   p.epi = kStore;
   p.err = err;
+  p.kc = kKC;
   const long kpad = ((K + kKC - 1) / kKC) * kKC;
   // operand rows the boxes may touch: whole tiles (callers pad A to a multiple of tm rows and
   // B to a multiple of the tile rows when bstack == 1)
@@ -182,8 +185,8 @@ extern "C" int mpsqmc_tc_gemm(float *D, const float *A, const float *B, int M, i
   const long brows = bstack > 1 ? N : ((N + p.tn - 1) / p.tn) * p.tn;
   int rc = pick_stages(p);
   pick_store(p, Z);
-  if (!rc) rc = make_operand_map(&p.tmA, A, kpad, arows, std::max(1L, a_zcount), lda, a_zstride, p.tm, 1);
-  if (!rc) rc = make_operand_map(&p.tmB, B, kpad, brows, std::max(1L, b_zcount), ldb, b_zstride, p.brows, bstack);
+  if (!rc) rc = make_operand_map(&p.tmA, A, kpad, arows, std::max(1L, a_zcount), lda, a_zstride, p.tm, 1, p.kc);
+  if (!rc) rc = make_operand_map(&p.tmB, B, kpad, brows, std::max(1L, b_zcount), ldb, b_zstride, p.brows, bstack, p.kc);
   if (rc) return rc;
   const long mt = (M + p.tm - 1) / p.tm;
   const long nt = bstack > 1 ? (Z + bstack - 1) / bstack : (long)Z * ((N + p.tn - 1) / p.tn);
@@ -656,6 +659,7 @@ int add_gemm(Plan *p, const Opnd &A, const Opnd &B, int M, int N, int K, int zpe
   g.K = K;
   g.tm = tm_for(M);
   const Tiles &t = p->pr.tiles;
+  g.kc = A.div == 0 ? t.kc_trial : kKC;  // k-values per stage (the trial products' is a tile choice)
   int bstack = 1;
   if (A.div == 0 && (N & 7) == 0 && 2 * N <= t.stack_tn) bstack = t.stack_tn / N;
   if (bstack > 1) {
@@ -701,12 +705,12 @@ int add_gemm(Plan *p, const Opnd &A, const Opnd &B, int M, int N, int K, int zpe
   const float *ah = (g.presplit & 1) ? A.hi : A.base, *bh = (g.presplit & 2) ? B.hi : B.base;
   const long brows_map = bstack > 1 ? N : B.rows;
   int rc = pick_stages(g, t.max_stages);
-  if (!rc) rc = make_operand_map(&g.tmA, ah, K, A.rows, std::max(1L, A.zn), A.ld, A.zs, g.tm, 1);
-  if (!rc) rc = make_operand_map(&g.tmB, bh, K, brows_map, std::max(1L, B.zn), B.ld, B.zs, g.brows, bstack);
+  if (!rc) rc = make_operand_map(&g.tmA, ah, K, A.rows, std::max(1L, A.zn), A.ld, A.zs, g.tm, 1, g.kc);
+  if (!rc) rc = make_operand_map(&g.tmB, bh, K, brows_map, std::max(1L, B.zn), B.ld, B.zs, g.brows, bstack, g.kc);
   if (!rc && (g.presplit & 1))
-    rc = make_operand_map(&g.tmA2, A.lo, K, A.rows, std::max(1L, A.zn), A.ld, A.zs, g.tm, 1);
+    rc = make_operand_map(&g.tmA2, A.lo, K, A.rows, std::max(1L, A.zn), A.ld, A.zs, g.tm, 1, g.kc);
   if (!rc && (g.presplit & 2))
-    rc = make_operand_map(&g.tmB2, B.lo, K, brows_map, std::max(1L, B.zn), B.ld, B.zs, g.brows, bstack);
+    rc = make_operand_map(&g.tmB2, B.lo, K, brows_map, std::max(1L, B.zn), B.ld, B.zs, g.brows, bstack, g.kc);
   if (rc) return rc;
   const long zt = (long)zper * p->cap;
   const long mt = (M + g.tm - 1) / g.tm;

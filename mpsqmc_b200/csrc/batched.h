@@ -19,12 +19,15 @@ struct Tiles {
                         // stacked along N up to this width (64, 128 or 256; 64 with N = 64 means
                         // one walker per tile)
   int wide_tn = 256;    // widest N tile of the walker-by-walker products (64, 128 or 256)
-  int max_stages = 4;   // load-ring depth cap (2 .. 4; fewer when shared memory is short)
+  int max_stages = 8;   // load-ring depth cap (2 .. 8; fewer when shared memory is short)
+  int kc_trial = 32;    // k-values per stage of the trial products (32, or 16: half the stage
+                        // and twice the ring depth)
   int split_out = 0;    // three passes: 1 = the right factors of the trial products are written as
                         // TF32 head and tail arrays and loaded split (no conversion in the trial
                         // products, twice the bytes written by their producers)
   bool operator==(const Tiles &o) const {
-    return stack_tn == o.stack_tn && wide_tn == o.wide_tn && max_stages == o.max_stages && split_out == o.split_out;
+    return stack_tn == o.stack_tn && wide_tn == o.wide_tn && max_stages == o.max_stages && split_out == o.split_out &&
+           kc_trial == o.kc_trial;
   }
   bool operator!=(const Tiles &o) const { return !(*this == o); }
 };

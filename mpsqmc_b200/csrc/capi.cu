@@ -1415,6 +1415,7 @@ int apply_tuned(mpsqmc_ctx *c, const Tuned &t) {
   if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_TC_WIDE_TN, t.tiles.wide_tn);
   if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_TC_STAGES, t.tiles.max_stages);
   if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_TC_SPLIT_OUT, t.tiles.split_out);
+  if (!rc) rc = mpsqmc_set_option(c, MPSQMC_OPT_TC_KC, t.tiles.kc_trial);
   return rc;
 }
 }  // namespace
@@ -1520,20 +1521,22 @@ int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspa
     }
   } else {
     // tcgen05 sweep: coordinate search over the tile choices, one at a time from the defaults
-    // (split right factors, stacked tile width, the walker products' tile width, ring depth)
     Tuned cur = {keep.sweep, keep.workspace, mq::bs::Tiles()};
     if (!(rc = trial(cur, &best))) choice = cur;
-    const int axes = c->precision == MPSQMC_PRECISION_TF32_TC ? 3 : 4;  // one pass: nothing to split
-    for (int ax = 0; ax < axes && !rc; ++ax) {
-      const int axis = axes == 4 ? ax : ax + 1;
+    // axes: 0 split right factors, 1 k-values per stage of the trial products, 2 stacked tile
+    // width, 3 the walker products' tile width, 4 ring depth cap
+    for (int axis = 0; axis < 5 && !rc; ++axis) {
+      if (axis == 0 && c->precision == MPSQMC_PRECISION_TF32_TC) continue;  // one pass: nothing to split
       const std::vector<int> vals = axis == 0   ? std::vector<int>{1}
-                                    : axis == 3 ? std::vector<int>{3, 2}
+                                    : axis == 1 ? std::vector<int>{16}
+                                    : axis == 4 ? std::vector<int>{4, 2}
                                                 : std::vector<int>{128, 64};
       for (int v : vals) {
         Tuned cd = choice;
         (axis == 0   ? cd.tiles.split_out
-         : axis == 1 ? cd.tiles.stack_tn
-         : axis == 2 ? cd.tiles.wide_tn
+         : axis == 1 ? cd.tiles.kc_trial
+         : axis == 2 ? cd.tiles.stack_tn
+         : axis == 3 ? cd.tiles.wide_tn
                      : cd.tiles.max_stages) = v;
         double per = 0.0;
         if ((rc = trial(cd, &per))) break;
@@ -1690,12 +1693,16 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
       (option == MPSQMC_OPT_TC_STACK_TN ? c->tc_tiles.stack_tn : c->tc_tiles.wide_tn) = (int)value;
       break;
     case MPSQMC_OPT_TC_STAGES:
-      if (value < 2 || value > 4) return fail(MPSQMC_E_ARG, "load-ring stages are 2..4");
+      if (value < 2 || value > 8) return fail(MPSQMC_E_ARG, "load-ring stages are 2..8");
       c->tc_tiles.max_stages = (int)value;
       break;
     case MPSQMC_OPT_TC_SPLIT_OUT:
       if (value != 0 && value != 1) return fail(MPSQMC_E_ARG, "split outputs are 0 or 1");
       c->tc_tiles.split_out = (int)value;
+      break;
+    case MPSQMC_OPT_TC_KC:
+      if (value != 16 && value != 32) return fail(MPSQMC_E_ARG, "k-values per stage are 16 or 32");
+      c->tc_tiles.kc_trial = (int)value;
       break;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");
@@ -1748,6 +1755,9 @@ int mpsqmc_get_option(mpsqmc_ctx *c, int option, long *value) {
       return 0;
     case MPSQMC_OPT_TC_SPLIT_OUT:
       *value = c->tc_tiles.split_out;
+      return 0;
+    case MPSQMC_OPT_TC_KC:
+      *value = c->tc_tiles.kc_trial;
       return 0;
     default:
       return fail(MPSQMC_E_ARG, "unknown option");

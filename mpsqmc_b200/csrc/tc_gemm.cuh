@@ -4,8 +4,9 @@
 //   D_z[m, n] = alpha * sum_k A_{z/adiv}[m, k] * B_{z/bdiv}[n, k]  (+ D_z[m, n] when beta)
 //
 // Both operands are K-major FP32 matrices (k contiguous) read by TMA (cp.async.bulk.tensor, no
-// multicast, tensor maps over this GPU's memory only) into 128-byte-swizzled shared-memory tiles
-// of 32 k-values, the canonical K-major SWIZZLE_128B layout of the UMMA descriptors.  A divisor
+// multicast, tensor maps over this GPU's memory only) into swizzled shared-memory tiles of 32
+// k-values (128-byte rows, the canonical K-major SWIZZLE_128B layout of the UMMA descriptors) or
+// of 16 (64-byte rows, SWIZZLE_64B: half the stage, twice the ring depth).  A divisor
 // of 0 makes the operand shared by the whole batch (the trial tensor); B may stack `bstack`
 // consecutive batch entries along N in one tile, so that products with a shared A become one
 // wide GEMM (M = trial bond, N = walkers x walker bond).
@@ -39,8 +40,8 @@ namespace mq {
 namespace tc {
 
 constexpr int kThreads = 384;
-constexpr int kMaxStages = 4;        // shared-memory stages of the load ring (2 .. 4 by tile size)
-constexpr int kKC = 32;                 // k-values per stage (128 bytes of FP32: one swizzle row)
+constexpr int kMaxStages = 8;        // shared-memory stages of the load ring (2 .. 8 by tile size)
+constexpr int kKC = 32;                 // k-values per stage, largest choice (128 bytes of FP32)
 constexpr int kMaxTN = 256;
 constexpr int kErrTimeout = 4;          // bit in the device error word (batched.h: bs::kErrTimeout)
 constexpr long long kWaitCycles = 4000000000LL;  // a pipeline wait gives up after ~2 s of SM cycles
@@ -71,6 +72,7 @@ struct alignas(64) GemmParams {
   int beta;          // 1: accumulate into D
   int passes;        // 1 or 3
   int stages;        // shared-memory stages of the load ring (2 .. kMaxStages)
+  int kc;            // k-values per stage: 32 (SWIZZLE_128B) or 16 (SWIZZLE_64B)
   float *D;
   long dz, dm, dn;   // D_z[m, n] = D[z dz + m dm + n dn]
   int epi;           // kStore, or kDot4: out[z] += sum_mn D_z[m,n] * E_{z,q}[m,n] for q < 4 (no store)
@@ -166,14 +168,14 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// K-major, 128-byte swizzle: 8-row groups of 1024 bytes (stride byte offset 1024), version 1.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+// K-major, swizzled rows of 128 or 64 bytes: 8-row groups of 8 rows (stride byte offset), version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t row_bytes) {
   uint64_t d = 0;
   d |= (uint64_t)((addr >> 4) & 0x3FFF);
-  d |= (uint64_t)1 << 16;                  // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;        // stride byte offset
-  d |= (uint64_t)1 << 46;                  // descriptor version (sm_100)
-  d |= (uint64_t)2 << 61;                  // SWIZZLE_128B
+  d |= (uint64_t)1 << 16;                          // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)((8 * row_bytes) >> 4) << 32;     // stride byte offset: one 8-row group
+  d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
+  d |= (uint64_t)(row_bytes == 128 ? 2 : 4) << 61;  // SWIZZLE_128B or SWIZZLE_64B
   return d;
 }
 
@@ -238,11 +240,12 @@ __device__ __forceinline__ void tile_coords(const GemmParams &p, const Tiling &t
   }
 }
 
-// x rounded to the nearest TF32 value (10 explicit mantissa bits), as an FP32 bit pattern
+// x rounded to the nearest TF32 value (10 explicit mantissa bits), ties away from zero, as an
+// FP32 bit pattern: half of the 13 dropped bits' range is added to the magnitude bits, which are
+// then cleared (a carry into the exponent is the correct rounding).  Two integer operations at
+// full rate (finite x); the same values as the host's tf32_round.
 __device__ __forceinline__ float to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -259,15 +262,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int NS = p.stages;
   uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const uint32_t a_bytes = (uint32_t)p.tm * 128, b_bytes = (uint32_t)p.tn * 128;
+  const uint32_t row_bytes = (uint32_t)p.kc * 4;  // one tile row of kc FP32 values
+  const uint32_t a_bytes = (uint32_t)p.tm * row_bytes, b_bytes = (uint32_t)p.tn * row_bytes;
   const uint32_t lo_mult = (p.passes == 3) ? 2u : 1u;  // head (+ tail) tiles per operand
   const uint32_t stage_bytes = lo_mult * (a_bytes + b_bytes);
-  const uint32_t b_load = (uint32_t)p.brows * p.bstack * 128;  // bytes one B box brings
+  const uint32_t b_load = (uint32_t)p.brows * p.bstack * row_bytes;  // bytes one B box brings
   const int split = p.passes == 3 ? (p.presplit & 3) : 0;
   const bool conv = p.passes == 3 && split != 3;  // a landed stage still needs splitting
   float *stagebuf = reinterpret_cast<float *>(base + NS * stage_bytes);  // epilogue transposes
   const Tiling t = tiling(p);
-  const int nk = (p.K + kKC - 1) / kKC;
+  const int KC = p.kc, nk = (p.K + KC - 1) / KC;
   // accumulators in TMEM: four when they fit in its 512 columns (more slack between the products
   // of one tile and the epilogue of an earlier one), else two
   const int nacc = p.tn <= 128 ? 4 : 2;
@@ -317,11 +321,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           }
           uint8_t *st = base + s * stage_bytes;
           mbar_expect_tx(&bar_full[s], ((split & 1) ? 2 : 1) * a_bytes + ((split & 2) ? 2 : 1) * b_load);
-          tma_load_3d(st, &p.tmA, &bar_full[s], kc * kKC, m0, za);
-          tma_load_3d(st + lo_mult * a_bytes, &p.tmB, &bar_full[s], kc * kKC, n0, zb);
+          tma_load_3d(st, &p.tmA, &bar_full[s], kc * KC, m0, za);
+          tma_load_3d(st + lo_mult * a_bytes, &p.tmB, &bar_full[s], kc * KC, n0, zb);
           // tails of operands stored split, into the slots the conversion would fill
-          if (split & 1) tma_load_3d(st + a_bytes, &p.tmA2, &bar_full[s], kc * kKC, m0, za);
-          if (split & 2) tma_load_3d(st + 2 * a_bytes + b_bytes, &p.tmB2, &bar_full[s], kc * kKC, n0, zb);
+          if (split & 1) tma_load_3d(st + a_bytes, &p.tmA2, &bar_full[s], kc * KC, m0, za);
+          if (split & 2) tma_load_3d(st + 2 * a_bytes + b_bytes, &p.tmB2, &bar_full[s], kc * KC, n0, zb);
           issued[s] += 1;
           if (++s == NS) {
             s = 0;
@@ -352,14 +356,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           tc_fence_after();
           uint8_t *st = base + s * stage_bytes;
           const uint32_t ahi = smem_u32(st), alo = ahi + a_bytes, bhi = ahi + lo_mult * a_bytes, blo = bhi + b_bytes;
-#pragma unroll
-          for (int kk = 0; kk < kKC / 8; ++kk) {
+          for (int kk = 0; kk < KC / 8; ++kk) {
             const uint32_t off = kk * 32;  // 8 TF32 values = 32 bytes inside the swizzle row
             const uint32_t first = (kc == 0 && kk == 0) ? 0u : 1u;
-            mma_tf32(dt, smem_desc(ahi + off), smem_desc(bhi + off), idesc, first);
+            mma_tf32(dt, smem_desc(ahi + off, row_bytes), smem_desc(bhi + off, row_bytes), idesc, first);
             if (p.passes == 3) {
-              mma_tf32(dt, smem_desc(ahi + off), smem_desc(blo + off), idesc, 1u);
-              mma_tf32(dt, smem_desc(alo + off), smem_desc(bhi + off), idesc, 1u);
+              mma_tf32(dt, smem_desc(ahi + off, row_bytes), smem_desc(blo + off, row_bytes), idesc, 1u);
+              mma_tf32(dt, smem_desc(alo + off, row_bytes), smem_desc(bhi + off, row_bytes), idesc, 1u);
             }
           }
           mma_commit(&bar_empty[s]);  // frees the stage once these products are done
@@ -393,21 +396,32 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           // A: [hi | lo] then B: [hi | lo]; 16-byte vectors; operands loaded split are skipped
           const int na = (int)(a_bytes / 16), nb = (int)(b_bytes / 16);
           const int v0 = (split & 1) ? na : 0, v1 = (split & 2) ? na : na + nb;
-          for (int v = v0 + ct; v < v1; v += 192) {
-            uint8_t *hp = (v < na) ? st + 16 * v : st + 2 * a_bytes + 16 * (v - na);
-            uint8_t *lp = hp + ((v < na) ? a_bytes : b_bytes);
-            const float4 x = *reinterpret_cast<float4 *>(hp);
-            float4 h, l;
-            h.x = to_tf32(x.x);
-            h.y = to_tf32(x.y);
-            h.z = to_tf32(x.z);
-            h.w = to_tf32(x.w);
-            l.x = to_tf32(x.x - h.x);
-            l.y = to_tf32(x.y - h.y);
-            l.z = to_tf32(x.z - h.z);
-            l.w = to_tf32(x.w - h.w);
-            *reinterpret_cast<float4 *>(hp) = h;
-            *reinterpret_cast<float4 *>(lp) = l;
+          // four vectors per thread in flight: their loads issue before the first conversion
+          for (int vb = v0 + ct; vb < v1; vb += 4 * 192) {
+            float4 x[4];
+            uint8_t *hp[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int v = vb + u * 192;
+              hp[u] = (v < na) ? st + 16 * v : st + 2 * a_bytes + 16 * (v - na);
+              if (v < v1) x[u] = *reinterpret_cast<float4 *>(hp[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int v = vb + u * 192;
+              if (v >= v1) break;
+              float4 h, l;
+              h.x = to_tf32(x[u].x);
+              h.y = to_tf32(x[u].y);
+              h.z = to_tf32(x[u].z);
+              h.w = to_tf32(x[u].w);
+              l.x = to_tf32(x[u].x - h.x);
+              l.y = to_tf32(x[u].y - h.y);
+              l.z = to_tf32(x[u].z - h.z);
+              l.w = to_tf32(x[u].w - h.w);
+              *reinterpret_cast<float4 *>(hp[u]) = h;
+              *reinterpret_cast<float4 *>(hp[u] + ((v < na) ? a_bytes : b_bytes)) = l;
+            }
           }
           fence_proxy_async();
           __syncwarp();
@@ -673,19 +687,19 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
 
 // Shared memory of one launch: the stage ring (head and, with 3 passes, tail tiles), the
 // epilogue's transpose buffers and the 1024-byte alignment slack.
-__host__ __device__ constexpr int stage_bytes_of(int tm, int tn, int passes) {
-  return (passes == 3 ? 2 : 1) * (tm + tn) * 128;
+__host__ __device__ constexpr int stage_bytes_of(int tm, int tn, int passes, int kc = kKC) {
+  return (passes == 3 ? 2 : 1) * (tm + tn) * kc * 4;
 }
 // The epilogue's staging area: transposes (4 warps x 32 x 33 floats) or store boxes (4 warps x
 // 2 boxes of 32 x 16 floats, twice that with head and tail boxes).
 __host__ __device__ constexpr int staging_bytes(int dsplit) { return dsplit ? 4 * 2048 * 4 : 4 * 32 * 33 * 4; }
-__host__ __device__ constexpr int smem_bytes(int tm, int tn, int passes, int stages, int dsplit = 0) {
-  return stages * stage_bytes_of(tm, tn, passes) + staging_bytes(dsplit) + 1024;
+__host__ __device__ constexpr int smem_bytes(int tm, int tn, int passes, int stages, int dsplit = 0, int kc = kKC) {
+  return stages * stage_bytes_of(tm, tn, passes, kc) + staging_bytes(dsplit) + 1024;
 }
 // As many stages (2 .. kMaxStages) as fit in the opt-in shared memory.
-inline int stages_for(int tm, int tn, int passes, int smem_limit, int dsplit = 0) {
+inline int stages_for(int tm, int tn, int passes, int smem_limit, int dsplit = 0, int kc = kKC) {
   int s = kMaxStages;
-  while (s > 2 && smem_bytes(tm, tn, passes, s, dsplit) > smem_limit) --s;
+  while (s > 2 && smem_bytes(tm, tn, passes, s, dsplit, kc) > smem_limit) --s;
   return s;
 }
 

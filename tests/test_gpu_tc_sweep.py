@@ -12,8 +12,8 @@ import pytest
 
 from conftest import couplings, load_golden
 from mpsqmc_b200 import Engine
-from mpsqmc_b200.capi import (E_UNSUPPORTED, OPT_PRECISION, OPT_TC_SPLIT_OUT, OPT_TC_STACK_TN, OPT_TC_STAGES,
-                              OPT_TC_WIDE_TN,
+from mpsqmc_b200.capi import (E_UNSUPPORTED, OPT_PRECISION, OPT_TC_KC, OPT_TC_SPLIT_OUT, OPT_TC_STACK_TN,
+                              OPT_TC_STAGES, OPT_TC_WIDE_TN,
                               PRECISION_TF32_TC, PRECISION_TF32X3, PRECISION_TF32X3_TC, TRACE_STRIDE, MpsqmcError)
 
 pytestmark = pytest.mark.gpu
@@ -100,14 +100,15 @@ def test_tc_rejects_uneven_populations():
 
 
 def test_tc_tile_choices_give_the_same_walk():
-    """Other tile shapes, ring depths and split right factors (the autotuner's candidates) only
-    regroup the same per-element products (a factor written as TF32 head and tail is split as the
+    """Other tile shapes, ring depths, stage depths in k and split right factors (the autotuner's
+    candidates) only regroup the same per-element products (a factor written as TF32 head and tail is split as the
     shared-memory conversion would split it): the step's results agree with the defaults' to FP32
     rounding."""
     z = load_golden("walk_snake4x4_D16_DW8_branch")
     a = engine_for(z, PRECISION_TF32X3_TC)
     b = engine_for(z, PRECISION_TF32X3_TC)
-    for opt, v in ((OPT_TC_STACK_TN, 64), (OPT_TC_WIDE_TN, 128), (OPT_TC_STAGES, 2), (OPT_TC_SPLIT_OUT, 1)):
+    for opt, v in ((OPT_TC_STACK_TN, 64), (OPT_TC_WIDE_TN, 128), (OPT_TC_STAGES, 2), (OPT_TC_SPLIT_OUT, 1),
+                   (OPT_TC_KC, 16)):
         b.set_option(opt, v)
         assert b.get_option(opt) == v
     sa, sb = a.walk(3), b.walk(3)
@@ -130,7 +131,8 @@ def test_tc_autotune_picks_valid_tiles_and_keeps_the_walk():
     b.autotune(steps=1)  # population, random stream and step count restored afterwards
     assert b.get_option(OPT_TC_STACK_TN) in (64, 128, 256)
     assert b.get_option(OPT_TC_WIDE_TN) in (64, 128, 256)
-    assert b.get_option(OPT_TC_STAGES) in (2, 3, 4)
+    assert b.get_option(OPT_TC_STAGES) in (2, 4, 8)
+    assert b.get_option(OPT_TC_KC) in (16, 32)
     assert b.get_option(OPT_TC_SPLIT_OUT) in (0, 1)
     sa, sb = a.walk(2), b.walk(2)
     for x, y in zip(sa, sb):
