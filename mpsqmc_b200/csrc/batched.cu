@@ -72,24 +72,50 @@ int make_operand_map(CUtensorMap *map, const float *base, long k_ext, long rows,
 // Column-major D (element (m, n, z) at D[m + n dn + z dz]) as the epilogue's store map: box
 // (box_rows, 16, 1), no swizzle; extents M x N x zs clip what a box holds past them.  Used when
 // dn and dz are multiples of 4 and D is 16-byte aligned (else the epilogue stores directly).
-bool make_store_map(CUtensorMap *map, float *D, long M, long N, long zs, long dn, long dz, int box_rows) {
+bool make_store_map(CUtensorMap *map, float *D, long M, long N, long zs, long dn, long dz, int box_rows,
+                    int box_cols = 16) {
   EncodeTiled enc = encoder();
   if (!enc || (reinterpret_cast<uintptr_t>(D) & 15) || (dn & 3) || (dz & 3) || dn < M || (zs > 1 && dz < N * dn))
     return false;
   cuuint64_t dims[3] = {(cuuint64_t)M, (cuuint64_t)N, (cuuint64_t)std::max(1L, zs)};
   cuuint64_t strides[2] = {(cuuint64_t)dn * 4, (cuuint64_t)std::max(dz, N * dn) * 4};
-  cuuint32_t box[3] = {(cuuint32_t)box_rows, 16, 1};
+  cuuint32_t box[3] = {(cuuint32_t)box_rows, (cuuint32_t)box_cols, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, D, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
          CUDA_SUCCESS;
 }
 
-// The epilogue's store route: TMA boxes for column-major outputs without accumulation.
+// Row-major D (element (m, n, z) at D[n + m dm + z dz]) as the epilogue's store map: box
+// (32, box_rows, 1) with a 128-byte swizzle; extents N x M x zs clip what a box holds past them.
+bool make_row_store_map(CUtensorMap *map, float *D, long M, long N, long zs, long dm, long dz, int box_rows) {
+  EncodeTiled enc = encoder();
+  if (!enc || (reinterpret_cast<uintptr_t>(D) & 15) || (dm & 3) || (dz & 3) || dm < N || (zs > 1 && dz < M * dm))
+    return false;
+  cuuint64_t dims[3] = {(cuuint64_t)N, (cuuint64_t)M, (cuuint64_t)std::max(1L, zs)};
+  cuuint64_t strides[2] = {(cuuint64_t)dm * 4, (cuuint64_t)std::max(dz, M * dm) * 4};
+  cuuint32_t box[3] = {32, (cuuint32_t)box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, D, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+// The epilogue's store route: TMA boxes for column-major outputs without accumulation, 32 columns
+// wide for unstacked tiles whose width is a multiple of 32 (dsplit, set later, narrows them), and
+// for row-major ones whose 32-column steps stay in one batch entry.
 void pick_store(GemmParams &p, long zs) {
-  p.dtma = 0;
-  if (p.epi == kStore && p.dm == 1 && !p.beta && p.dn > 1)
-    p.dtma = make_store_map(&p.tmD, p.D, p.M, p.N, zs, p.dn, p.dz, p.tm == 128 ? 32 : 16) ? 1 : 0;
+  p.dtma = p.dwide = p.rtma = 0;
+  if (p.epi == kStore && p.dn == 1 && p.dm > 1 && !p.beta && (p.tn & 31) == 0 &&
+      (p.bstack == 1 || (p.N & 31) == 0)) {
+    p.rtma = make_row_store_map(&p.tmD, p.D, p.M, p.N, zs, p.dm, p.dz, p.tm == 128 ? 32 : 16) ? 1 : 0;
+    return;
+  }
+  if (p.epi == kStore && p.dm == 1 && !p.beta && p.dn > 1) {
+    const int wide = p.bstack == 1 && (p.tn & 31) == 0;
+    p.dtma = make_store_map(&p.tmD, p.D, p.M, p.N, zs, p.dn, p.dz, p.tm == 128 ? 32 : 16, wide ? 32 : 16) ? 1 : 0;
+    p.dwide = p.dtma && wide;
+  }
 }
 
 // SM count and the dynamic shared memory a launch may use (the opt-in limit less the kernel's
@@ -697,9 +723,11 @@ int add_gemm(Plan *p, const Opnd &A, const Opnd &B, int M, int N, int K, int zpe
   const bool three = p->pr.passes == 3;
   if (three && Dlo) {
     // the consumer loads this output split: only the TMA store route writes the two arrays
-    if (!g.dtma || !make_store_map(&g.tmD2, Dlo, M, N, (long)zper * p->cap, dn, dz, g.tm == 128 ? 32 : 16))
+    if (!g.dtma || !make_store_map(&g.tmD2, Dlo, M, N, (long)zper * p->cap, dn, dz, g.tm == 128 ? 32 : 16) ||
+        !make_store_map(&g.tmD, D, M, N, (long)zper * p->cap, dn, dz, g.tm == 128 ? 32 : 16))
       return fail(MPSQMC_E_UNSUPPORTED, "batched sweep: a split output needs the TMA store route");
     g.dsplit = 1;
+    g.dwide = 0;  // head and tail boxes of 16 columns
   }
   g.presplit = three ? ((A.lo ? 1 : 0) | (B.lo ? 2 : 0)) : 0;
   const float *ah = (g.presplit & 1) ? A.hi : A.base, *bh = (g.presplit & 2) ? B.hi : B.base;

@@ -61,6 +61,11 @@ struct alignas(64) GemmParams {
                      // tail arrays and loaded split (no conversion of its tiles)
   int dsplit;        // dtma and passes = 3: D is written as head and tail arrays for a consumer
                      // that loads it split
+  int dwide;         // dtma, not dsplit, unstacked tiles with tn a multiple of 32: tmD's box is
+                     // 32 columns wide and the epilogue handles 32 columns per step
+  int rtma;          // row-major D (dn = 1), no accumulation, 32-column steps that stay in one
+                     // batch entry: tmD maps D as (n, m, z) with a 128-byte-swizzled box of 32
+                     // columns x (rows per epilogue warp), filled with conflict-free 16-byte stores
   int M, N, K;       // per batch entry
   int tm, tn;        // MMA M (64 or 128) and tile N (multiple of 16, <= 256)
   int adiv, bdiv;    // operand batch coordinate = z / div; 0: shared (coordinate 0)
@@ -162,6 +167,8 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void 
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 // wait until at most one committed group of this thread still reads shared memory
 __device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+// wait until at most three committed groups of this thread still read shared memory
+__device__ __forceinline__ void bulk_wait_read3() { asm volatile("cp.async.bulk.wait_group.read 3;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -206,6 +213,21 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float *v) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, float *v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
+      "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -453,12 +475,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     const int q = warp & 3;  // TMEM lane quarter of this warp
     float *stg = stagebuf + (warp - 8) * 32 * 33;
     const bool dtma = p.dtma != 0;
-    const bool staged = !dtma && !dot4 && dn == 1 && dm != 1;  // row-major output: transpose first
-    // dtma: two 32 x 16 boxes per warp (column-major: 16 columns of nrow contiguous rows), used in
-    // turn, so that filling one overlaps the bulk store of the other; dsplit: two such pairs
-    // (head and tail boxes)
+    const bool staged = !dtma && !p.rtma && !dot4 && dn == 1 && dm != 1;  // row-major: transpose first
+    // dtma: four 32 x 16 boxes per warp (column-major: 16 columns of nrow contiguous rows), used
+    // in turn, so that up to four bulk stores per warp are in flight while the next box fills;
+    // dsplit: two pairs of head and tail boxes
     const bool dsplit = dtma && p.dsplit;
-    float *dbox = stagebuf + (warp - 8) * (dsplit ? 2048 : 1024);
+    const bool dwide = dtma && p.dwide;
+    const bool rtma = p.rtma != 0;
+    float *dbox = stagebuf + (warp - 8) * 2048;
     int nbox = 0;
     const int nrow = (tm == 128) ? 32 : 16;            // accumulator rows this warp holds (lanes 0 .. nrow-1)
     // tile column j -> batch entry z (-1: past the stacked box, stale shared memory) and row n of B
@@ -511,7 +535,63 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       const int m = mq0 + lane;
       const bool mrow = lane < nrow && m < M;
       int zlast = -1;
-      for (int c0 = 0; c0 < tn; c0 += 16) {
+      if (dwide) {
+        // column-major output of an unstacked tile, 32 columns per step: one TMEM load, one
+        // fence and one 32 x 32 bulk store amortise the loop's fixed cost (the epilogue warps
+        // run one per SM sub-partition, so each step's dependent instructions are not hidden)
+        for (int c0 = 0; c0 < tn; c0 += 32) {
+          float v[32];
+          __syncwarp();
+          tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * tn + c0), v);
+          const int n = n0 + c0;
+          if (z0 >= Zt || n >= N) break;  // the same for every lane
+          float *bx = dbox + (nbox & 1) * 1024;
+          if (lane == 0) bulk_wait_read1();  // the store issued two steps ago has read bx
+          __syncwarp();
+          if (lane < nrow) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) bx[i * nrow + lane] = alpha * v[i];
+          }
+          fence_proxy_async();
+          __syncwarp();
+          if (lane == 0) {
+            tma_store_3d(&p.tmD, bx, mq0, n, z0);
+            bulk_commit();
+          }
+          ++nbox;
+        }
+      }
+      if (rtma) {
+        // row-major output, 32 columns per step: lane r writes its row's 32 values as eight
+        // 16-byte pieces, piece c at position c ^ (r % 8) of the 128-byte row (the SWIZZLE_128B
+        // layout the bulk store reads), so each quarter-warp's stores hit distinct banks
+        for (int c0 = 0; c0 < tn; c0 += 32) {
+          float v[32];
+          __syncwarp();
+          tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * tn + c0), v);
+          int z, n;
+          col(c0, z0, n0, z, n);
+          if (z < 0 || z >= Zt || n >= N) break;  // later steps are past the entries too
+          float *bx = dbox + (nbox & 1) * 1024;
+          if (lane == 0) bulk_wait_read1();  // the store issued two steps ago has read bx
+          __syncwarp();
+          if (lane < nrow) {
+            float4 *row = reinterpret_cast<float4 *>(bx + lane * 32);
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+              row[c ^ (lane & 7)] = make_float4(alpha * v[4 * c], alpha * v[4 * c + 1], alpha * v[4 * c + 2],
+                                                alpha * v[4 * c + 3]);
+          }
+          fence_proxy_async();
+          __syncwarp();
+          if (lane == 0) {
+            tma_store_3d(&p.tmD, bx, n, mq0, z);
+            bulk_commit();
+          }
+          ++nbox;
+        }
+      }
+      for (int c0 = 0; c0 < (dwide || rtma ? 0 : tn); c0 += 16) {
         float v[16];
         __syncwarp();  // tcgen05.ld is warp-collective
         tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * tn + c0), v);
@@ -523,8 +603,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           const int nv = min(16, N - n);
           if (dtma) {
             // rows past M and columns past N are clipped by the tensor map's extents
-            float *bx = dbox + (nbox & 1) * (dsplit ? 1024 : 512);
-            if (lane == 0) bulk_wait_read1();  // the stores issued two chunks ago have read bx
+            float *bx = dsplit ? dbox + (nbox & 1) * 1024 : dbox + (nbox & 3) * 512;
+            if (lane == 0) {  // the stores that last used bx have read it
+              if (dsplit) bulk_wait_read1();
+              else bulk_wait_read3();
+            }
             __syncwarp();
             if (lane < nrow) {
               if (dsplit) {  // head = x rounded to TF32, tail = (x - head) rounded to TF32
@@ -658,7 +741,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       acc = (acc + 1 == nacc) ? 0 : acc + 1;
     }
     // the bulk stores this warp issued have completed (they read its boxes until then)
-    if (dtma && lane == 0) bulk_wait_all();
+    if ((dtma || rtma) && lane == 0) bulk_wait_all();
   }
 
   // ---------------- teardown ----------------
@@ -691,8 +774,8 @@ __host__ __device__ constexpr int stage_bytes_of(int tm, int tn, int passes, int
   return (passes == 3 ? 2 : 1) * (tm + tn) * kc * 4;
 }
 // The epilogue's staging area: transposes (4 warps x 32 x 33 floats) or store boxes (4 warps x
-// 2 boxes of 32 x 16 floats, twice that with head and tail boxes).
-__host__ __device__ constexpr int staging_bytes(int dsplit) { return dsplit ? 4 * 2048 * 4 : 4 * 32 * 33 * 4; }
+// 4 boxes of 32 x 16 floats, or two pairs of head and tail boxes).
+__host__ __device__ constexpr int staging_bytes(int dsplit) { return 4 * 2048 * 4 + 0 * dsplit; }
 __host__ __device__ constexpr int smem_bytes(int tm, int tn, int passes, int stages, int dsplit = 0, int kc = kKC) {
   return stages * stage_bytes_of(tm, tn, passes, kc) + staging_bytes(dsplit) + 1024;
 }

@@ -6,7 +6,8 @@ the error of a plain FP32 product of the same inputs (torch, TF32 off), and at m
 1 pass (TF32 operands) 4e-3.  Shapes cover the sweep's uses: a shared trial operand with walkers
 stacked along N (M = 256, K = 512), per-walker operands with M = 64 (half-datapath accumulator
 layout), padding of M, N and K to whole tiles, an operand shared by pairs of batch entries,
-row- and column-major outputs, and accumulation."""
+row- and column-major outputs (written through shared-memory boxes and TMA bulk stores when
+nothing accumulates), and accumulation."""
 import numpy as np
 import pytest
 
@@ -105,3 +106,8 @@ def test_tc_gemm_matches_fp64(case, passes):
 def test_tc_gemm_alpha_beta_and_layouts(colmajor):
     assert fp32_accurate(*run_case(128, 64, 64, 5, 1, 1, 1, 3, alpha=0.5, beta=1, colmajor=colmajor))
     assert fp32_accurate(*run_case(256, 32, 256, 8, 0, 1, 8, 3, alpha=-2.0, beta=1, colmajor=colmajor))
+    # without accumulation the epilogue writes through TMA bulk stores (32-column boxes where the
+    # tile allows, 16-column ones otherwise)
+    assert fp32_accurate(*run_case(128, 64, 64, 5, 1, 1, 1, 3, alpha=0.5, beta=0, colmajor=colmajor))
+    assert fp32_accurate(*run_case(256, 32, 256, 8, 0, 1, 8, 3, alpha=-2.0, beta=0, colmajor=colmajor))
+    assert fp32_accurate(*run_case(64, 48, 32, 7, 1, 1, 1, 3, alpha=1.5, beta=0, colmajor=colmajor))
