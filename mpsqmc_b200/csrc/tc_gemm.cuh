@@ -591,7 +591,47 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           ++nbox;
         }
       }
-      for (int c0 = 0; c0 < (dwide || rtma ? 0 : tn); c0 += 16) {
+      // closures with contiguous, aligned rows of E, 32 columns per step that stay in one entry
+      const bool dot_wide = dot4 && e_vec && (tn & 31) == 0 && (bstack == 1 || (N & 31) == 0);
+      if (dot_wide) {
+        for (int c0 = 0; c0 < tn; c0 += 32) {
+          float v[32];
+          __syncwarp();
+          tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * tn + c0), v);
+          int z, n;
+          col(c0, z0, n0, z, n);
+          if (z < 0 || z >= Zt || n >= N) break;  // later steps are past the entries too
+          if (z != zlast) {
+            if (zlast >= 0) flush(zlast);
+            zlast = z;
+          }
+          if (!mrow) continue;
+          const float *e = E + (long)z * ez + (long)m * em + (long)n;
+          if (n + 32 <= N) {
+#pragma unroll
+            for (int i4 = 0; i4 < 8; ++i4) {
+              float4 ev[4];
+#pragma unroll
+              for (int qq = 0; qq < 4; ++qq) ev[qq] = __ldg(reinterpret_cast<const float4 *>(e + qq * eq) + i4);
+              const double x0 = (double)(alpha * v[4 * i4]), x1 = (double)(alpha * v[4 * i4 + 1]),
+                           x2 = (double)(alpha * v[4 * i4 + 2]), x3 = (double)(alpha * v[4 * i4 + 3]);
+              ds0 += x0 * (double)ev[0].x + x1 * (double)ev[0].y + x2 * (double)ev[0].z + x3 * (double)ev[0].w;
+              ds1 += x0 * (double)ev[1].x + x1 * (double)ev[1].y + x2 * (double)ev[1].z + x3 * (double)ev[1].w;
+              ds2 += x0 * (double)ev[2].x + x1 * (double)ev[2].y + x2 * (double)ev[2].z + x3 * (double)ev[2].w;
+              ds3 += x0 * (double)ev[3].x + x1 * (double)ev[3].y + x2 * (double)ev[3].z + x3 * (double)ev[3].w;
+            }
+          } else {
+            for (int i = 0; i < 32 && n + i < N; ++i) {
+              float x = v[0];
+#pragma unroll
+              for (int j = 1; j < 32; ++j)
+                if (j == i) x = v[j];  // v[i] without an indexed (local-memory) register array
+              accum((double)(alpha * x), e + i);
+            }
+          }
+        }
+      }
+      for (int c0 = 0; c0 < (dwide || rtma || dot_wide ? 0 : tn); c0 += 16) {
         float v[16];
         __syncwarp();  // tcgen05.ld is warp-collective
         tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * tn + c0), v);
