@@ -251,10 +251,12 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
                                       *   products */
 #define MPSQMC_OPT_TC_STAGES 13       /*   load-ring depth cap, 2..8 (fewer when shared memory is
                                       *   short; default 8) */
-#define MPSQMC_OPT_TC_SPLIT_OUT 14    /*   0 (default) / 1: with three passes, the walker-side right
-                                      *   factors of the trial products are written as TF32 head
-                                      *   and tail arrays and loaded split (the trial itself always
-                                      *   is), instead of being split in shared memory */
+#define MPSQMC_OPT_TC_SPLIT_OUT 14    /*   mask 0..31 (default 0): with three passes, the classes
+                                      *   of walker-side right factors of the trial products that
+                                      *   are written as TF32 head and tail arrays and loaded split
+                                      *   (the trial itself always is) instead of being split in
+                                      *   shared memory: 1 right environments and closures, 2 left
+                                      *   branches, 4 branch carries, 8 energy, 16 energy channels */
 #define MPSQMC_OPT_TC_KC 15           /*   k-values per load stage of the trial products: 32
                                       *   (default, 128-byte swizzled rows) or 16 (64-byte rows:
                                       *   half the stage, twice the ring depth) */

@@ -768,8 +768,12 @@ size_t bytes_needed(const Problem &pr) {
   const long szBl = pad64(maxA * ldB), szX = pad64(2 * maxB * ldA), szN = pad64(maxB * ldB), szW = pad64(2 * maxB * ldB);
   const int ns = std::max(1, pr.nslots);
   per += szBl * (1 + 4 + 2 + 2 + 3L * ns) + szX * (1 + 4 + 1 + 3L * ns) + 2 * szN + szW + pad64(2 * maxB * ldA);
-  if (pr.passes == 3 && pr.tiles.split_out)
-    per += szX * (1 + 4 + 1 + 3L * ns) + pad64(2 * maxB * ldA);  // tails of the right factors
+  if (pr.passes == 3) {  // tails of the right factors stored split
+    const int sb = pr.tiles.split_out;
+    per += szX * (((sb & kSplitY) ? 1 : 0) + ((sb & kSplitX) ? 1 : 0) + ((sb & kSplitX4) ? 4 : 0) +
+                  ((sb & kSplitXch) ? 3L * ns : 0)) +
+           ((sb & kSplitQ) ? pad64(2 * maxB * ldA) : 0);
+  }
   return (size_t)per * pr.capacity * sizeof(float) + (size_t)pr.capacity * 48 * sizeof(double);
 }
 
@@ -902,10 +906,14 @@ int build(const Problem &pr, Plan **out) {
         palloc(p, &p->Fd[1], p->szBl * cap) | palloc(p, &p->Gb, 2 * p->szBl * cap) |
         palloc(p, &p->Q, pad64(2 * maxB * p->ldA) * cap) | palloc(p, &p->Fch, 3L * ns * p->szBl * cap) |
         palloc(p, &p->Xch, 3L * ns * p->szX * cap);
-  const bool split_b = split && pr.tiles.split_out;  // right factors written split
-  if (split_b)
-    rc |= palloc(p, &p->Xl, p->szX * cap) | palloc(p, &p->X4l, 4 * p->szX * cap) | palloc(p, &p->Yl, p->szX * cap) |
-          palloc(p, &p->Ql, pad64(2 * maxB * p->ldA) * cap) | palloc(p, &p->Xchl, 3L * ns * p->szX * cap);
+  // right factors written split, by class (bits of Tiles::split_out): the tails' arrays exist
+  // only for the classes that are
+  const int sb = split ? pr.tiles.split_out : 0;
+  if (sb & kSplitY) rc |= palloc(p, &p->Yl, p->szX * cap);
+  if (sb & kSplitX) rc |= palloc(p, &p->Xl, p->szX * cap);
+  if (sb & kSplitX4) rc |= palloc(p, &p->X4l, 4 * p->szX * cap);
+  if (sb & kSplitQ) rc |= palloc(p, &p->Ql, pad64(2 * maxB * p->ldA) * cap);
+  if (sb & kSplitXch) rc |= palloc(p, &p->Xchl, 3L * ns * p->szX * cap);
   rc |= palloc(p, &p->ovb, cap) | palloc(p, &p->wtb, cap) | palloc(p, &p->scl, cap) | palloc(p, &p->ob, 8 * cap) |
         palloc(p, &p->dot, 16 * cap) | palloc(p, &p->err_tc, 1) | palloc(p, &p->nb, 1);
   if (rc) return bail(MPSQMC_E_CUDA);
@@ -959,8 +967,8 @@ int build(const Problem &pr, Plan **out) {
   auto TOso = [P, Tr](int k) { return Tr(P->TOs, P->ntos, P->tos_off[k], 2 * P->ldA, P->pr.aT[k + 1]); };
   auto TTso = [P, Tr](int k) { return Tr(P->TTs, P->ntts, P->tts_off[k], 2 * P->ldA, P->pr.aT[k]); };
   // a right factor written as heads (base) with its tails at the same offset of `tails`
-  auto Sp = [split_b](Opnd o, const float *heads, const float *tails) {
-    if (split_b) {
+  auto Sp = [](Opnd o, const float *heads, const float *tails) {
+    if (tails) {
       o.hi = o.base;
       o.lo = tails + (o.base - heads);
     }

@@ -13,6 +13,11 @@
 namespace mq {
 namespace bs {
 
+// Classes of right factors that may be stored split (Tiles::split_out bits): Y (right
+// environments and closures), X (left branches), X4 (branch carries), Q (energy), Xch (energy
+// channels).
+constexpr int kSplitY = 1, kSplitX = 2, kSplitX4 = 4, kSplitQ = 8, kSplitXch = 16, kSplitAll = 31;
+
 // Tile choices of the plan's products (what the autotuner varies per bond-profile bucket).
 struct Tiles {
   int stack_tn = 256;   // widest N tile of products whose A (a trial tensor) is shared: walkers are
@@ -22,9 +27,10 @@ struct Tiles {
   int max_stages = 8;   // load-ring depth cap (2 .. 8; fewer when shared memory is short)
   int kc_trial = 32;    // k-values per stage of the trial products (32, or 16: half the stage
                         // and twice the ring depth)
-  int split_out = 0;    // three passes: 1 = the right factors of the trial products are written as
-                        // TF32 head and tail arrays and loaded split (no conversion in the trial
-                        // products, twice the bytes written by their producers)
+  int split_out = 0;    // three passes: bits (kSplit*) of the classes of right factors of the trial
+                        // products that are written as TF32 head and tail arrays and loaded
+                        // split (no conversion in their consumers, twice the bytes written by
+                        // their producers)
   bool operator==(const Tiles &o) const {
     return stack_tn == o.stack_tn && wide_tn == o.wide_tn && max_stages == o.max_stages && split_out == o.split_out &&
            kc_trial == o.kc_trial;

@@ -1527,17 +1527,16 @@ int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspa
     // width, 3 the walker products' tile width, 4 ring depth cap
     for (int axis = 0; axis < 5 && !rc; ++axis) {
       if (axis == 0 && c->precision == MPSQMC_PRECISION_TF32_TC) continue;  // one pass: nothing to split
-      const std::vector<int> vals = axis == 0   ? std::vector<int>{1}
+      const std::vector<int> vals = axis == 0   ? std::vector<int>{mq::bs::kSplitX4, mq::bs::kSplitXch, mq::bs::kSplitY,
+                                                                 mq::bs::kSplitX, mq::bs::kSplitQ}
                                     : axis == 1 ? std::vector<int>{16}
                                     : axis == 4 ? std::vector<int>{4, 2}
                                                 : std::vector<int>{128, 64};
       for (int v : vals) {
         Tuned cd = choice;
-        (axis == 0   ? cd.tiles.split_out
-         : axis == 1 ? cd.tiles.kc_trial
-         : axis == 2 ? cd.tiles.stack_tn
-         : axis == 3 ? cd.tiles.wide_tn
-                     : cd.tiles.max_stages) = v;
+        if (axis == 0) cd.tiles.split_out |= v;  // one class of right factors more, stored split
+        else (axis == 1 ? cd.tiles.kc_trial : axis == 2 ? cd.tiles.stack_tn : axis == 3 ? cd.tiles.wide_tn
+                                                                                      : cd.tiles.max_stages) = v;
         double per = 0.0;
         if ((rc = trial(cd, &per))) break;
         if (per < best) best = per, choice = cd;
@@ -1555,6 +1554,12 @@ int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspa
   }
   if (rr) return rr;
   drop_graphs(c);  // captured with the subset's population size
+  if (tc && c->bplan) {
+    // the trials' plans were sized for the measured subset: the next walk builds one for the
+    // population's own target
+    mq::bs::destroy(c->bplan);
+    c->bplan = nullptr;
+  }
   rc = apply_tuned(c, choice);
   if (rc) return rc;
   {
@@ -1697,7 +1702,7 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
       c->tc_tiles.max_stages = (int)value;
       break;
     case MPSQMC_OPT_TC_SPLIT_OUT:
-      if (value != 0 && value != 1) return fail(MPSQMC_E_ARG, "split outputs are 0 or 1");
+      if (value < 0 || value > mq::bs::kSplitAll) return fail(MPSQMC_E_ARG, "split outputs are a mask 0..31");
       c->tc_tiles.split_out = (int)value;
       break;
     case MPSQMC_OPT_TC_KC:

@@ -107,7 +107,7 @@ def test_tc_tile_choices_give_the_same_walk():
     z = load_golden("walk_snake4x4_D16_DW8_branch")
     a = engine_for(z, PRECISION_TF32X3_TC)
     b = engine_for(z, PRECISION_TF32X3_TC)
-    for opt, v in ((OPT_TC_STACK_TN, 64), (OPT_TC_WIDE_TN, 128), (OPT_TC_STAGES, 2), (OPT_TC_SPLIT_OUT, 1),
+    for opt, v in ((OPT_TC_STACK_TN, 64), (OPT_TC_WIDE_TN, 128), (OPT_TC_STAGES, 2), (OPT_TC_SPLIT_OUT, 31),
                    (OPT_TC_KC, 16)):
         b.set_option(opt, v)
         assert b.get_option(opt) == v
@@ -133,7 +133,7 @@ def test_tc_autotune_picks_valid_tiles_and_keeps_the_walk():
     assert b.get_option(OPT_TC_WIDE_TN) in (64, 128, 256)
     assert b.get_option(OPT_TC_STAGES) in (2, 4, 8)
     assert b.get_option(OPT_TC_KC) in (16, 32)
-    assert b.get_option(OPT_TC_SPLIT_OUT) in (0, 1)
+    assert 0 <= b.get_option(OPT_TC_SPLIT_OUT) <= 31
     sa, sb = a.walk(2), b.walk(2)
     for x, y in zip(sa, sb):
         assert x["n_walkers"] == y["n_walkers"]
