@@ -615,8 +615,10 @@ struct Plan {
   // FP32 trial copies: TO_k[s] rows c < a_{k+1}, k = r (ld pad4(a_k)); TT_k[s] rows r < a_k, k = c
   std::vector<long> to_off, tt_off;  // per (k, s): k * 2 + s
   float *TO = nullptr, *TT = nullptr;
-  // the same with sigma stacked along K (blocks of ldA): TOs_k[c][s ldA + r] = B_k[s](r, c),
-  // TTs_k[r][s ldA + c] = B_k[s](r, c); zero beyond the site's bond
+  // the same with sigma stacked along K in blocks of the contracted bond padded to 4 (so that K =
+  // 2 pad4(bond) at every site, not twice the largest bond): TOs_k[c][s l + r] = B_k[s](r, c)
+  // with l = pad4(a_k), TTs_k[r][s l' + c] = B_k[s](r, c) with l' = pad4(a_{k+1}); zero beyond
+  // the site's bond
   std::vector<long> tos_off, tts_off;  // per k
   float *TOs = nullptr, *TTs = nullptr;
   // walker forms and right environments
@@ -819,9 +821,9 @@ int build(const Problem &pr, Plan **out) {
   long ntos = 0, ntts = 0;
   for (int k = 0; k < L; ++k) {
     p->tos_off[k] = ntos;
-    ntos += pad64((long)a[k + 1] * 2 * p->ldA);
+    ntos += pad64((long)a[k + 1] * 2 * pad4(a[k]));
     p->tts_off[k] = ntts;
-    ntts += pad64((long)a[k] * 2 * p->ldA);
+    ntts += pad64((long)a[k] * 2 * pad4(a[k + 1]));
   }
   p->nto = nto;
   p->ntt = ntt;
@@ -838,7 +840,6 @@ int build(const Problem &pr, Plan **out) {
     if (cudaMemcpy(tr.data(), pr.trial, sizeof(double) * tot, cudaMemcpyDeviceToHost) != cudaSuccess)
       return bail(fail(MPSQMC_E_CUDA, "batched sweep: trial download failed"));
     std::vector<float> to(nto, 0.f), tt(ntt, 0.f), tos(ntos, 0.f), tts(ntts, 0.f);
-    const long l2 = 2 * p->ldA;
     for (int k = 0; k < L; ++k)
       for (int s = 0; s < 2; ++s) {
         const long lo = pad4(a[k]), lt = pad4(a[k + 1]);
@@ -847,8 +848,8 @@ int build(const Problem &pr, Plan **out) {
             const float x = (float)tr[pr.toff[k] + r + (long)a[k] * (c + (long)a[k + 1] * s)];
             to[p->to_off[2 * k + s] + c * lo + r] = x;
             tt[p->tt_off[2 * k + s] + (long)r * lt + c] = x;
-            tos[p->tos_off[k] + c * l2 + s * p->ldA + r] = x;
-            tts[p->tts_off[k] + (long)r * l2 + s * p->ldA + c] = x;
+            tos[p->tos_off[k] + c * 2 * lo + s * lo + r] = x;
+            tts[p->tts_off[k] + (long)r * 2 * lt + s * lt + c] = x;
           }
       }
     // sections: values, then (three passes) heads x rounded to TF32 and tails (x - head) rounded
@@ -964,8 +965,8 @@ int build(const Problem &pr, Plan **out) {
   };
   auto TOo = [P, Tr](int k, int s) { return Tr(P->TO, P->nto, P->to_off[2 * k + s], pad4(P->pr.aT[k]), P->pr.aT[k + 1]); };
   auto TTo = [P, Tr](int k, int s) { return Tr(P->TT, P->ntt, P->tt_off[2 * k + s], pad4(P->pr.aT[k + 1]), P->pr.aT[k]); };
-  auto TOso = [P, Tr](int k) { return Tr(P->TOs, P->ntos, P->tos_off[k], 2 * P->ldA, P->pr.aT[k + 1]); };
-  auto TTso = [P, Tr](int k) { return Tr(P->TTs, P->ntts, P->tts_off[k], 2 * P->ldA, P->pr.aT[k]); };
+  auto TOso = [P, Tr](int k) { return Tr(P->TOs, P->ntos, P->tos_off[k], 2 * pad4(P->pr.aT[k]), P->pr.aT[k + 1]); };
+  auto TTso = [P, Tr](int k) { return Tr(P->TTs, P->ntts, P->tts_off[k], 2 * pad4(P->pr.aT[k + 1]), P->pr.aT[k]); };
   // a right factor written as heads (base) with its tails at the same offset of `tails`
   auto Sp = [](Opnd o, const float *heads, const float *tails) {
     if (tails) {
@@ -974,15 +975,18 @@ int build(const Problem &pr, Plan **out) {
     }
     return o;
   };
-  const long l2 = 2 * p->ldA;  // K of the sigma-stacked trial products
+  const long l2 = 2 * p->ldA;  // row stride of the unstacked right factors (X, Y as read by T3_P, T_dot)
+  // sigma stride of a stacked right factor whose rows run over the trial bond a_k (K = 2 ls(k))
+  auto ls = [&](int k) { return pad4((long)a[k]); };
   // right environment R_k from R_{k+1}: Y = R_{k+1} SR_k^T (rows (r, s)), then
   // R_k = sum_s TT_k[s] Y_s as one product with s stacked along K
   auto right_env = [&](int k) -> int {
-    int r = add_gemm(p, Ro(k + 1), SRo(k), a[k + 1], 2 * b[k], b[k + 1], 1, p->Y, p->szX, 1, p->ldA, 0, 1.f, nullptr, 0,
+    int r = add_gemm(p, Ro(k + 1), SRo(k), a[k + 1], 2 * b[k], b[k + 1], 1, p->Y, p->szX, 1, ls(k + 1), 0, 1.f, nullptr, 0,
                      0, 0, 0, 0, p->Yl);
     if (!r) {
-      const Opnd Yr = Sp(Opnd{p->Y, l2, b[k], p->szX, cap, 1}, p->Y, p->Yl);
-      r = add_gemm(p, TTso(k), Yr, a[k], b[k], (int)l2, 1, p->R + p->r_off[k], p->r_sz[k], p->r_ld[k], 1, 0);
+      const Opnd Yr = Sp(Opnd{p->Y, 2 * ls(k + 1), b[k], p->szX, cap, 1}, p->Y, p->Yl);
+      r = add_gemm(p, TTso(k), Yr, a[k], b[k], (int)(2 * ls(k + 1)), 1, p->R + p->r_off[k], p->r_sz[k], p->r_ld[k], 1,
+                   0);
     }
     return r;
   };
@@ -1004,11 +1008,11 @@ int build(const Problem &pr, Plan **out) {
     Opnd Pq{p->P, p->ldB, a[m], p->szBl, 4L * cap, 1};
     Opnd S = SLo(m);
     S.div = 4;
-    int r = add_gemm(p, Pq, S, a[m], 2 * b[m + 1], b[m], 4, p->X4, p->szX, 1, p->ldA, 0, 1.f, nullptr, 0, 0, 0, 0, 0,
+    int r = add_gemm(p, Pq, S, a[m], 2 * b[m + 1], b[m], 4, p->X4, p->szX, 1, ls(m), 0, 1.f, nullptr, 0, 0, 0, 0, 0,
                      p->X4l);
     if (!r) {
-      const Opnd Xr = Sp(Opnd{p->X4, l2, b[m + 1], p->szX, 4L * cap, 1}, p->X4, p->X4l);
-      r = add_gemm(p, TOso(m), Xr, a[m + 1], b[m + 1], (int)l2, 4, p->P, p->szBl, p->ldB, 1, 0);
+      const Opnd Xr = Sp(Opnd{p->X4, 2 * ls(m), b[m + 1], p->szX, 4L * cap, 1}, p->X4, p->X4l);
+      r = add_gemm(p, TOso(m), Xr, a[m + 1], b[m + 1], (int)(2 * ls(m)), 4, p->P, p->szBl, p->ldB, 1, 0);
     }
     return r;
   };
@@ -1163,12 +1167,12 @@ int build(const Problem &pr, Plan **out) {
           p->launches += 1;
           Opnd Gr{p->Gb, 2 * ldl, ai, 2 * p->szBl, cap, 1};
           Opnd Cr{p->SL + p->sl_off[i], 2 * ldl, bi1, p->sl_sz[i], cap, 1};
-          rc = add_gemm(p, Gr, Cr, ai, bi1, (int)(2 * ldl), 1, p->Q + (long)s * p->ldA, szQ, 1, l2, 0, 1.f, nullptr, 0,
-                        0, 0, 0, 0, p->Ql ? p->Ql + (long)s * p->ldA : nullptr);
+          rc = add_gemm(p, Gr, Cr, ai, bi1, (int)(2 * ldl), 1, p->Q + s * ls(i), szQ, 1, 2 * ls(i), 0, 1.f, nullptr, 0,
+                        0, 0, 0, 0, p->Ql ? p->Ql + s * ls(i) : nullptr);
           if (rc) return bail(rc);
         }
-        const Opnd Qr = Sp(Opnd{p->Q, l2, bi1, szQ, cap, 1}, p->Q, p->Ql);
-        rc = add_gemm(p, TOso(i), Qr, ai1, bi1, (int)l2, 1, Fdn, p->szBl, p->ldB, 1, 0);
+        const Opnd Qr = Sp(Opnd{p->Q, 2 * ls(i), bi1, szQ, cap, 1}, p->Q, p->Ql);
+        rc = add_gemm(p, TOso(i), Qr, ai1, bi1, (int)(2 * ls(i)), 1, Fdn, p->szBl, p->ldB, 1, 0);
         if (rc) return bail(rc);
         if (q.h != 0.0) field_term(1);
       }
@@ -1178,11 +1182,11 @@ int build(const Problem &pr, Plan **out) {
         Opnd Fo{p->Fch, p->ldB, a[i], p->szBl, 3L * ns * cap, 1};
         Opnd S = SLo(i);
         S.div = 3 * ns;
-        rc = add_gemm(p, Fo, S, a[i], 2 * bi1, b[i], 3 * ns, p->Xch, p->szX, 1, p->ldA, 0, 1.f, nullptr, 0, 0, 0, 0, 0,
+        rc = add_gemm(p, Fo, S, a[i], 2 * bi1, b[i], 3 * ns, p->Xch, p->szX, 1, ls(i), 0, 1.f, nullptr, 0, 0, 0, 0, 0,
                       p->Xchl);
         if (!rc) {
-          const Opnd Xr = Sp(Opnd{p->Xch, l2, bi1, p->szX, 3L * ns * cap, 1}, p->Xch, p->Xchl);
-          rc = add_gemm(p, TOso(i), Xr, ai1, bi1, (int)l2, 3 * ns, p->Fch, p->szBl, p->ldB, 1, 0);
+          const Opnd Xr = Sp(Opnd{p->Xch, 2 * ls(i), bi1, p->szX, 3L * ns * cap, 1}, p->Xch, p->Xchl);
+          rc = add_gemm(p, TOso(i), Xr, ai1, bi1, (int)(2 * ls(i)), 3 * ns, p->Fch, p->szBl, p->ldB, 1, 0);
         }
         if (rc) return bail(rc);
       }

@@ -215,6 +215,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float *v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Eight consecutive FP32 values through the read-only path in one 32-byte access (p 32-byte
+// aligned): a lane reads whole sectors.
+__device__ __forceinline__ void ldg_v8(const float *p, float *r) {
+  asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]), "=f"(r[7])
+               : "l"(p));
+}
+
 __device__ __forceinline__ void tmem_ld32(uint32_t addr, float *v) {
   uint32_t r[32];
   asm volatile(
@@ -523,6 +531,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     // E rows read as 16-byte vectors when they are contiguous and aligned (chunks start at
     // columns that are multiples of 16)
     const bool e_vec = dot4 && en == 1 && ((ez | eq | em) & 3) == 0 && (reinterpret_cast<uintptr_t>(E) & 15) == 0;
+    const bool e_v8 = e_vec && ((ez | eq | em) & 7) == 0 && (reinterpret_cast<uintptr_t>(E) & 31) == 0;
     int acc = 0;
     uint32_t aph = 0;
     for (int tile = blockIdx.x; tile < t.total; tile += gridDim.x) {
@@ -607,7 +616,25 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           }
           if (!mrow) continue;
           const float *e = E + (long)z * ez + (long)m * em + (long)n;
-          if (n + 32 <= N) {
+          if (e_v8 && n + 32 <= N) {
+            // whole 32-byte sectors per lane: the rows of E a warp reads are 256 bytes apart,
+            // and L1 beside the stage ring is too small to keep half-read sectors
+#pragma unroll
+            for (int i8 = 0; i8 < 4; ++i8) {
+#pragma unroll
+              for (int qq = 0; qq < 4; ++qq) {
+                float ev[8];
+                ldg_v8(e + qq * eq + 8 * i8, ev);
+                double d = 0.0;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) d += (double)(alpha * v[8 * i8 + j]) * (double)ev[j];
+                if (qq == 0) ds0 += d;
+                else if (qq == 1) ds1 += d;
+                else if (qq == 2) ds2 += d;
+                else ds3 += d;
+              }
+            }
+          } else if (n + 32 <= N) {
 #pragma unroll
             for (int i4 = 0; i4 < 8; ++i4) {
               float4 ev[4];

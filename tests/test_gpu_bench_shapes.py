@@ -96,3 +96,35 @@ def test_bench_shape_step_matches_oracle(case, precision):
         for k in ("weight", "overlap", "energy"):
             assert lw[k][w] == pytest.approx(r[k], rel=tol), (case, w, k)
     eng.close()
+
+
+def test_tc_sweep_follows_the_fp64_walk_at_the_headline_shape():
+    """Config 5's shapes (8x8 lattice, D_T = 256 trial, D_W = 64): from the same start and random
+    stream, the tcgen05 sweep's population follows the FP64 sweep's step by step and its E_P stays
+    within half the energy criterion (1e-4 J per site) of the FP64 value.  The three-pass products
+    are FP32-accurate per term; through the 64-site chains of contractions the local energies
+    carry about 1e-5 relative rounding (2.8e-5 relative, 1.7e-5 J per site, measured on E_P)."""
+    wl = workloads.snake8x8(Nw=64) if workloads.snake8x8().has_trial() else workloads.snake8x8_random(Nw=64)
+    ci, cj, cJ = wl.couplings()
+    trial = wl.trial()
+    U, S, VT = pb.trotter_tables(1.0, wl.dtau)
+    N = 64
+    inputs = dict(L=wl.L, ci=ci, cj=cj, cJ=cJ, h=0.0, dtau=wl.dtau, trial_dims=trial.dims, trial=trial.data,
+                  Jvals=[1.0], U=U, S=S, VT=VT, grid=pb.grid_marsaglia(4, 4), Ndesired=N, capacity=256)
+    w = pb.compress(trial, 64)
+    rng = np.random.default_rng(3)
+    start = w.data[None, :] + 1e-3 * rng.normal(size=(N, w.data.size))
+    runs = []
+    for precision in (PRECISION_FP64, PRECISION_TF32X3_TC):
+        eng = Engine(walker_dims=w.dims, **inputs)
+        eng.set_walkers(start, np.ones(N), normalize=True)
+        eng.set_option(OPT_PRECISION, precision)
+        eng.set_rng(SEED, 0)
+        runs.append(eng.walk(4))
+        eng.close()
+    for step, (x, y) in enumerate(zip(*runs)):
+        print(f"step {step}: E_P {x['E_P']:.10f} / {y['E_P']:.10f}, per site {abs(y['E_P'] - x['E_P']) / wl.L:.2e}, "
+              f"sum w rel {abs(y['sum_weight'] / x['sum_weight'] - 1):.2e}")
+        assert x["n_walkers"] == y["n_walkers"]
+        assert abs(y["E_P"] - x["E_P"]) / wl.L < 5e-5
+        assert y["sum_weight"] == pytest.approx(x["sum_weight"], rel=1e-4)

@@ -140,3 +140,23 @@ def test_tc_autotune_picks_valid_tiles_and_keeps_the_walk():
         assert x["E_P"] == pytest.approx(y["E_P"], rel=1e-6)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("mask", [1, 2, 4, 8, 16])
+def test_tc_each_split_class_gives_the_same_step(mask):
+    """Each class of right factors stored as TF32 head and tail arrays (right environments and
+    closures, left branches, carries, energy, channels) on its own: the step agrees with the
+    default (every right factor split in shared memory) to FP32 rounding."""
+    z = load_golden("walk_snake4x4_D16_DW8_branch")
+    a = engine_for(z, PRECISION_TF32X3_TC)
+    b = engine_for(z, PRECISION_TF32X3_TC)
+    b.set_option(OPT_TC_SPLIT_OUT, mask)
+    sa, sb = a.walk(2), b.walk(2)
+    for x, y in zip(sa, sb):
+        assert x["n_walkers"] == y["n_walkers"]
+        assert x["E_P"] == pytest.approx(y["E_P"], rel=1e-6)
+    la, lb = a.last_step_walkers(), b.last_step_walkers()
+    for k in ("weight", "overlap", "energy"):
+        assert np.max(rel(lb[k], la[k])) < 1e-6, k
+    a.close()
+    b.close()
