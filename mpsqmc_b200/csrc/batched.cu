@@ -268,8 +268,20 @@ struct SiteForms {          // device tables, one entry per site
 // FP64 walker sites -> the two FP32 forms: SL_k[(2c + s) ldl + r] (rows (c, sigma), k = the left
 // bond) and SR_k[(2r + s) ldr + c] (rows (r, sigma), k = the right bond).  Interleaving sigma in the
 // rows lets the sums over sigma of the trial products run as one product with sigma stacked along K.
+// One element of a site form from the FP64 walker: its FP32 value, or (tail != 0, three passes)
+// its TF32 head at p[i] and the TF32 rounding of what the head misses at p[tail + i].
+__device__ __forceinline__ void put_form(float *p, long tail, long i, double y) {
+  if (!tail) {
+    p[i] = (float)y;
+    return;
+  }
+  const float h = to_tf32((float)y);
+  p[i] = h;
+  p[tail + i] = to_tf32((float)(y - (double)h));
+}
+
 __global__ void convert_kernel(SiteForms f, const double *walkers, long wstride, const int *slot_of, const int *n_cur,
-                               int cap, float *SL, float *SR) {
+                               int cap, float *SL, float *SR, long slt, long srt) {
   const int k = blockIdx.y;
   const int N = min(*n_cur, cap);
   const int bl = f.bl[k], br = f.br[k];
@@ -280,8 +292,8 @@ __global__ void convert_kernel(SiteForms f, const double *walkers, long wstride,
     const long q = e % per;
     const int r = (int)(q % bl), c = (int)((q / bl) % br), s = (int)(q / ((long)bl * br));
     const double x = walkers[(long)slot_of[w] * wstride + f.woff[k] + q];
-    SL[f.sl_off[k] + (long)w * f.sl_sz[k] + (2L * c + s) * ldl + r] = (float)x;
-    SR[f.sr_off[k] + (long)w * f.sr_sz[k] + (2L * r + s) * ldr + c] = (float)x;
+    put_form(SL, slt, f.sl_off[k] + (long)w * f.sl_sz[k] + (2L * c + s) * ldl + r, x);
+    put_form(SR, srt, f.sr_off[k] + (long)w * f.sr_sz[k] + (2L * r + s) * ldr + c, x);
   }
 }
 
@@ -401,7 +413,8 @@ __global__ void __launch_bounds__(128) sample_kernel(const double *dot, const do
 // O1 (ob[0..3]) on site i and O2 (ob[4..7]) on site j of every walker: the FP64 slot and both FP32
 // forms.  blockIdx.y = 0: site i, 1: site j.
 __global__ void site_op_kernel(SiteForms f, int si, int sj, const double *ob, double *walkers, long wstride,
-                               const int *slot_of, const int *n_cur, int cap, float *SL, float *SR) {
+                               const int *slot_of, const int *n_cur, int cap, float *SL, float *SR, long slt,
+                               long srt) {
   const int k = blockIdx.y == 0 ? si : sj;
   const int oo = blockIdx.y == 0 ? 0 : 4;
   const int N = min(*n_cur, cap);
@@ -420,17 +433,17 @@ __global__ void site_op_kernel(SiteForms f, int si, int sj, const double *ob, do
     X[blk + q] = y1;
     float *sl = SL + f.sl_off[k] + (long)w * f.sl_sz[k];
     float *sr = SR + f.sr_off[k] + (long)w * f.sr_sz[k];
-    sl[2L * c * ldl + r] = (float)y0;
-    sl[(2L * c + 1) * ldl + r] = (float)y1;
-    sr[2L * r * ldr + c] = (float)y0;
-    sr[(2L * r + 1) * ldr + c] = (float)y1;
+    put_form(sl, slt, 2L * c * ldl + r, y0);
+    put_form(sl, slt, (2L * c + 1) * ldl + r, y1);
+    put_form(sr, srt, 2L * r * ldr + c, y0);
+    put_form(sr, srt, (2L * r + 1) * ldr + c, y1);
   }
 }
 
 // QR-free sweep: the finished centre (site i) rescaled to the Frobenius norm of an isometry,
 // sqrt(b_r); the overlap takes the same factor (walker_general.cuh).  One block per walker.
 __global__ void rescale_kernel(SiteForms f, int k, double *walkers, long wstride, const int *slot_of, const int *n_cur,
-                               int cap, float *SL, float *SR, double *ovb, double *scl) {
+                               int cap, float *SL, float *SR, long slt, long srt, double *ovb, double *scl) {
   __shared__ double red[8];
   const int w = blockIdx.x;
   if (w >= min(*n_cur, cap)) return;
@@ -452,8 +465,8 @@ __global__ void rescale_kernel(SiteForms f, int k, double *walkers, long wstride
     const double y = X[q] * inv;
     X[q] = y;
     const int r = (int)(q % bl), c = (int)((q / bl) % br), s = (int)(q / ((long)bl * br));
-    sl[(2L * c + s) * ldl + r] = (float)y;
-    sr[(2L * r + s) * ldr + c] = (float)y;
+    put_form(sl, slt, (2L * c + s) * ldl + r, y);
+    put_form(sr, srt, (2L * r + s) * ldr + c, y);
   }
   if (threadIdx.x == 0) {
     ovb[w] *= inv;
@@ -624,6 +637,7 @@ struct Plan {
   // walker forms and right environments
   std::vector<long> sl_off, sr_off, sl_sz, sr_sz, sl_ld, sr_ld, r_off, r_sz, r_ld;
   float *SL = nullptr, *SR = nullptr, *R = nullptr;
+  long slt = 0, srt = 0;           // three passes: offset of the site forms' TF32 tails (0: FP32 values)
   // work buffers (per walker, fixed strides)
   long ldA = 0, ldB = 0;           // pad4(maxA), pad4(maxB)
   long szBl = 0;                   // maxA x ldB (a row-major a x b block)
@@ -763,8 +777,9 @@ size_t bytes_needed(const Problem &pr) {
   const long maxA = *std::max_element(pr.aT.begin(), pr.aT.end()), maxB = *std::max_element(pr.bW.begin(), pr.bW.end());
   const long ldA = pad4(maxA), ldB = pad4(maxB);
   long per = 0;  // floats per walker
+  const int forms = pr.passes == 3 ? 2 : 1;  // site forms as TF32 heads and tails with three passes
   for (int k = 0; k < L; ++k) {
-    per += pad64(2L * pr.bW[k + 1] * pad4(pr.bW[k])) + pad64(2L * pr.bW[k] * pad4(pr.bW[k + 1]));
+    per += forms * (pad64(2L * pr.bW[k + 1] * pad4(pr.bW[k])) + pad64(2L * pr.bW[k] * pad4(pr.bW[k + 1])));
     per += pad64((long)pr.aT[k + 1] * pad4(pr.bW[k + 1]));
   }
   const long szBl = pad64(maxA * ldB), szX = pad64(2 * maxB * ldA), szN = pad64(maxB * ldB), szW = pad64(2 * maxB * ldB);
@@ -900,7 +915,10 @@ int build(const Problem &pr, Plan **out) {
     p->r_off[k] = nr;
     nr += p->r_sz[k] * cap;
   }
-  rc = palloc(p, &p->SL, nsl) | palloc(p, &p->SR, nsr) | palloc(p, &p->R, nr);
+  // three passes: the site forms as TF32 heads with their tails nsl (nsr) floats further on
+  p->slt = split ? nsl : 0;
+  p->srt = split ? nsr : 0;
+  rc = palloc(p, &p->SL, (split ? 2 : 1) * nsl) | palloc(p, &p->SR, (split ? 2 : 1) * nsr) | palloc(p, &p->R, nr);
   rc |= palloc(p, &p->Lenv, p->szBl * cap) | palloc(p, &p->P, 4 * p->szBl * cap) | palloc(p, &p->X, p->szX * cap) |
         palloc(p, &p->X4, 4 * p->szX * cap) | palloc(p, &p->Y, p->szX * cap) | palloc(p, &p->Nl[0], p->szN * cap) |
         palloc(p, &p->Nl[1], p->szN * cap) | palloc(p, &p->Wn, p->szW * cap) | palloc(p, &p->Fd[0], p->szBl * cap) |
@@ -951,8 +969,20 @@ int build(const Problem &pr, Plan **out) {
   const int *ncur = q.n_cur;
   const int icap = p->cap;
   Plan *P = p;
-  auto SLo = [P](int k) { return Opnd{P->SL + P->sl_off[k], P->sl_ld[k], 2L * P->pr.bW[k + 1], P->sl_sz[k], P->cap, 1}; };
-  auto SRo = [P](int k) { return Opnd{P->SR + P->sr_off[k], P->sr_ld[k], 2L * P->pr.bW[k], P->sr_sz[k], P->cap, 1}; };
+  // a site form as an operand (with its TF32 tails when they are stored)
+  auto Fm = [](Opnd o, long tail) {
+    if (tail) {
+      o.hi = o.base;
+      o.lo = o.base + tail;
+    }
+    return o;
+  };
+  auto SLo = [P, Fm](int k) {
+    return Fm(Opnd{P->SL + P->sl_off[k], P->sl_ld[k], 2L * P->pr.bW[k + 1], P->sl_sz[k], P->cap, 1}, P->slt);
+  };
+  auto SRo = [P, Fm](int k) {
+    return Fm(Opnd{P->SR + P->sr_off[k], P->sr_ld[k], 2L * P->pr.bW[k], P->sr_sz[k], P->cap, 1}, P->srt);
+  };
   auto Ro = [P](int k) { return Opnd{P->R + P->r_off[k], P->r_ld[k], P->pr.aT[k], P->r_sz[k], P->cap, 1}; };
   // a trial copy, with its head and tail sections when they exist
   auto Tr = [P, split](const float *arr, long n, long off, long ld, long rows) {
@@ -1044,7 +1074,8 @@ int build(const Problem &pr, Plan **out) {
 
   // step start: FP32 forms of every walker, weights, unit environments
   p->ops.push_back([=](cudaStream_t s, double *) {
-    convert_kernel<<<dim3(gconv, L), 256, 0, s>>>(sf, q.walkers, q.wstride, q.slot_of, ncur, icap, P->SL, P->SR);
+    convert_kernel<<<dim3(gconv, L), 256, 0, s>>>(sf, q.walkers, q.wstride, q.slot_of, ncur, icap, P->SL, P->SR,
+                                                  P->slt, P->srt);
     init_kernel<<<(icap + 255) / 256, 256, 0, s>>>(q.weight, q.slot_of, ncur, icap, P->wtb, P->Lenv, P->szBl,
                                                    P->Nl[0], P->szN, P->R + P->r_off[L], P->r_sz[L], q.err, P->nb);
     return cudaGetLastError() == cudaSuccess ? 0 : fail(MPSQMC_E_CUDA, "batched sweep: start kernels");
@@ -1081,7 +1112,7 @@ int build(const Problem &pr, Plan **out) {
                                                      trace);
         const int g = (int)std::max(1L, std::min(8L * P->sms, ((long)std::max(b[i] * b[i + 1], b[j] * b[j + 1]) * icap + 255) / 256));
         site_op_kernel<<<dim3(g, 2), 256, 0, s>>>(sf, i, j, P->ob, q.walkers, q.wstride, q.slot_of, ncur, icap, P->SL,
-                                                  P->SR);
+                                                  P->SR, P->slt, P->srt);
         return cudaGetLastError() == cudaSuccess ? 0 : fail(MPSQMC_E_CUDA, "batched sweep: sampling");
       });
       p->launches += 2;
@@ -1091,7 +1122,8 @@ int build(const Problem &pr, Plan **out) {
     const int ai1 = a[i + 1], bi1 = b[i + 1];
     if (i < L - 1) {
       p->ops.push_back([=](cudaStream_t s, double *) {
-        rescale_kernel<<<icap, 256, 0, s>>>(sf, i, q.walkers, q.wstride, q.slot_of, ncur, icap, P->SL, P->SR, P->ovb,
+        rescale_kernel<<<icap, 256, 0, s>>>(sf, i, q.walkers, q.wstride, q.slot_of, ncur, icap, P->SL, P->SR, P->slt,
+                                            P->srt, P->ovb,
                                             P->scl);
         if (kept)
           derive_p_kernel<<<grid_elems(P, (long)ai1 * bi1), 256, 0, s>>>(P->P, P->szBl, P->ldB, ai1, bi1, P->ob,
@@ -1108,7 +1140,7 @@ int build(const Problem &pr, Plan **out) {
         Opnd Nlo{p->Nl[nl], p->ldB, b[i], p->szN, cap, 1};
         rc = add_gemm(p, Nlo, SLo(i), b[i], 2 * bi1, b[i], 1, p->Wn, p->szW, 1, ldl, 0);
         if (!rc) {
-          Opnd Ct{p->SL + p->sl_off[i], 2 * ldl, bi1, p->sl_sz[i], cap, 1};
+          const Opnd Ct = Fm(Opnd{p->SL + p->sl_off[i], 2 * ldl, bi1, p->sl_sz[i], cap, 1}, p->slt);
           Opnd Wr{p->Wn, 2 * ldl, bi1, p->szW, cap, 1};
           rc = add_gemm(p, Ct, Wr, bi1, bi1, (int)(2 * ldl), 1, p->Nl[1 - nl], p->szN, p->ldB, 1, 0);
         }
@@ -1166,7 +1198,7 @@ int build(const Problem &pr, Plan **out) {
           });
           p->launches += 1;
           Opnd Gr{p->Gb, 2 * ldl, ai, 2 * p->szBl, cap, 1};
-          Opnd Cr{p->SL + p->sl_off[i], 2 * ldl, bi1, p->sl_sz[i], cap, 1};
+          const Opnd Cr = Fm(Opnd{p->SL + p->sl_off[i], 2 * ldl, bi1, p->sl_sz[i], cap, 1}, p->slt);
           rc = add_gemm(p, Gr, Cr, ai, bi1, (int)(2 * ldl), 1, p->Q + s * ls(i), szQ, 1, 2 * ls(i), 0, 1.f, nullptr, 0,
                         0, 0, 0, 0, p->Ql ? p->Ql + s * ls(i) : nullptr);
           if (rc) return bail(rc);
