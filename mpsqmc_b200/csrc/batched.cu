@@ -524,9 +524,11 @@ __global__ void env_init_kernel(const float *P, long psz, long pld, int a, int b
 
 // G[t](r, c) = delta_st Fd + sum_e J_e (Sx(s,t) F_x - iSy(s,t) F_y + Sz(s,t) F_z) for the channels
 // e closing on site k (a_k x b_k), sigma = s; stored Gb[r (2 gld) + t gld + c] (t stacked along K).
-__global__ void gbuild_kernel(int s, const float *Fd, long fsz, long fld, const float *Fch, long csz, int nslots,
+__global__ void gbuild_kernel(const float *Fd, long fsz, long fld, const float *Fch, long csz, int nslots,
                               const int *eslot, const float *eJ, int ne, int a, int b, EnvOps ops, float *Gb,
-                              long gsz, long gld, const int *n_cur, int cap) {
+                              long gsz, long gsig, long gld, const int *n_cur, int cap) {
+  // both sigma blocks of the site's operator rows from one read of Fd and the closing channels:
+  // G_s[t] = delta_st Fd + sum_e J_e (op_x[s + 2t] F_x - op_iy[s + 2t] F_iy + op_z[s + 2t] F_z)
   const int N = min(*n_cur, cap);
   const long blk = (long)a * b;
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < blk * N; e += (long)gridDim.x * blockDim.x) {
@@ -543,10 +545,13 @@ __global__ void gbuild_kernel(int s, const float *Fd, long fsz, long fld, const 
     }
     float *Gw = Gb + (long)w * gsz + (q / b) * 2 * gld + q % b;
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      const int o = s + 2 * t;
-      Gw[t * gld] = ((s == t) ? fd : 0.f) + (float)ops.opSx[o] * gx - (float)ops.opISy[o] * gy + (float)ops.opSz[o] * gz;
-    }
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int o = s + 2 * t;
+        Gw[s * gsig + t * gld] =
+            ((s == t) ? fd : 0.f) + (float)ops.opSx[o] * gx - (float)ops.opISy[o] * gy + (float)ops.opSz[o] * gz;
+      }
   }
 }
 
@@ -784,7 +789,7 @@ size_t bytes_needed(const Problem &pr) {
   }
   const long szBl = pad64(maxA * ldB), szX = pad64(2 * maxB * ldA), szN = pad64(maxB * ldB), szW = pad64(2 * maxB * ldB);
   const int ns = std::max(1, pr.nslots);
-  per += szBl * (1 + 4 + 2 + 2 + 3L * ns) + szX * (1 + 4 + 1 + 3L * ns) + 2 * szN + szW + pad64(2 * maxB * ldA);
+  per += szBl * (1 + 4 + 2 + 4 + 3L * ns) + szX * (1 + 4 + 1 + 3L * ns) + 2 * szN + szW + pad64(2 * maxB * ldA);
   if (pr.passes == 3) {  // tails of the right factors stored split
     const int sb = pr.tiles.split_out;
     per += szX * (((sb & kSplitY) ? 1 : 0) + ((sb & kSplitX) ? 1 : 0) + ((sb & kSplitX4) ? 4 : 0) +
@@ -922,7 +927,7 @@ int build(const Problem &pr, Plan **out) {
   rc |= palloc(p, &p->Lenv, p->szBl * cap) | palloc(p, &p->P, 4 * p->szBl * cap) | palloc(p, &p->X, p->szX * cap) |
         palloc(p, &p->X4, 4 * p->szX * cap) | palloc(p, &p->Y, p->szX * cap) | palloc(p, &p->Nl[0], p->szN * cap) |
         palloc(p, &p->Nl[1], p->szN * cap) | palloc(p, &p->Wn, p->szW * cap) | palloc(p, &p->Fd[0], p->szBl * cap) |
-        palloc(p, &p->Fd[1], p->szBl * cap) | palloc(p, &p->Gb, 2 * p->szBl * cap) |
+        palloc(p, &p->Fd[1], p->szBl * cap) | palloc(p, &p->Gb, 4 * p->szBl * cap) |
         palloc(p, &p->Q, pad64(2 * maxB * p->ldA) * cap) | palloc(p, &p->Fch, 3L * ns * p->szBl * cap) |
         palloc(p, &p->Xch, 3L * ns * p->szX * cap);
   // right factors written split, by class (bits of Tiles::split_out): the tails' arrays exist
@@ -1189,15 +1194,15 @@ int build(const Problem &pr, Plan **out) {
         const long szQ = pad64(2 * maxB * p->ldA);
         // per sigma: G_s[t] (rows r, K = (t, c)), Q_s = sum_t G_st C[t] in one product (t along K),
         // stored Q[c (2 ldA) + s ldA + m]; then done' += sum_s TO_i[s] Q_s in one product
+        p->ops.push_back([=](cudaStream_t st, double *) {
+          gbuild_kernel<<<grid_elems(P, (long)ai * bi), 256, 0, st>>>(Fdc, P->szBl, P->ldB, P->Fch, P->szBl, nsl, es_d,
+                                                                      ej_d, ne, ai, bi, eo, P->Gb, 4 * P->szBl,
+                                                                      2 * P->szBl, ldl, ncur, icap);
+          return cudaGetLastError() == cudaSuccess ? 0 : fail(MPSQMC_E_CUDA, "batched sweep: energy");
+        });
+        p->launches += 1;
         for (int s = 0; s < 2; ++s) {
-          p->ops.push_back([=](cudaStream_t st, double *) {
-            gbuild_kernel<<<grid_elems(P, (long)ai * bi), 256, 0, st>>>(s, Fdc, P->szBl, P->ldB, P->Fch, P->szBl, nsl,
-                                                                        es_d, ej_d, ne, ai, bi, eo, P->Gb, 2 * P->szBl,
-                                                                        ldl, ncur, icap);
-            return cudaGetLastError() == cudaSuccess ? 0 : fail(MPSQMC_E_CUDA, "batched sweep: energy");
-          });
-          p->launches += 1;
-          Opnd Gr{p->Gb, 2 * ldl, ai, 2 * p->szBl, cap, 1};
+          Opnd Gr{p->Gb + 2L * s * p->szBl, 2 * ldl, ai, 4 * p->szBl, cap, 1};
           const Opnd Cr = Fm(Opnd{p->SL + p->sl_off[i], 2 * ldl, bi1, p->sl_sz[i], cap, 1}, p->slt);
           rc = add_gemm(p, Gr, Cr, ai, bi1, (int)(2 * ldl), 1, p->Q + s * ls(i), szQ, 1, 2 * ls(i), 0, 1.f, nullptr, 0,
                         0, 0, 0, 0, p->Ql ? p->Ql + s * ls(i) : nullptr);
