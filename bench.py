@@ -57,7 +57,7 @@ def parse():
                          "throughput (blocking error of the mixed energy; first 20%% discarded)")
     ap.add_argument("--workspace", default="auto", choices=["auto", "global"],
                     help="matrix work buffers: shared memory when they fit (auto) or global scratch")
-    ap.add_argument("--precision", default=None, choices=["fp64", "tf32x3", "tf32", "tf32x3_tc", "tf32_tc"],
+    ap.add_argument("--precision", default=None, choices=["fp64", "tf32x3", "tf32", "tf32x3_tc", "tf32_tc", "bf16_tc"],
                     help="walker-step contractions: FP64 tensor cores, or FP32 buffers on TF32 tensor cores "
                          "(three passes / one pass; *_tc: the walker-batched sweep on tcgen05); weights, "
                          "overlaps, energies stay FP64.  Default: tf32x3_tc on snake8x8, fp64 otherwise")
@@ -93,7 +93,7 @@ def parse():
     return a
 
 
-PRECISIONS = {"fp64": 0, "tf32": 1, "tf32x3": 2, "tf32x3_tc": 3, "tf32_tc": 4}
+PRECISIONS = {"fp64": 0, "tf32": 1, "tf32x3": 2, "tf32x3_tc": 3, "tf32_tc": 4, "bf16_tc": 5}
 
 
 def configure(eng, args, sweep, plain=False):
@@ -244,15 +244,16 @@ def fp64_peak_tflops():
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def tf32_peak_tflops():
-    """cuBLAS FP32 GEMM 8192^3 with TF32 tensor cores allowed, best of 5 (CUDA events): the
-    denominator of the mixed-precision sweep."""
+def tf32_peak_tflops(dtype="float32"):
+    """cuBLAS GEMM 8192^3, best of 5 (CUDA events): FP32 with TF32 tensor cores allowed (the
+    denominator of the TF32 sweeps) or bfloat16 (that of the BF16 sweep)."""
     import torch
     keep = torch.backends.cuda.matmul.allow_tf32
     torch.backends.cuda.matmul.allow_tf32 = True
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float32, device="cuda")
-    b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    dt = getattr(torch, dtype)
+    a = torch.randn(n, n, dtype=torch.float32, device="cuda").to(dt)
+    b = torch.randn(n, n, dtype=torch.float32, device="cuda").to(dt)
     c = a @ b
     best = 1e9
     for _ in range(5):
@@ -460,7 +461,7 @@ def main():
     achieved = flops_ws * ws_done / (k_ms * 1e-3) / 1e12
     mixed = args.precision != "fp64"
     tc = args.precision.endswith("_tc")
-    passes = 1 if args.precision in ("tf32", "tf32_tc") else 3
+    passes = 1 if args.precision in ("tf32", "tf32_tc", "bf16_tc") else 3
     E_last = {"E_P_last": stats[-1]["E_P"], "E_T_last": stats[-1]["E_T"], "walkers_last": stats[-1]["n_after"],
               "E_P_mean": float(np.mean([s["E_P"] for s in stats]))}
 
@@ -548,7 +549,8 @@ def main():
 
     peak = None
     if rank == 0:
-        peak = tf32_peak_tflops() if mixed else fp64_peak_tflops()
+        peak = (tf32_peak_tflops("bfloat16") if args.precision == "bf16_tc" else tf32_peak_tflops()) if mixed \
+            else fp64_peak_tflops()
 
     # end to end through the public API: host population -> device, K steps (stats read back each
     # step), population -> host; host wall clock.
@@ -604,8 +606,10 @@ def main():
                                    if tc else "the walker-step kernel on the engine's stream"),
                          **({"passes": passes, "executed_frac": passes * achieved / peak if peak else None}
                             if mixed else {}),
-                         "peak_source": ("cuBLAS TF32 GEMM 8192^3 measured in this run (TF32 tensor path; the "
-                                         "canonical flops count each product once)") if mixed else
+                         "peak_source": ("cuBLAS %s GEMM 8192^3 measured in this run (%s tensor path; the "
+                                         "canonical flops count each product once)"
+                                         % (("BF16", "BF16") if args.precision == "bf16_tc" else ("TF32", "TF32")))
+                         if mixed else
                                         "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor path)"},
             "cpu_baseline": cpu,
             "e2e": e2e,

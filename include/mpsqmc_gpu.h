@@ -226,6 +226,10 @@ int mpsqmc_last_timing(mpsqmc_ctx *ctx, double *step_kernel_ms, double *total_ms
                                       *   proposal; its trace records C/ov, the factor, uniform,
                                       *   index, weight and the overlap ratio per coupling. */
 #define MPSQMC_PRECISION_TF32_TC 4   /*   the same with one TF32 pass per product */
+#define MPSQMC_PRECISION_BF16_TC 5   /*   the same with one bfloat16 pass per product (tcgen05
+                                      *   kind::f16, FP32 accumulation): operands rounded to 8
+                                      *   mantissa bits, for callers that trade accuracy (local
+                                      *   energies about 1e-2 relative) for speed */
 #define MPSQMC_OPT_PROPOSAL 8        /* how a coupling's grid point is drawn (what a
                                       * set_proposal(GRID | LEARNED) entry point would select): */
 #define MPSQMC_PROPOSAL_GRID 0       /*   the exact grid PDF, as MPSQMC2.cpp:551-588 (default) */
@@ -325,7 +329,8 @@ int mpsqmc_autotune(mpsqmc_ctx *ctx, int steps, int *best_sweep, int *best_works
  * cover it), A rows up to a multiple of 64 (M <= 64) or 128, B rows up to a multiple of the tile
  * width (N rounded up to 16, at most 256) when bstack = 1, and a_zcount / b_zcount operand
  * entries allocated (B: at least Z rounded up to bstack when stacked).  Strides are multiples of 4
- * and pointers 16-byte aligned.  passes = 3: FP32-accurate (head/tail TF32 split), 1: TF32.
+ * and pointers 16-byte aligned.  passes = 3: FP32-accurate (head/tail TF32 split), 1: TF32,
+ * 16: one bfloat16 pass (kind::f16; operands rounded to bfloat16, FP32 accumulation).
  * Device pointers; asynchronous on `stream`.  *err (device int) receives bit 4 if a pipeline wait
  * timed out.  Returns 0 or a negative status. */
 int mpsqmc_tc_gemm(float *D, const float *A, const float *B, int M, int N, int K, long lda, long a_zstride,

@@ -27,6 +27,8 @@ PROJECTOR_TROTTER, PROJECTOR_MPO_TERMS = 0, 1
 OPT_CANONICAL_INTERVAL = 6
 OPT_PRECISION = 7
 PRECISION_FP64, PRECISION_TF32, PRECISION_TF32X3, PRECISION_TF32X3_TC, PRECISION_TF32_TC = 0, 1, 2, 3, 4
+PRECISION_BF16_TC = 5  # the tcgen05 sweep with one bfloat16 pass per product
+TC_PASSES_BF16 = 16    # tc_gemm's `passes` for one bfloat16 pass
 OPT_PROPOSAL = 8
 PROPOSAL_GRID, PROPOSAL_LEARNED = 0, 1
 OPT_PROPOSAL_TRAINING = 9

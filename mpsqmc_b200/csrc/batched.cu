@@ -144,8 +144,8 @@ int pick_stages(GemmParams &p, int max_stages = kMaxStages) {
   int sms = 0, limit = 0;
   const int rc = configure_kernel(&sms, &limit);
   if (rc) return rc;
-  p.stages = std::max(2, std::min(max_stages, stages_for(p.tm, p.tn, p.passes, limit, p.dsplit, p.kc)));
-  if (smem_bytes(p.tm, p.tn, p.passes, p.stages, p.dsplit, p.kc) > limit)
+  p.stages = std::max(2, std::min(max_stages, stages_for(p.tm, p.tn, p.passes, limit, p.dsplit, p.kc, p.bf16)));
+  if (smem_bytes(p.tm, p.tn, p.passes, p.stages, p.dsplit, p.kc, p.bf16) > limit)
     return fail(MPSQMC_E_UNSUPPORTED, "tcgen05 GEMM tile does not fit in shared memory");
   return 0;
 }
@@ -156,7 +156,7 @@ int launch(const GemmParams &p, long max_tiles, cudaStream_t stream) {
   int rc = configure_kernel(&sms, nullptr);
   if (rc) return rc;
   const int grid = (int)std::max(1L, std::min((long)sms, max_tiles));
-  tc_gemm_kernel<<<grid, kThreads, smem_bytes(p.tm, p.tn, p.passes, p.stages, p.dsplit, p.kc), stream>>>(p);
+  tc_gemm_kernel<<<grid, kThreads, smem_bytes(p.tm, p.tn, p.passes, p.stages, p.dsplit, p.kc, p.bf16), stream>>>(p);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(MPSQMC_E_CUDA, std::string("tcgen05 GEMM launch: ") + cudaGetErrorString(e));
   return 0;
@@ -172,7 +172,8 @@ extern "C" int mpsqmc_tc_gemm(float *D, const float *A, const float *B, int M, i
   using namespace mq::tc;
   if (!D || !A || !B || !err) return fail(MPSQMC_E_ARG, "null pointer");
   if (M < 1 || N < 1 || K < 1 || Z < 1 || bstack < 1) return fail(MPSQMC_E_ARG, "sizes must be positive");
-  if (passes != 1 && passes != 3) return fail(MPSQMC_E_ARG, "passes must be 1 or 3");
+  if (passes != 1 && passes != 3 && passes != kPassesBF16)
+    return fail(MPSQMC_E_ARG, "passes must be 1, 3 or 16 (one BF16 pass)");
   if (lda < ((K + kKC - 1) / kKC) * kKC || ldb < ((K + kKC - 1) / kKC) * kKC)
     return fail(MPSQMC_E_ARG, "lda and ldb must cover K rounded up to a multiple of 32 (zero padded)");
   GemmParams p;
@@ -196,7 +197,8 @@ extern "C" int mpsqmc_tc_gemm(float *D, const float *A, const float *B, int M, i
   p.Z = Z;
   p.alpha = alpha;
   p.beta = beta;
-  p.passes = passes;
+  p.passes = passes == kPassesBF16 ? 1 : passes;
+  p.bf16 = passes == kPassesBF16;
   p.D = D;
   p.dz = dz;
   p.dm = dm;
@@ -706,7 +708,9 @@ int add_gemm(Plan *p, const Opnd &A, const Opnd &B, int M, int N, int K, int zpe
   g.K = K;
   g.tm = tm_for(M);
   const Tiles &t = p->pr.tiles;
-  g.kc = A.div == 0 ? t.kc_trial : kKC;  // k-values per stage (the trial products' is a tile choice)
+  g.bf16 = p->pr.bf16 ? 1 : 0;
+  // k-values per stage (the trial products' is a tile choice; BF16 stages take 32)
+  g.kc = (A.div == 0 && !g.bf16) ? t.kc_trial : kKC;
   int bstack = 1;
   if (A.div == 0 && (N & 7) == 0 && 2 * N <= t.stack_tn) bstack = t.stack_tn / N;
   if (bstack > 1) {

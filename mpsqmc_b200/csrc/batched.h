@@ -59,7 +59,8 @@ struct Problem {
   const double *tabU = nullptr, *tabSq = nullptr, *tabVT = nullptr, *grid = nullptr;
   int *err = nullptr;
   int capacity = 0;                // walkers the batched buffers hold
-  int passes = 3;                  // 3: FP32-accurate products, 1: TF32
+  int passes = 3;                  // 3: FP32-accurate products, 1: TF32 (or BF16 with bf16)
+  bool bf16 = false;               // one BF16 pass (kind::f16) instead of TF32
   Tiles tiles;
 };
 

@@ -293,7 +293,9 @@ bool qr_free(const mpsqmc_ctx *c) {
 
 // The walker-batched sweep on the tcgen05 tensor cores (batched.h).
 bool tc_sweep(const mpsqmc_ctx *c) {
-  return (c->precision == MPSQMC_PRECISION_TF32X3_TC || c->precision == MPSQMC_PRECISION_TF32_TC) && mixed(c);
+  return (c->precision == MPSQMC_PRECISION_TF32X3_TC || c->precision == MPSQMC_PRECISION_TF32_TC ||
+          c->precision == MPSQMC_PRECISION_BF16_TC) &&
+         mixed(c);
 }
 
 // Steps between two left-normalisations of the QR-free sweep.
@@ -1123,8 +1125,10 @@ static int ensure_batched(mpsqmc_ctx *c) {
     for (int k = 0; k <= L; ++k)
       if (all[(size_t)slots[w] * (L + 1) + k] != c->bW[k])
         return fail(MPSQMC_E_UNSUPPORTED, "the tcgen05 sweep needs every walker in the slot layout's bond profile");
-  const int passes = c->precision == MPSQMC_PRECISION_TF32_TC ? 1 : 3;
-  if (c->bplan && c->bplan_passes == passes && c->bplan_tiles == c->tc_tiles) return 0;
+  const bool bf16 = c->precision == MPSQMC_PRECISION_BF16_TC;
+  const int passes = (c->precision == MPSQMC_PRECISION_TF32_TC || bf16) ? 1 : 3;
+  const int kind = bf16 ? 16 : passes;  // what the plan was built for
+  if (c->bplan && c->bplan_passes == kind && c->bplan_tiles == c->tc_tiles) return 0;
   if (c->bplan) {
     mq::bs::destroy(c->bplan);
     c->bplan = nullptr;
@@ -1169,6 +1173,7 @@ static int ensure_batched(mpsqmc_ctx *c) {
   pr.grid = c->d_grid;
   pr.err = c->d_err;
   pr.passes = passes;
+  pr.bf16 = bf16;
   pr.tiles = c->tc_tiles;
   // buffers for the whole slot capacity when they fit in half the free memory, else for 1.5x the
   // target population (a step with more walkers then stops with MPSQMC_E_CAPACITY)
@@ -1181,7 +1186,7 @@ static int ensure_batched(mpsqmc_ctx *c) {
     return fail(MPSQMC_E_CAPACITY, "the tcgen05 sweep's work buffers do not fit in device memory");
   const int rc = mq::bs::build(pr, &c->bplan);
   if (rc) return rc;
-  c->bplan_passes = passes;
+  c->bplan_passes = kind;
   c->bplan_tiles = pr.tiles;
   c->bcap = pr.capacity;
   drop_graphs(c);
@@ -1404,7 +1409,11 @@ std::string tune_key(const mpsqmc_ctx *c) {
   for (int v : c->aT) k << v << ',';
   k << '|';
   for (int v : c->bW) k << v << ',';
-  k << '|' << (tc_sweep(c) ? (c->precision == MPSQMC_PRECISION_TF32_TC ? "tc1" : "tc3") : "cta");
+  k << '|'
+    << (tc_sweep(c) ? (c->precision == MPSQMC_PRECISION_TF32_TC   ? "tc1"
+                       : c->precision == MPSQMC_PRECISION_BF16_TC ? "bf16"
+                                                                  : "tc3")
+                    : "cta");
   return k.str();
 }
 
@@ -1526,7 +1535,8 @@ int mpsqmc_autotune(mpsqmc_ctx *c, int steps, int *best_sweep, int *best_workspa
     // axes: 0 split right factors, 1 k-values per stage of the trial products, 2 stacked tile
     // width, 3 the walker products' tile width, 4 ring depth cap
     for (int axis = 0; axis < 5 && !rc; ++axis) {
-      if (axis == 0 && c->precision == MPSQMC_PRECISION_TF32_TC) continue;  // one pass: nothing to split
+      if (axis == 0 && c->precision != MPSQMC_PRECISION_TF32X3_TC) continue;  // one pass: nothing to split
+      if (axis == 1 && c->precision == MPSQMC_PRECISION_BF16_TC) continue;    // BF16 stages take 32 values
       const std::vector<int> vals = axis == 0   ? std::vector<int>{mq::bs::kSplitX4, mq::bs::kSplitXch, mq::bs::kSplitY,
                                                                  mq::bs::kSplitX, mq::bs::kSplitQ}
                                     : axis == 1 ? std::vector<int>{16}
@@ -1656,7 +1666,7 @@ int mpsqmc_set_option(mpsqmc_ctx *c, int option, long value) {
       c->canon_interval = (int)value;
       break;
     case MPSQMC_OPT_PRECISION:
-      if (value < MPSQMC_PRECISION_FP64 || value > MPSQMC_PRECISION_TF32_TC) return fail(MPSQMC_E_ARG, "unknown precision");
+      if (value < MPSQMC_PRECISION_FP64 || value > MPSQMC_PRECISION_BF16_TC) return fail(MPSQMC_E_ARG, "unknown precision");
       c->precision = (int)value;
       if (c->bplan && !tc_sweep(c)) {
         CK(cudaStreamSynchronize(c->stream));

@@ -34,6 +34,7 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 #include <stdint.h>
 
 namespace mq {
@@ -47,6 +48,7 @@ constexpr int kErrTimeout = 4;          // bit in the device error word (batched
 constexpr long long kWaitCycles = 4000000000LL;  // a pipeline wait gives up after ~2 s of SM cycles
 
 enum Epilogue : int { kStore = 0, kDot4 = 1 };
+constexpr int kPassesBF16 = 16;         // mpsqmc_tc_gemm's `passes` value for one BF16 pass
 
 struct alignas(64) GemmParams {
   CUtensorMap tmA;   // 3D (k, row, z): FP32, box (32, tm, 1), SWIZZLE_128B
@@ -76,6 +78,8 @@ struct alignas(64) GemmParams {
   float alpha;
   int beta;          // 1: accumulate into D
   int passes;        // 1 or 3
+  int bf16;          // 1: one BF16 pass (kind::f16): each landed FP32 stage (kc = 32) is rounded to
+                     // bfloat16 into a 64-byte-swizzled copy that the products read
   int stages;        // shared-memory stages of the load ring (2 .. kMaxStages)
   int kc;            // k-values per stage: 32 (SWIZZLE_128B) or 16 (SWIZZLE_64B)
   float *D;
@@ -186,9 +190,18 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t row_bytes)
   return d;
 }
 
-// kind::tf32, FP32 accumulator, both operands K-major.
-__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// kind::tf32 (operand format 2) or kind::f16 with bfloat16 operands (format 1), FP32 accumulator,
+// both operands K-major.
+__host__ __device__ constexpr uint32_t instr_desc(int M, int N, bool bf16 = false) {
+  return (1u << 4) | ((bf16 ? 1u : 2u) << 7) | ((bf16 ? 1u : 2u) << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc));
 }
 
 __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
@@ -270,6 +283,13 @@ __device__ __forceinline__ void tile_coords(const GemmParams &p, const Tiling &t
   }
 }
 
+// Two FP32 values rounded to bfloat16 (nearest, ties to even) and packed, the first in the low half
+// (the lower k in a K-major row).
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t *>(&v);
+}
+
 // x rounded to the nearest TF32 value (10 explicit mantissa bits), ties away from zero, as an
 // FP32 bit pattern: half of the 13 dropped bits' range is added to the magnitude bits, which are
 // then cleared (a carry into the exponent is the correct rounding).  Two integer operations at
@@ -294,11 +314,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
   uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const uint32_t row_bytes = (uint32_t)p.kc * 4;  // one tile row of kc FP32 values
   const uint32_t a_bytes = (uint32_t)p.tm * row_bytes, b_bytes = (uint32_t)p.tn * row_bytes;
-  const uint32_t lo_mult = (p.passes == 3) ? 2u : 1u;  // head (+ tail) tiles per operand
-  const uint32_t stage_bytes = lo_mult * (a_bytes + b_bytes);
+  const bool bf16 = p.bf16 != 0;
+  const uint32_t lo_mult = (p.passes == 3 && !bf16) ? 2u : 1u;  // head (+ tail) tiles per operand
+  // BF16: [A FP32 | B FP32 | A BF16 | B BF16], the BF16 rows 64 bytes (32 values)
+  const uint32_t stage_bytes = bf16 ? (a_bytes + b_bytes) * 3 / 2 : lo_mult * (a_bytes + b_bytes);
   const uint32_t b_load = (uint32_t)p.brows * p.bstack * row_bytes;  // bytes one B box brings
-  const int split = p.passes == 3 ? (p.presplit & 3) : 0;
-  const bool conv = p.passes == 3 && split != 3;  // a landed stage still needs splitting
+  const int split = (p.passes == 3 && !bf16) ? (p.presplit & 3) : 0;
+  const bool conv = bf16 || (p.passes == 3 && split != 3);  // a landed stage still needs splitting
   float *stagebuf = reinterpret_cast<float *>(base + NS * stage_bytes);  // epilogue transposes
   const Tiling t = tiling(p);
   const int KC = p.kc, nk = (p.K + KC - 1) / KC;
@@ -371,7 +393,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       uint32_t ph = 0;
       int acc = 0;
       uint32_t aph = 0;  // phase bit per accumulator (a register, not an indexed array)
-      const uint32_t idesc = instr_desc(p.tm, p.tn);
+      const uint32_t idesc = instr_desc(p.tm, p.tn, bf16);
       bool ok = true;
       for (int tile = blockIdx.x; tile < t.total && ok; tile += gridDim.x) {
         if (!mbar_wait(&bar_tempty[acc], ((aph >> acc) & 1u) ^ 1u, &abort_flag, p.err)) break;
@@ -386,7 +408,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           tc_fence_after();
           uint8_t *st = base + s * stage_bytes;
           const uint32_t ahi = smem_u32(st), alo = ahi + a_bytes, bhi = ahi + lo_mult * a_bytes, blo = bhi + b_bytes;
-          for (int kk = 0; kk < KC / 8; ++kk) {
+          if (bf16) {
+            // two K = 16 products over the stage's 32 BF16 values (32 bytes apart in the row)
+            const uint32_t ab = ahi + a_bytes + b_bytes, bb = ab + (uint32_t)p.tm * 64;
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk)
+              mma_bf16(dt, smem_desc(ab + kk * 32, 64), smem_desc(bb + kk * 32, 64), idesc,
+                       (kc == 0 && kk == 0) ? 0u : 1u);
+          }
+          for (int kk = 0; kk < (bf16 ? 0 : KC / 8); ++kk) {
             const uint32_t off = kk * 32;  // 8 TF32 values = 32 bytes inside the swizzle row
             const uint32_t first = (kc == 0 && kk == 0) ? 0u : 1u;
             mma_tf32(dt, smem_desc(ahi + off, row_bytes), smem_desc(bhi + off, row_bytes), idesc, first);
@@ -423,6 +453,35 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             break;
           }
           uint8_t *st = base + s * stage_bytes;
+          if (bf16) {
+            // each 16-byte BF16 piece (8 values of a 64-byte row, swizzled by (row / 2) % 4) from
+            // two 16-byte FP32 pieces of the landed 128-byte row (swizzled by row % 8)
+            const int rows = p.tm + p.tn;
+            uint8_t *dst = st + a_bytes + b_bytes;
+            for (int v = ct; v < rows * 4; v += 192) {
+              const int rr = v >> 2, c16 = v & 3;
+              const bool isa = rr < p.tm;
+              const int r = isa ? rr : rr - p.tm;  // row within its operand tile
+              const uint8_t *src = st + (isa ? 0u : a_bytes) + (uint32_t)r * 128;
+              const float4 x0 = *reinterpret_cast<const float4 *>(src + (((2 * c16) ^ (r & 7)) << 4));
+              const float4 x1 = *reinterpret_cast<const float4 *>(src + (((2 * c16 + 1) ^ (r & 7)) << 4));
+              uint4 o;
+              o.x = pack_bf16(x0.x, x0.y);
+              o.y = pack_bf16(x0.z, x0.w);
+              o.z = pack_bf16(x1.x, x1.y);
+              o.w = pack_bf16(x1.z, x1.w);
+              uint8_t *row = dst + (isa ? 0u : (uint32_t)p.tm * 64) + (uint32_t)r * 64;
+              *reinterpret_cast<uint4 *>(row + ((c16 ^ ((r >> 1) & 3)) << 4)) = o;
+            }
+            fence_proxy_async();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar_conv[s]);
+            if (++s == NS) {
+              s = 0;
+              ph ^= 1;
+            }
+            continue;
+          }
           // A: [hi | lo] then B: [hi | lo]; 16-byte vectors; operands loaded split are skipped
           const int na = (int)(a_bytes / 16), nb = (int)(b_bytes / 16);
           const int v0 = (split & 1) ? na : 0, v1 = (split & 2) ? na : na + nb;
@@ -837,19 +896,20 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
 
 // Shared memory of one launch: the stage ring (head and, with 3 passes, tail tiles), the
 // epilogue's transpose buffers and the 1024-byte alignment slack.
-__host__ __device__ constexpr int stage_bytes_of(int tm, int tn, int passes, int kc = kKC) {
-  return (passes == 3 ? 2 : 1) * (tm + tn) * kc * 4;
+__host__ __device__ constexpr int stage_bytes_of(int tm, int tn, int passes, int kc = kKC, int bf16 = 0) {
+  return bf16 ? (tm + tn) * kc * 6 : (passes == 3 ? 2 : 1) * (tm + tn) * kc * 4;
 }
 // The epilogue's staging area: transposes (4 warps x 32 x 33 floats) or store boxes (4 warps x
 // 4 boxes of 32 x 16 floats, or two pairs of head and tail boxes).
 __host__ __device__ constexpr int staging_bytes(int dsplit) { return 4 * 2048 * 4 + 0 * dsplit; }
-__host__ __device__ constexpr int smem_bytes(int tm, int tn, int passes, int stages, int dsplit = 0, int kc = kKC) {
-  return stages * stage_bytes_of(tm, tn, passes, kc) + staging_bytes(dsplit) + 1024;
+__host__ __device__ constexpr int smem_bytes(int tm, int tn, int passes, int stages, int dsplit = 0, int kc = kKC,
+                                            int bf16 = 0) {
+  return stages * stage_bytes_of(tm, tn, passes, kc, bf16) + staging_bytes(dsplit) + 1024;
 }
 // As many stages (2 .. kMaxStages) as fit in the opt-in shared memory.
-inline int stages_for(int tm, int tn, int passes, int smem_limit, int dsplit = 0, int kc = kKC) {
+inline int stages_for(int tm, int tn, int passes, int smem_limit, int dsplit = 0, int kc = kKC, int bf16 = 0) {
   int s = kMaxStages;
-  while (s > 2 && smem_bytes(tm, tn, passes, s, dsplit, kc) > smem_limit) --s;
+  while (s > 2 && smem_bytes(tm, tn, passes, s, dsplit, kc, bf16) > smem_limit) --s;
   return s;
 }
 

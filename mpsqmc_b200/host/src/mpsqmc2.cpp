@@ -121,21 +121,21 @@ void MPSQMC2::Setup(MPSstate *trial) {
     struct Named {
       const char *var;
       int option;
-      const char *names[5];
-      long values[5];
+      const char *names[6];
+      long values[6];
     };
     const Named named[] = {
-        {"MPSQMC_PRECISION", MPSQMC_OPT_PRECISION, {"fp64", "tf32", "tf32x3", "tf32x3_tc", "tf32_tc"},
+        {"MPSQMC_PRECISION", MPSQMC_OPT_PRECISION, {"fp64", "tf32", "tf32x3", "tf32x3_tc", "tf32_tc", "bf16_tc"},
          {MPSQMC_PRECISION_FP64, MPSQMC_PRECISION_TF32, MPSQMC_PRECISION_TF32X3, MPSQMC_PRECISION_TF32X3_TC,
-          MPSQMC_PRECISION_TF32_TC}},
-        {"MPSQMC_RESAMPLING", MPSQMC_OPT_RESAMPLING, {"threshold", "comb", nullptr, nullptr, nullptr},
-         {MPSQMC_RESAMPLE_THRESHOLD, MPSQMC_RESAMPLE_COMB, 0, 0, 0}}};
+          MPSQMC_PRECISION_TF32_TC, MPSQMC_PRECISION_BF16_TC}},
+        {"MPSQMC_RESAMPLING", MPSQMC_OPT_RESAMPLING, {"threshold", "comb", nullptr, nullptr, nullptr, nullptr},
+         {MPSQMC_RESAMPLE_THRESHOLD, MPSQMC_RESAMPLE_COMB, 0, 0, 0, 0}}};
     for (const Named &o : named) {
       const char *v = getenv(o.var);
       if (!v) continue;
       int k = 0;
-      while (k < 5 && o.names[k] && std::string(v) != o.names[k]) ++k;
-      if (k == 5 || !o.names[k] || mpsqmc_set_option(ctx, o.option, o.values[k]) != MPSQMC_OK)
+      while (k < 6 && o.names[k] && std::string(v) != o.names[k]) ++k;
+      if (k == 6 || !o.names[k] || mpsqmc_set_option(ctx, o.option, o.values[k]) != MPSQMC_OK)
         cerr << "MPSQMC2: ignoring " << o.var << "=" << v << endl;
     }
     const std::pair<const char *, int> counts[] = {{"MPSQMC_CANONICAL_INTERVAL", MPSQMC_OPT_CANONICAL_INTERVAL},

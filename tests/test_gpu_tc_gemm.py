@@ -111,3 +111,49 @@ def test_tc_gemm_alpha_beta_and_layouts(colmajor):
     assert fp32_accurate(*run_case(128, 64, 64, 5, 1, 1, 1, 3, alpha=0.5, beta=0, colmajor=colmajor))
     assert fp32_accurate(*run_case(256, 32, 256, 8, 0, 1, 8, 3, alpha=-2.0, beta=0, colmajor=colmajor))
     assert fp32_accurate(*run_case(64, 48, 32, 7, 1, 1, 1, 3, alpha=1.5, beta=0, colmajor=colmajor))
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"M{c[0]}N{c[1]}K{c[2]}Z{c[3]}a{c[4]}b{c[5]}s{c[6]}" for c in CASES])
+def test_tc_gemm_bf16_pass(case):
+    """One bfloat16 pass (kind::f16): the product equals that of the operands rounded to bfloat16
+    (nearest, ties to even), accumulated in FP32; against an FP64 product of the rounded inputs
+    within FP32 accumulation error (5e-5 of max |D|), and within 1e-2 of the unrounded product."""
+    import torch
+
+    M, N, K, Z, adiv, bdiv, bstack = case
+    g = torch.Generator().manual_seed(1)
+    dev = "cuda"
+    tm = 64 if M <= 64 else 128
+    kp = _pad(K, 32)
+    tn = _pad(N * bstack, 16) if bstack > 1 else min(256, _pad(N, 16))
+    ar, br = _pad(M, tm), (N if bstack > 1 else _pad(N, tn))
+    za = 1 if adiv == 0 else (Z - 1) // adiv + 1
+    zb = 1 if bdiv == 0 else (Z - 1) // bdiv + 1
+    if bstack > 1:
+        zb = _pad(zb, bstack)
+    A = torch.zeros((za, ar, kp))
+    B = torch.zeros((zb, br, kp))
+    A[:, :M, :K] = torch.randn((za, M, K), generator=g)
+    B[:, :N, :K] = torch.randn((zb, N, K), generator=g)
+    ai = torch.tensor([z // adiv if adiv else 0 for z in range(Z)])
+    bi = torch.tensor([z // bdiv if bdiv else 0 for z in range(Z)])
+    Ar, Br = A.bfloat16().double(), B.bfloat16().double()
+    ref_r = torch.einsum("zmk,znk->zmn", Ar[ai, :M, :K], Br[bi, :N, :K])
+    ref = torch.einsum("zmk,znk->zmn", A[ai, :M, :K].double(), B[bi, :N, :K].double())
+    D = torch.zeros((Z, M, N), device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    Ad, Bd = A.to(dev), B.to(dev)
+    rc = capi.tc_gemm(D=D.data_ptr(), A=Ad.data_ptr(), B=Bd.data_ptr(), M=M, N=N, K=K, lda=kp, a_zstride=ar * kp,
+                      adiv=adiv, a_zcount=za, ldb=kp, b_zstride=br * kp, bdiv=bdiv, b_zcount=zb, Z=Z, bstack=bstack,
+                      alpha=1.0, beta=0, passes=capi.TC_PASSES_BF16, dz=M * N, dm=N, dn=1, err=err.data_ptr(),
+                      stream=torch.cuda.current_stream().cuda_stream)
+    assert rc == 0, capi.load().mpsqmc_last_error().decode()
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    out = D.cpu().double()
+    scale = float(ref_r.abs().max())
+    e_r = float((out - ref_r).abs().max()) / scale
+    e = float((out - ref).abs().max()) / scale
+    print(f"{case} bf16: {e_r:.2e} vs rounded inputs, {e:.2e} vs FP64")
+    assert e_r < 5e-5
+    assert e < 1e-2

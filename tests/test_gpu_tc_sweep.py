@@ -13,7 +13,7 @@ import pytest
 from conftest import couplings, load_golden
 from mpsqmc_b200 import Engine
 from mpsqmc_b200.capi import (E_UNSUPPORTED, OPT_PRECISION, OPT_TC_KC, OPT_TC_SPLIT_OUT, OPT_TC_STACK_TN,
-                              OPT_TC_STAGES, OPT_TC_WIDE_TN,
+                              OPT_TC_STAGES, OPT_TC_WIDE_TN, PRECISION_BF16_TC,
                               PRECISION_TF32_TC, PRECISION_TF32X3, PRECISION_TF32X3_TC, TRACE_STRIDE, MpsqmcError)
 
 pytestmark = pytest.mark.gpu
@@ -79,6 +79,18 @@ def test_tc_one_pass_is_close():
     eng = engine_for(z, PRECISION_TF32_TC)
     st = eng.walk(1)[0]
     assert st["E_P"] == pytest.approx(z["stat_EP"][0], rel=2e-3)
+    eng.close()
+
+
+def test_tc_bf16_pass_is_close():
+    """The tcgen05 sweep with one bfloat16 pass per product (MPSQMC_PRECISION_BF16_TC): operands
+    carry 8 mantissa bits, so the first step's E_P is checked loosely against the reference
+    (5e-2; the FP32-accurate mode is the one held to the reference's trajectory)."""
+    z = load_golden("walk_L16D16_DW16")
+    eng = engine_for(z, PRECISION_BF16_TC)
+    st = eng.walk(1)[0]
+    print(f"bf16 E_P {st['E_P']:.8f} vs {z['stat_EP'][0]:.8f}")
+    assert st["E_P"] == pytest.approx(z["stat_EP"][0], rel=5e-2)
     eng.close()
 
 
