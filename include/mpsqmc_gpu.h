@@ -310,7 +310,7 @@ int mpsqmc_proposal_stats(mpsqmc_ctx *ctx, double *last_loss, int *updates);
  * (MPSQMC_OPT_SWEEP, MPSQMC_OPT_WORKSPACE) choice on the first walkers of the current population
  * (two waves of one CTA per SM), restores the population, random stream and step count after
  * each trial, and keeps the fastest.  Under the tcgen05 sweep (MPSQMC_PRECISION_TF32X3_TC,
- * TF32_TC) it instead tunes that sweep's choices (MPSQMC_OPT_TC_SPLIT_OUT, _KC, _STACK_TN,
+ * TF32_TC, BF16_TC) it instead tunes that sweep's choices (MPSQMC_OPT_TC_SPLIT_OUT, _KC, _STACK_TN,
  * _WIDE_TN, _STAGES) by a coordinate search from the defaults, each timed on up to 1024 walkers (its tile counts
  * grow with the population).  The choice is remembered per problem shape (L, trial and walker
  * bond dims, couplings, projector, sweep family) for later contexts of this process, which then
