@@ -14,7 +14,8 @@
 // Precision: with passes = 3 every tile is split in shared memory into an exactly-TF32 head
 // (x rounded to TF32) and a tail ((x - head) rounded to TF32), and the accumulator takes
 // A_hi B_hi + A_hi B_lo + A_lo B_hi: about FP32 accuracy (relative error ~2^-22 per product term)
-// with FP32 accumulation in TMEM.  passes = 1 runs A_hi B_hi only (TF32).  Operands kept in
+// with FP32 accumulation in TMEM.  passes = 1 runs A_hi B_hi only (TF32); bf16 runs one
+// kind::f16 pass on the operands rounded to bfloat16 by the converter warps.  Operands kept in
 // memory as separate head and tail arrays (the trial tensors, and outputs a product writes
 // split for the next one) are loaded split: four TMA boxes per stage and no conversion, which
 // takes the split's shared-memory reads and writes off the stage.
@@ -22,7 +23,8 @@
 // Roles (384 threads, one CTA per SM, persistent over tiles):
 //   warp 0      TMA producer (one lane), ring of 2-4 shared-memory stages (as many as fit);
 //   warp 1      TMEM owner and MMA issuer (one lane); two or four accumulators of tn columns;
-//   warps 2-7   head/tail split of each landed stage (passes = 3, operands not stored split);
+//   warps 2-7   head/tail split of each landed stage (passes = 3, operands not stored split), or
+//               its rounding to bfloat16 (bf16);
 //   warps 8-11  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM lanes 32 (w % 4)...),
 //               alpha/beta and the store to D; column-major outputs go through shared-memory
 //               boxes and TMA bulk tensor stores (as head and tail arrays when the consumer
