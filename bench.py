@@ -74,8 +74,9 @@ def parse():
     ap.add_argument("--vn-compare", type=int, default=None, metavar="STEPS",
                     help="variance-normalised throughput (the headline metric) of the plain FP64 grid walk "
                          "and of the --vn-arms variants, STEPS steps each after their timed steps, from the "
-                         "same start and random stream; ratios against the plain walk (default: 300 on the "
-                         "default chain64 run, else off)")
+                         "same start and random stream; ratios against the plain walk (default off: the FP64 "
+                         "arm's steps at config 5 take 20 s each; the default line reports the throughput "
+                         "ratio of the same walk in fp64_arm)")
     ap.add_argument("--sharded", action="store_true",
                     help="N>1: one walk split over the ranks (global population control and walker "
                          "balancing, mpsqmc_b200.population; NCCL, records in device buffers) instead of N "
